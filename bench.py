@@ -1,0 +1,330 @@
+#!/usr/bin/env python3
+"""Benchmark: LDE + Merkle commit throughput on B200 (elements/s).
+
+Workload (one step = one commit on each GPU): 256 columns of 2^15 Goldilocks
+coefficients, rate_bits 3 -> coset LDE of 2^18 points per column, bit-reversed
+into 2^18 leaf rows of 256 elements, Poseidon2 Merkle forest with cap height 4.
+Unit of work: one committed LDE element (2^18 * 256 = 67,108,864 per step).
+Synthetic seeded field data (splitmix64, values in [0, p)).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+For N > 1 run under torchrun; every rank commits its own job (weak scaling,
+no data-path collective).  Rank 0 prints one JSON line.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+P = 0xFFFFFFFF00000001
+METRIC = "LDE+Merkle commit elems/s"
+LG_N, RATE, COLS, CAP, HASH = 15, 3, 256, 4, 3  # Poseidon2
+HBM_FALLBACK_GBS = 6650.0
+P2_MULS_PER_PERM = 736  # full-width multiplies per Poseidon2 permutation
+
+
+def field_data(seed, n):
+    """Seeded field elements in [0, p) (splitmix64 counters, values >= p folded)."""
+    k = np.arange(n, dtype=np.uint64)
+    with np.errstate(over="ignore"):
+        z = np.uint64((seed << 32) & 0xFFFFFFFFFFFFFFFF) + (k + np.uint64(1)) * np.uint64(0x9E3779B97F4A7C15)
+        z = (z ^ (z >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)
+        z = (z ^ (z >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
+        z = z ^ (z >> np.uint64(31))
+    return np.where(z >= np.uint64(P), z - np.uint64(P), z)
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return HBM_FALLBACK_GBS, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.Q,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.t.join(timeout=2)
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx.append(float(f[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def cpu_commit_sample(lg_n, cols, threads):
+    """One commit of the workload's shape at 2^lg_n coefficients on the host:
+    LDE by the oracle's CPU restatement (the reference has no CPU NTT), bit
+    reversal, then the reference's own fill_digests_buf_linear_cpu when built
+    (oracle/_ref), else the oracle Merkle.  Returns (seconds, elements, kind)."""
+    from oracle import oracle as O
+    os.environ["OMP_NUM_THREADS"] = str(threads)
+    O.set_threads(threads)
+    c = field_data(99, cols << lg_n)
+    t0 = time.perf_counter()
+    rows = O.lde_rows(c, lg_n, RATE, cols)
+    if O.ref_available():
+        O.ref_merkle(rows, cols, CAP, HASH)
+        kind = "reference"
+    else:
+        O.merkle(rows, cols, CAP, HASH)
+        kind = "port"
+    return time.perf_counter() - t0, (cols << (lg_n + RATE)), kind
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    threads = os.cpu_count() or 1
+    lg = args.cpu_lg
+    for _ in range(args.warmup):
+        cpu_commit_sample(lg, COLS, threads)
+    times, elems, kind = [], 0, "port"
+    for _ in range(args.steps):
+        t, e, kind = cpu_commit_sample(lg, COLS, threads)
+        times.append(t)
+        elems = e
+    total = sum(times)
+    value = elems * len(times) / total
+    sample = ("%d cols x 2^%d coeffs, rate_bits %d (2^%d leaves x %d), Poseidon2 cap %d per step; LDE: CPU restatement "
+              "(the reference has no CPU NTT), Merkle: %s" % (COLS, lg, RATE, lg + RATE, COLS, CAP,
+                                                              "reference fill_digests_buf_linear_cpu" if kind ==
+                                                              "reference" else "oracle port"))
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "elems/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / len(times),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64", "data": "synthetic",
+        "config": config_dict(), "cpu_baseline": {"value": value, "unit": "elems/s", "cores": threads, "kind": kind,
+                                                  "sample": sample},
+        "e2e": {"value": value, "unit": "elems/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def config_dict():
+    return {"workload": "lde_poseidon2_commit: 256 cols x 2^15 coeffs, rate_bits 3 -> 2^18 leaves x 256, "
+                        "Poseidon2 Merkle cap_height 4",
+            "cols": COLS, "lg_n": LG_N, "rate_bits": RATE, "leaves": 1 << (LG_N + RATE), "cap_height": CAP,
+            "hash": "poseidon2", "parallelism": "replicas", "l2": "flushed between steps (256 MiB write)"}
+
+
+def run_ours(args, rank, world):
+    import torch
+    import zeknox_b200 as zk
+
+    dev = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(dev)
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)  # every torch op below is ordered with the commits
+    sptr = stream.cuda_stream
+    n, N = 1 << LG_N, 1 << (LG_N + RATE)
+    elems = N * COLS
+    host = torch.from_numpy(field_data(1000 + rank, COLS * n).view(np.int64).copy())
+    inp = host.to("cuda")
+    host_pinned = host.pin_memory()
+    leaves = torch.empty(N * COLS, dtype=torch.int64, device="cuda")
+    n_dig, n_cap = zk.merkle_sizes(N, CAP)
+    dig = torch.empty(n_dig * 4, dtype=torch.int64, device="cuda")
+    caps = torch.empty(n_cap * 4, dtype=torch.int64, device="cuda")
+    caps_host = torch.empty(n_cap * 4, dtype=torch.int64).pin_memory()
+    job = zk.commit_job(LG_N, RATE, COLS, CAP, HASH, inp, leaves, dig, caps)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+
+    def barrier():
+        if world > 1:
+            torch.distributed.barrier()
+
+    for _ in range(args.warmup):
+        zk.commit(dev, job, stream=sptr)
+    torch.cuda.synchronize()
+
+    # ---- headline: device-resident inputs, one commit per step
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    sampler = ClockSampler(dev)
+    barrier()
+    torch.cuda.synchronize()
+    sampler.start()
+    launches0 = zk.launch_count()
+    for s in range(args.steps):
+        flush.fill_(s & 0xFF)  # evict the previous step's data from L2 (untimed)
+        ev[s][0].record(stream)
+        zk.commit(dev, job, stream=sptr)
+        ev[s][1].record(stream)
+    torch.cuda.synchronize()
+    launches = zk.launch_count() - launches0
+    barrier()
+    clocks = sampler.stop()
+    step_ms = [a.elapsed_time(b) for a, b in ev]
+    total_ms = sum(step_ms)
+    if world > 1:
+        t = torch.tensor([total_ms], device="cuda")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        total_ms = float(t.item())
+    value = elems * world * args.steps / (total_ms * 1e-3)
+
+    # ---- end to end through the public API: pinned host input -> commit -> caps to host
+    ev2 = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    barrier()
+    torch.cuda.synchronize()
+    for s in range(args.steps):
+        flush.fill_(s & 0xFF)
+        ev2[s][0].record(stream)
+        inp.copy_(host_pinned, non_blocking=True)
+        zk.commit(dev, job, stream=sptr)
+        caps_host.copy_(caps, non_blocking=True)
+        ev2[s][1].record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = sum(a.elapsed_time(b) for a, b in ev2)
+    if world > 1:
+        t = torch.tensor([e2e_ms], device="cuda")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    e2e_value = elems * world * args.steps / (e2e_ms * 1e-3)
+
+    # ---- per-stage timing for the rooflines (same stream, same buffers)
+    reps = max(3, args.steps)
+    lde_ms, mk_ms = [], []
+    dstream = torch.cuda.default_stream()
+    for s in range(reps):
+        flush.fill_(s & 0xFF)
+        a, b, c, d = (torch.cuda.Event(enable_timing=True) for _ in range(4))
+        a.record(stream)
+        zk.lde_rows(dev, leaves, inp, LG_N, RATE, COLS, 7, stream=sptr)
+        b.record(stream)
+        torch.cuda.synchronize()
+        # the Merkle entry point queues on the legacy default stream, like the reference
+        c.record(dstream)
+        zk.load().fill_digests_buf_linear_gpu_with_gpu_ptr(zk._ptr(dig), zk._ptr(caps), zk._ptr(leaves), n_dig, n_cap,
+                                                            N, COLS, CAP, HASH, dev)
+        d.record(dstream)
+        torch.cuda.synchronize()
+        lde_ms.append(a.elapsed_time(b))
+        mk_ms.append(c.elapsed_time(d))
+    lde_t = statistics.median(lde_ms) * 1e-3
+    mk_t = statistics.median(mk_ms) * 1e-3
+    hbm, hbm_src = peaks()
+    lde_bytes = 8 * (n + N) * COLS
+    traffic = None
+    try:
+        with open(os.path.join(ROOT, "profiles", "ncu_traffic.json")) as f:
+            traffic = json.load(f).get("lde_rows_config2_bytes_per_call")
+    except Exception:
+        pass
+    roofline = {"bound": "hbm", "kernel": "ntt_pass_kernel x2 (fused coset LDE -> leaf rows)",
+                "achieved": lde_bytes / lde_t / 1e9, "peak": hbm, "unit": "GB/s",
+                "frac": lde_bytes / lde_t / 1e9 / hbm, "traffic": traffic, "peak_source": hbm_src + " hbm_gbs",
+                "algorithmic_bytes": lde_bytes, "ms": lde_t * 1e3}
+    perms = N * ((COLS + 7) // 8) + (N - 1)
+    mul_rate = zk.measure_mul_rate(dev)
+    achieved_mul = perms * P2_MULS_PER_PERM / mk_t
+    roofline_hash = {"bound": "int", "kernel": "merkle_leaf_kernel<Poseidon2> + tail", "achieved": achieved_mul / 1e9,
+                     "peak": mul_rate / 1e9, "unit": "Gmul/s", "frac": achieved_mul / mul_rate if mul_rate > 0 else None,
+                     "perms_per_s": perms / mk_t, "leaves_per_s": N / mk_t, "ms": mk_t * 1e3,
+                     "peak_source": "measured register-loop Goldilocks multiply (zeknox_measure_mul_rate)"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        threads = os.cpu_count() or 1
+        t, e, kind = cpu_commit_sample(args.cpu_lg, COLS, threads)
+        cpu = {"value": e / t, "unit": "elems/s", "cores": threads, "kind": kind,
+               "sample": "one commit of %d cols x 2^%d coeffs (rate 3, Poseidon2 cap 4): LDE by the CPU restatement, "
+                         "Merkle by %s" % (COLS, args.cpu_lg, "the reference's fill_digests_buf_linear_cpu"
+                                           if kind == "reference" else "the oracle port")}
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "elems/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "u64", "data": "synthetic (seeded splitmix64 field elements)",
+            "config": config_dict(), "roofline": roofline, "roofline_hash": roofline_hash, "cpu_baseline": cpu,
+            "e2e": {"value": e2e_value, "unit": "elems/s", "h2d_bytes_per_step": COLS * n * 8,
+                    "d2h_bytes_per_step": n_cap * 32},
+            "gpu_launches": launches, "clocks": clocks,
+            "stage_ms": {"lde_rows": lde_t * 1e3, "merkle": mk_t * 1e3},
+        }
+        print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--cpu-lg", type=int, default=12, help="log2 coefficients per column of the CPU sample")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    args = ap.parse_args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if args.impl == "reference":
+        return run_reference(args, rank, world)
+    if world > 1:
+        import datetime
+
+        import torch
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    try:
+        run_ours(args, rank, world)
+    finally:
+        if world > 1:
+            import torch
+            torch.distributed.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

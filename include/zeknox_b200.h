@@ -1,0 +1,75 @@
+/*
+ * zeknox_b200.h -- entry points this library adds to the zeknox ABI.
+ *
+ * None of these exist in the reference.  They expose the fused commit path
+ * (LDE -> bit-reversed leaf-major rows -> Merkle forest in one call), its
+ * batched multi-job form, and diagnostics.  All pointers in a job are device
+ * pointers on the job's device; sizes are in 64-bit words.
+ */
+#ifndef ZEKNOX_B200_H
+#define ZEKNOX_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#include "utils/rusterror.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Message of the last failure recorded on this host thread by an entry point
+ * that returns void (the fill_digests_* family), or NULL.  The string stays
+ * valid until the next call on the same thread. */
+const char *zeknox_last_error(void);
+
+/* One polynomial-commitment job (Plonky2 PolynomialBatch::from_coeffs /
+ * from_values followed by MerkleTree::new on the LDE rows). */
+typedef struct {
+    uint32_t lg_n;            /* log2 column length before extension (>= 1) */
+    uint32_t rate_bits;       /* blowup 2^rate_bits (>= 1) */
+    uint32_t cols;            /* number of polynomials (columns, >= 1) */
+    uint32_t cap_height;      /* Merkle cap height, <= lg_n + rate_bits */
+    uint32_t hash_type;       /* HashType: 0 Poseidon, 1 Keccak, 3 Poseidon2, 4 Monolith */
+    uint32_t input_is_values; /* 0: columns are coefficients; 1: evaluations on H (inverse NTT first) */
+    uint64_t coset_gen;       /* coset shift; 0 means 7 */
+    const uint64_t *input;    /* cols x 2^lg_n, column-major */
+    uint64_t *leaves;         /* out: 2^(lg_n+rate_bits) rows x cols; row r = evaluation rev(r) */
+    uint64_t *digests;        /* out: 2 * (2^(lg_n+rate_bits) - 2^cap_height) x 4 */
+    uint64_t *caps;           /* out: 2^cap_height x 4 */
+} zk_commit_job;
+
+/* Run one commit on `device_id`, ordered on `stream` (a cudaStream_t; NULL
+ * selects the library's stream for the device).  Returns after queuing the work
+ * when stream is non-NULL, after completion otherwise. */
+RustError zeknox_commit(size_t device_id, const zk_commit_job *job, void *stream);
+
+/* Run `njobs` commits of any sizes as one batch (see DESIGN: batched path):
+ * the whole batch is recorded once as a CUDA graph keyed by its shape and
+ * replayed on later calls with the same shapes.  Synchronous. */
+RustError zeknox_commit_batch(size_t device_id, const zk_commit_job *jobs, uint32_t njobs);
+
+/* Words of temporary device memory zeknox_commit needs for a job (it
+ * allocates them from the stream-ordered pool when called). */
+uint64_t zeknox_commit_scratch_words(const zk_commit_job *job);
+
+/* The LDE stage of a commit alone: rows[r * cols + b] = LDE_b(rev(r)), the
+ * leaf-major bit-reversed matrix (compute_batched_lde + compute_transpose_rev
+ * in one pass structure).  coeffs: cols x 2^lg_n column-major; rows:
+ * 2^(lg_n+rate_bits) x cols.  coset_gen 0 means 7.  Stream semantics as
+ * zeknox_commit. */
+RustError zeknox_lde_rows(size_t device_id, uint64_t *rows, const uint64_t *coeffs, uint32_t lg_n, uint32_t rate_bits,
+                          uint32_t cols, uint64_t coset_gen, void *stream);
+
+/* Number of kernels this library has launched so far in the process. */
+uint64_t zeknox_launch_count(void);
+
+/* Measured register-resident Goldilocks multiplies per second on the device
+ * (the integer roofline the hash kernels are compared against); < 0 on error. */
+double zeknox_measure_mul_rate(size_t device_id);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* ZEKNOX_B200_H */

@@ -1,0 +1,118 @@
+"""Fused commit path (zeknox_commit / zeknox_lde_rows / zeknox_commit_batch)
+vs the oracle: LDE -> bit-reverse transpose -> Merkle forest, bit-exact."""
+import numpy as np
+import pytest
+import torch
+
+import zeknox_b200 as zk
+from oracle import oracle as O
+from tests.helpers import to_dev, to_np
+
+pytestmark = pytest.mark.gpu
+
+
+def alloc_job(lg, rate, cols, cap, h, inp, values=False, gen=7):
+    N = 1 << (lg + rate)
+    leaves = torch.zeros(N * cols, dtype=torch.int64, device="cuda")
+    n_dig, n_cap = zk.merkle_sizes(N, cap)
+    dig = torch.zeros(max(n_dig, 1) * 4, dtype=torch.int64, device="cuda")
+    caps = torch.zeros(n_cap * 4, dtype=torch.int64, device="cuda")
+    job = zk.commit_job(lg, rate, cols, cap, h, inp, leaves, dig, caps, input_is_values=values, coset_gen=gen)
+    return job, (leaves, dig, caps, n_dig)
+
+
+def expect(coeffs, lg, rate, cols, cap, h, gen=7):
+    rows = O.lde_rows(coeffs, lg, rate, cols, coset_gen=gen)
+    d, c = O.merkle(rows, cols, cap, h)
+    return rows, d, c
+
+
+@pytest.mark.parametrize("lg,rate,cols,cap,h", [
+    (1, 1, 1, 0, 3), (2, 2, 3, 1, 0), (4, 3, 16, 2, 3), (6, 1, 17, 0, 4), (9, 3, 8, 4, 1), (10, 2, 33, 3, 3),
+    (12, 1, 5, 12, 0), (13, 3, 20, 4, 3), (14, 2, 64, 16, 3), (15, 3, 24, 4, 3)])
+def test_commit_matches_oracle(lg, rate, cols, cap, h):
+    c = O.field_data(lg * 100 + cols, cols << lg)
+    job, (leaves, dig, caps, n_dig) = alloc_job(lg, rate, cols, cap, h, to_dev(c))
+    zk.commit(0, job)
+    rows, d, cp = expect(c, lg, rate, cols, cap, h)
+    assert np.array_equal(to_np(leaves), rows)
+    assert np.array_equal(to_np(caps).reshape(-1, 4), cp)
+    assert np.array_equal(to_np(dig).reshape(-1, 4)[:n_dig], d)
+
+
+def test_commit_from_values():
+    lg, rate, cols, cap, h = 11, 2, 12, 3, 3
+    vals = O.field_data(5, cols << lg)
+    coeffs = O.batched_ntt(vals, lg, cols, inverse=True)
+    job, (leaves, dig, caps, n_dig) = alloc_job(lg, rate, cols, cap, h, to_dev(vals), values=True)
+    zk.commit(0, job)
+    rows, d, cp = expect(coeffs, lg, rate, cols, cap, h)
+    assert np.array_equal(to_np(leaves), rows)
+    assert np.array_equal(to_np(caps).reshape(-1, 4), cp)
+
+
+@pytest.mark.parametrize("lg,rate,cols", [(3, 1, 1), (8, 3, 16), (12, 2, 40), (16, 1, 3), (17, 3, 2)])
+def test_lde_rows(lg, rate, cols):
+    c = O.field_data(lg + cols, cols << lg)
+    rows = torch.zeros(cols << (lg + rate), dtype=torch.int64, device="cuda")
+    zk.lde_rows(0, rows, to_dev(c), lg, rate, cols)
+    assert np.array_equal(to_np(rows), O.lde_rows(c, lg, rate, cols))
+
+
+def test_batch_matches_single_jobs():
+    shapes = [(10, 1, 8, 2, 0), (12, 3, 20, 4, 3), (9, 2, 64, 1, 4), (11, 3, 3, 0, 1), (13, 1, 17, 5, 3)]
+    jobs, bufs, exps = [], [], []
+    for i, (lg, rate, cols, cap, h) in enumerate(shapes):
+        c = O.field_data(900 + i, cols << lg)
+        inp = to_dev(c)
+        j, b = alloc_job(lg, rate, cols, cap, h, inp)
+        jobs.append(j)
+        bufs.append((inp,) + b)
+        exps.append(expect(c, lg, rate, cols, cap, h))
+    zk.commit_batch(0, jobs)
+    for (inp, leaves, dig, caps, n_dig), (rows, d, cp) in zip(bufs, exps):
+        assert np.array_equal(to_np(leaves), rows)
+        assert np.array_equal(to_np(caps).reshape(-1, 4), cp)
+        assert np.array_equal(to_np(dig).reshape(-1, 4)[:n_dig], d)
+
+
+def test_full_size_workload_properties():
+    """256 columns x 2^15 coefficients, rate 3, Poseidon2, cap height 4 (the
+    benchmark workload): leaf rows spot-checked against Horner evaluation at
+    g * w_N^rev(r), 8 whole columns against the oracle LDE, and the whole
+    forest recomputed by the oracle from the GPU leaves."""
+    lg, rate, cols, cap, h = 15, 3, 256, 4, 3
+    N = 1 << (lg + rate)
+    c = O.field_data(2024, cols << lg)
+    job, (leaves, dig, caps, n_dig) = alloc_job(lg, rate, cols, cap, h, to_dev(c))
+    zk.commit(0, job)
+    rows = to_np(leaves).reshape(N, cols)
+    rng = np.random.default_rng(7)
+    w = O.omega(lg + rate)
+    for _ in range(64):
+        r, b = int(rng.integers(N)), int(rng.integers(cols))
+        i = int(format(r, "018b")[::-1], 2)
+        x = O.mul(7, pow(w, i, O.P))
+        assert int(rows[r, b]) == O.eval_poly(c[b << lg:(b + 1) << lg], x)
+    pick = [0, 1, 77, 128, 200, 253, 254, 255]
+    sub = np.concatenate([c[b << lg:(b + 1) << lg] for b in pick])
+    ev = O.batched_lde(sub, lg, rate, len(pick))
+    for k, b in enumerate(pick):
+        col = ev[k * N:(k + 1) * N]
+        rev = np.array([int(format(r, "018b")[::-1], 2) for r in range(0, N, 997)])
+        assert np.array_equal(rows[::997, b], col[rev])
+    d, cp = O.merkle(to_np(leaves), cols, cap, h)
+    assert np.array_equal(to_np(caps).reshape(-1, 4), cp)
+    assert np.array_equal(to_np(dig).reshape(-1, 4)[:n_dig], d)
+
+
+def test_commit_argument_errors():
+    t = torch.zeros(64, dtype=torch.int64, device="cuda")
+    job, _ = alloc_job(3, 1, 2, 0, 3, t)
+    job.rate_bits = 0
+    with pytest.raises(zk.ZeknoxError):
+        zk.commit(0, job)
+    job.rate_bits = 1
+    job.hash_type = 2
+    with pytest.raises(zk.ZeknoxError):
+        zk.commit(0, job)

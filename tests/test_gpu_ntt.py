@@ -1,0 +1,109 @@
+"""GPU NTT / LDE / transpose through the C ABI vs the oracle; bit-exact."""
+import numpy as np
+import pytest
+import torch
+
+import zeknox_b200 as zk
+from oracle import oracle as O
+from tests.helpers import to_dev, to_np
+
+pytestmark = pytest.mark.gpu
+
+SIZES = [1, 2, 3, 4, 5, 8, 9, 10, 11, 12, 13, 14, 15, 16, 17, 18, 20]
+
+
+@pytest.mark.parametrize("lg", SIZES)
+@pytest.mark.parametrize("inverse", [False, True])
+@pytest.mark.parametrize("coset", [False, True])
+def test_ntt_device(lg, inverse, coset):
+    batches = 3 if lg <= 16 else 1
+    x = O.field_data(lg * 7 + inverse, batches << lg)
+    t = to_dev(x)
+    zk.ntt_batch(0, t, lg, batches, with_coset=coset, inverse=inverse)
+    exp = O.batched_ntt(x, lg, batches, inverse=inverse, with_coset=coset)
+    assert np.array_equal(to_np(t), exp)
+
+
+@pytest.mark.parametrize("lg", [4, 12, 17])
+def test_ntt_host_buffers(lg):
+    x = O.field_data(lg, 2 << lg)
+    t = torch.from_numpy(x.view(np.int64).copy())
+    zk.ntt_batch(0, t, lg, 2)
+    assert np.array_equal(t.numpy().view(np.uint64), O.batched_ntt(x, lg, 2))
+    zk.intt_batch(0, t, lg, 2)
+    assert np.array_equal(t.numpy().view(np.uint64), x)
+
+
+@pytest.mark.parametrize("lg,rate,batches", [(1, 1, 2), (2, 3, 5), (4, 1, 2), (9, 3, 3), (10, 2, 7), (12, 1, 2),
+                                             (13, 3, 4), (15, 3, 2), (17, 3, 1), (18, 1, 2)])
+@pytest.mark.parametrize("coset", [True, False])
+def test_lde_device(lg, rate, batches, coset):
+    c = O.field_data(lg * 13 + rate, batches << lg)
+    out = torch.zeros(batches << (lg + rate), dtype=torch.int64, device="cuda")
+    zk.lde_batch(0, out, to_dev(c), lg, batches, rate, with_coset=coset)
+    assert np.array_equal(to_np(out), O.batched_lde(c, lg, rate, batches, with_coset=coset))
+
+
+@pytest.mark.parametrize("lg,rate", [(3, 1), (10, 2), (14, 1)])
+def test_lde_inverse_direction(lg, rate):
+    c = O.field_data(lg, 2 << lg)
+    out = torch.zeros(2 << (lg + rate), dtype=torch.int64, device="cuda")
+    zk.lde_batch(0, out, to_dev(c), lg, 2, rate, with_coset=True, inverse=True)
+    assert np.array_equal(to_np(out), O.batched_lde(c, lg, rate, 2, inverse=True, with_coset=True))
+
+
+def test_lde_host_buffers_and_salt():
+    lg, rate, b, salt = 11, 2, 3, 2
+    c = O.field_data(5, b << lg)
+    out = torch.zeros((b + salt) << (lg + rate), dtype=torch.int64)
+    zk.lde_batch(0, out, torch.from_numpy(c.view(np.int64).copy()), lg, b, rate, salt_size=salt)
+    got = out.numpy().view(np.uint64)
+    N = 1 << (lg + rate)
+    assert np.array_equal(got[:b * N], O.batched_lde(c, lg, rate, b))
+    s = got[b * N:]
+    assert (s < np.uint64(O.P)).all() and len(np.unique(s)) > 0.99 * s.size
+
+
+def test_custom_coset_generator():
+    lg, rate = 8, 2
+    zk.init_coset(0, lg + rate, 11)
+    try:
+        c = O.field_data(9, 2 << lg)
+        out = torch.zeros(2 << (lg + rate), dtype=torch.int64, device="cuda")
+        zk.lde_batch(0, out, to_dev(c), lg, 2, rate, with_coset=True)
+        assert np.array_equal(to_np(out), O.batched_lde(c, lg, rate, 2, coset_gen=11))
+        t = to_dev(c)
+        zk.ntt_batch(0, t, lg, 2, with_coset=True)
+        assert np.array_equal(to_np(t), O.batched_ntt(c, lg, 2, with_coset=True, coset_gen=11))
+    finally:
+        zk.init_coset(0, 20, 7)
+
+
+@pytest.mark.parametrize("lg,b", [(0, 3), (1, 1), (5, 3), (10, 33), (12, 256), (17, 7), (20, 2)])
+def test_transpose_rev(lg, b):
+    x = O.field_data(lg + b, b << lg)
+    out = torch.zeros(b << lg, dtype=torch.int64, device="cuda")
+    zk.transpose_rev_batch(0, out, to_dev(x), lg, b)
+    assert np.array_equal(to_np(out), O.transpose_rev(x, lg, b))
+    out2 = torch.zeros(b << lg, dtype=torch.int64, device="cuda")
+    zk.transpose_rev_batch(0, out2, to_dev(x), lg, b, naive=True)
+    assert torch.equal(out, out2)
+
+
+def test_argument_errors():
+    t = torch.zeros(16, dtype=torch.int64, device="cuda")
+    with pytest.raises(zk.ZeknoxError) as e:
+        zk.ntt_batch(0, t, 0, 1)
+    assert e.value.code == 1
+    with pytest.raises(zk.ZeknoxError) as e:
+        zk.lde_batch(0, t, t, 2, 1, 0)
+    assert e.value.code == 1
+    with pytest.raises(zk.ZeknoxError):
+        zk.ntt_batch(99, t, 2, 1)
+
+
+def test_init_entry_points():
+    assert zk.cuda_available()
+    assert zk.get_number_of_gpus() >= 1
+    zk.init_twiddle_factors(0, 16)
+    zk.init_cuda_degree(20)

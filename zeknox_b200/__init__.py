@@ -1,0 +1,334 @@
+"""zeknox_b200 -- B200-native Goldilocks commit path behind zeknox's C ABI.
+
+The computation lives in ``libzeknox.so`` (CUDA, sm_100a; built by
+``make -C zeknox_b200`` or ``__graft_entry__.build()``).  This module is the
+Python host side: it loads the library, declares the C entry points with
+ctypes, and offers the same operations as zeknox's Rust wrapper
+(wrappers/rust/src/lib.rs: ``lde_batch``, ``ntt_batch``, ``intt_batch``,
+``transpose_rev_batch``, ``init_*``) plus the Merkle builders of
+native/merkle/merkle.h and this library's fused commit extension.
+
+Buffers are torch tensors of dtype int64 (bit patterns of u64 field
+elements) or uint64; CUDA tensors are passed as device pointers, CPU tensors as
+host pointers.  There is no CPU fallback: every GPU entry point fails loudly
+(``ZeknoxError`` / ``OSError``) when the CUDA library or a GPU is missing.
+"""
+import ctypes
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libzeknox.so")
+
+P = 0xFFFFFFFF00000001
+HASH_POSEIDON, HASH_KECCAK, HASH_POSEIDON_BN128, HASH_POSEIDON2, HASH_MONOLITH = 0, 1, 2, 3, 4
+FORWARD, INVERSE = 0, 1
+
+# Exported C symbols (include/lib.h, include/merkle/merkle.h, include/zeknox_b200.h).
+ABI_SYMBOLS = [
+    "get_number_of_gpus", "list_devices_info", "init_cuda", "init_cuda_degree", "init_cuda_degree_and_generator",
+    "init_twiddle_factors", "init_coset", "compute_batched_ntt", "compute_batched_lde",
+    "compute_batched_lde_multi_gpu", "compute_transpose_rev", "compute_naive_transpose_rev",
+    "fill_digests_buf_linear_gpu_with_gpu_ptr", "fill_digests_buf_linear_multigpu_with_gpu_ptr",
+    "fill_digests_buf_linear_cpu", "cuda_available",
+]
+EXT_SYMBOLS = ["zeknox_last_error", "zeknox_commit", "zeknox_commit_batch", "zeknox_commit_scratch_words",
+               "zeknox_lde_rows", "zeknox_launch_count", "zeknox_measure_mul_rate"]
+
+
+class RustError(ctypes.Structure):
+    """native/utils/rusterror.h: {int code; char *message} returned by value."""
+    _fields_ = [("code", ctypes.c_int), ("message", ctypes.c_void_p)]
+
+
+class NTTConfig(ctypes.Structure):
+    """native/ntt/ntt.h NTT_Config (24 bytes)."""
+    _fields_ = [
+        ("batches", ctypes.c_uint32),
+        ("order", ctypes.c_int),
+        ("ntt_type", ctypes.c_int),
+        ("extension_rate_bits", ctypes.c_uint32),
+        ("are_inputs_on_device", ctypes.c_bool),
+        ("are_outputs_on_device", ctypes.c_bool),
+        ("with_coset", ctypes.c_bool),
+        ("is_multi_gpu", ctypes.c_bool),
+        ("salt_size", ctypes.c_uint32),
+    ]
+
+
+class TransposeConfig(ctypes.Structure):
+    """native/ntt/ntt.h NTT_TransposeConfig (8 bytes)."""
+    _fields_ = [
+        ("batches", ctypes.c_uint32),
+        ("are_inputs_on_device", ctypes.c_bool),
+        ("are_outputs_on_device", ctypes.c_bool),
+    ]
+
+
+class CommitJob(ctypes.Structure):
+    """include/zeknox_b200.h zk_commit_job."""
+    _fields_ = [
+        ("lg_n", ctypes.c_uint32),
+        ("rate_bits", ctypes.c_uint32),
+        ("cols", ctypes.c_uint32),
+        ("cap_height", ctypes.c_uint32),
+        ("hash_type", ctypes.c_uint32),
+        ("input_is_values", ctypes.c_uint32),
+        ("coset_gen", ctypes.c_uint64),
+        ("input", ctypes.c_void_p),
+        ("leaves", ctypes.c_void_p),
+        ("digests", ctypes.c_void_p),
+        ("caps", ctypes.c_void_p),
+    ]
+
+
+class ZeknoxError(RuntimeError):
+    def __init__(self, code, message):
+        super().__init__("zeknox error %d: %s" % (code, message))
+        self.code = code
+
+
+_lib = None
+_libc = ctypes.CDLL(None)
+_libc.free.argtypes = [ctypes.c_void_p]
+
+
+def load():
+    """Load libzeknox.so (raises OSError when it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise OSError("libzeknox.so not built: run `make -C %s` (or __graft_entry__.build())" % HERE)
+    L = ctypes.CDLL(LIB_PATH)
+    sz, u32, u64, vp = ctypes.c_size_t, ctypes.c_uint32, ctypes.c_uint64, ctypes.c_void_p
+    L.get_number_of_gpus.restype = RustError
+    L.get_number_of_gpus.argtypes = [ctypes.POINTER(sz)]
+    L.list_devices_info.restype = RustError
+    L.init_cuda.restype = None
+    L.init_cuda_degree.argtypes = [u32]
+    L.init_cuda_degree.restype = None
+    L.init_cuda_degree_and_generator.argtypes = [u32, u64]
+    L.init_cuda_degree_and_generator.restype = None
+    L.init_twiddle_factors.restype = RustError
+    L.init_twiddle_factors.argtypes = [sz, sz]
+    L.init_coset.restype = RustError
+    L.init_coset.argtypes = [sz, sz, u64]
+    L.compute_batched_ntt.restype = RustError
+    L.compute_batched_ntt.argtypes = [sz, vp, u32, ctypes.c_int, NTTConfig]
+    L.compute_batched_lde.restype = RustError
+    L.compute_batched_lde.argtypes = [sz, vp, vp, u32, ctypes.c_int, NTTConfig]
+    L.compute_batched_lde_multi_gpu.restype = RustError
+    L.compute_batched_lde_multi_gpu.argtypes = [vp, vp, u32, ctypes.c_int, NTTConfig, u32, sz, sz]
+    for f in (L.compute_transpose_rev, L.compute_naive_transpose_rev):
+        f.restype = RustError
+        f.argtypes = [sz, vp, vp, u32, TransposeConfig]
+    L.fill_digests_buf_linear_gpu_with_gpu_ptr.restype = None
+    L.fill_digests_buf_linear_gpu_with_gpu_ptr.argtypes = [vp, vp, vp] + [u64] * 7
+    L.fill_digests_buf_linear_multigpu_with_gpu_ptr.restype = None
+    L.fill_digests_buf_linear_multigpu_with_gpu_ptr.argtypes = [vp, vp, vp] + [u64] * 6
+    L.fill_digests_buf_linear_cpu.restype = None
+    L.fill_digests_buf_linear_cpu.argtypes = [vp, vp, vp] + [u64] * 6
+    L.cuda_available.restype = ctypes.c_bool
+    L.zeknox_last_error.restype = ctypes.c_char_p
+    L.zeknox_commit.restype = RustError
+    L.zeknox_commit.argtypes = [sz, ctypes.POINTER(CommitJob), vp]
+    L.zeknox_commit_batch.restype = RustError
+    L.zeknox_commit_batch.argtypes = [sz, ctypes.POINTER(CommitJob), u32]
+    L.zeknox_commit_scratch_words.restype = u64
+    L.zeknox_commit_scratch_words.argtypes = [ctypes.POINTER(CommitJob)]
+    L.zeknox_lde_rows.restype = RustError
+    L.zeknox_lde_rows.argtypes = [sz, vp, vp, u32, u32, u32, u64, vp]
+    L.zeknox_launch_count.restype = u64
+    L.zeknox_measure_mul_rate.restype = ctypes.c_double
+    L.zeknox_measure_mul_rate.argtypes = [sz]
+    _lib = L
+    return L
+
+
+def _check(err):
+    if err.code != 0:
+        msg = ctypes.string_at(err.message).decode() if err.message else ""
+        if err.message:
+            _libc.free(err.message)
+        raise ZeknoxError(err.code, msg)
+
+
+def last_error():
+    m = load().zeknox_last_error()
+    return m.decode() if m else None
+
+
+def _ptr(t):
+    if t is None:
+        return None
+    assert t.is_contiguous(), "buffers must be contiguous"
+    return ctypes.c_void_p(t.data_ptr())
+
+
+# ---------------------------------------------------------------- device info
+
+def get_number_of_gpus():
+    n = ctypes.c_size_t(0)
+    _check(load().get_number_of_gpus(ctypes.byref(n)))
+    return n.value
+
+
+def cuda_available():
+    return bool(load().cuda_available())
+
+
+def list_devices_info():
+    _check(load().list_devices_info())
+
+
+def init_twiddle_factors(device_id, lg_n):
+    _check(load().init_twiddle_factors(device_id, lg_n))
+
+
+def init_coset(device_id, lg_n, coset_gen=7):
+    _check(load().init_coset(device_id, lg_n, coset_gen))
+
+
+def init_cuda():
+    load().init_cuda()
+
+
+def init_cuda_degree(max_degree):
+    load().init_cuda_degree(max_degree)
+
+
+# ---------------------------------------------------------------- transforms
+
+def ntt_config(batches=1, rate_bits=0, inputs_on_device=False, outputs_on_device=False, with_coset=False,
+               salt_size=0):
+    c = NTTConfig()
+    c.batches = batches
+    c.order = 0
+    c.ntt_type = 0
+    c.extension_rate_bits = rate_bits
+    c.are_inputs_on_device = inputs_on_device
+    c.are_outputs_on_device = outputs_on_device
+    c.with_coset = with_coset
+    c.is_multi_gpu = False
+    c.salt_size = salt_size
+    return c
+
+
+def ntt_batch(device_id, inout, lg_n, batches, with_coset=False, inverse=False):
+    """compute_batched_ntt on a (batches, 2^lg_n) tensor, in place (host or device)."""
+    on_dev = inout.is_cuda
+    cfg = ntt_config(batches, 0, on_dev, on_dev, with_coset)
+    _check(load().compute_batched_ntt(device_id, _ptr(inout), lg_n, INVERSE if inverse else FORWARD, cfg))
+    return inout
+
+
+def intt_batch(device_id, inout, lg_n, batches, with_coset=False):
+    return ntt_batch(device_id, inout, lg_n, batches, with_coset, inverse=True)
+
+
+def lde_batch(device_id, output, inp, lg_n, batches, rate_bits, with_coset=True, inverse=False, salt_size=0):
+    """compute_batched_lde: (batches, 2^lg_n) coefficients -> (batches+salt, 2^(lg_n+rate)) evaluations."""
+    cfg = ntt_config(batches, rate_bits, inp.is_cuda, output.is_cuda, with_coset, salt_size)
+    _check(load().compute_batched_lde(device_id, _ptr(output), _ptr(inp), lg_n, INVERSE if inverse else FORWARD, cfg))
+    return output
+
+
+def lde_batch_multi_gpu(output, inp, num_gpu, lg_n, batches, rate_bits, with_coset=True):
+    cfg = ntt_config(batches, rate_bits, False, True, with_coset)
+    n_in = batches << lg_n
+    n_out = batches << (lg_n + rate_bits)
+    _check(load().compute_batched_lde_multi_gpu(_ptr(output), _ptr(inp), num_gpu, FORWARD, cfg, lg_n, n_in, n_out))
+    return output
+
+
+def transpose_rev_batch(device_id, output, inp, lg_n, batches, naive=False):
+    cfg = TransposeConfig()
+    cfg.batches = batches
+    cfg.are_inputs_on_device = inp.is_cuda
+    cfg.are_outputs_on_device = output.is_cuda
+    f = load().compute_naive_transpose_rev if naive else load().compute_transpose_rev
+    _check(f(device_id, _ptr(output), _ptr(inp), lg_n, cfg))
+    return output
+
+
+# -------------------------------------------------------------------- Merkle
+
+def merkle_sizes(n_leaves, cap_height):
+    n_caps = 1 << cap_height
+    return 2 * (n_leaves - n_caps), n_caps
+
+
+def fill_digests_buf_linear_gpu(digests, caps, leaves, n_leaves, leaf_size, cap_height, hash_type, gpu_id=0):
+    """fill_digests_buf_linear_gpu_with_gpu_ptr; raises ZeknoxError on a rejected call."""
+    n_dig, n_caps = merkle_sizes(n_leaves, cap_height)
+    L = load()
+    L.zeknox_last_error  # noqa: B018  (symbol presence)
+    before = last_error()
+    L.fill_digests_buf_linear_gpu_with_gpu_ptr(_ptr(digests), _ptr(caps), _ptr(leaves), n_dig, n_caps, n_leaves,
+                                               leaf_size, cap_height, hash_type, gpu_id)
+    after = last_error()
+    if after is not None and after != before:
+        raise ZeknoxError(1, after)
+
+
+def fill_digests_buf_linear_multigpu(digests, caps, leaves, n_leaves, leaf_size, cap_height, hash_type):
+    n_dig, n_caps = merkle_sizes(n_leaves, cap_height)
+    before = last_error()
+    load().fill_digests_buf_linear_multigpu_with_gpu_ptr(_ptr(digests), _ptr(caps), _ptr(leaves), n_dig, n_caps,
+                                                         n_leaves, leaf_size, cap_height, hash_type)
+    after = last_error()
+    if after is not None and after != before:
+        raise ZeknoxError(1, after)
+
+
+def fill_digests_buf_linear_cpu(digests, caps, leaves, n_leaves, leaf_size, cap_height, hash_type):
+    n_dig, n_caps = merkle_sizes(n_leaves, cap_height)
+    before = last_error()
+    load().fill_digests_buf_linear_cpu(_ptr(digests), _ptr(caps), _ptr(leaves), n_dig, n_caps, n_leaves, leaf_size,
+                                       cap_height, hash_type)
+    after = last_error()
+    if after is not None and after != before:
+        raise ZeknoxError(1, after)
+
+
+# ------------------------------------------------------------------- commits
+
+def commit_job(lg_n, rate_bits, cols, cap_height, hash_type, inp, leaves, digests, caps, input_is_values=False,
+               coset_gen=7):
+    j = CommitJob()
+    j.lg_n, j.rate_bits, j.cols, j.cap_height, j.hash_type = lg_n, rate_bits, cols, cap_height, hash_type
+    j.input_is_values = int(bool(input_is_values))
+    j.coset_gen = coset_gen
+    j.input, j.leaves = inp.data_ptr(), leaves.data_ptr()
+    j.digests = digests.data_ptr() if digests is not None and digests.numel() else None
+    j.caps = caps.data_ptr()
+    return j
+
+
+def commit(device_id, job, stream=None):
+    """zeknox_commit: LDE -> bit-reversed leaf rows -> Merkle forest for one job."""
+    _check(load().zeknox_commit(device_id, ctypes.byref(job), ctypes.c_void_p(stream) if stream else None))
+
+
+def commit_batch(device_id, jobs):
+    arr = (CommitJob * len(jobs))(*jobs)
+    _check(load().zeknox_commit_batch(device_id, arr, len(jobs)))
+
+
+def commit_scratch_words(job):
+    return load().zeknox_commit_scratch_words(ctypes.byref(job))
+
+
+def lde_rows(device_id, rows, coeffs, lg_n, rate_bits, cols, coset_gen=7, stream=None):
+    """zeknox_lde_rows: coefficient columns -> bit-reversed leaf-major LDE matrix."""
+    _check(load().zeknox_lde_rows(device_id, _ptr(rows), _ptr(coeffs), lg_n, rate_bits, cols, coset_gen,
+                                  ctypes.c_void_p(stream) if stream else None))
+    return rows
+
+
+def launch_count():
+    return load().zeknox_launch_count()
+
+
+def measure_mul_rate(device_id=0):
+    return load().zeknox_measure_mul_rate(device_id)

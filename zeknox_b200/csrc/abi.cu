@@ -1,0 +1,535 @@
+// abi.cu -- the exported C entry points (include/lib.h, include/merkle/merkle.h,
+// include/zeknox_b200.h).
+//
+// Argument checks, host<->device staging and error codes follow zeknox
+// native/lib.cu and native/ntt/ntt.cu; the computation is in ntt.cu/merkle.cu.
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include <string>
+
+#include "../../include/lib.h"
+#include "../../include/zeknox_b200.h"
+#include "gl64.cuh"
+#include "ntt_api.cuh"
+#include "runtime.cuh"
+#include "zk_constants.h"
+
+bool zk_merkle_cpu(void *digests, void *caps, const void *leaves, uint64_t n_dig, uint64_t n_cap, uint64_t n_leaves,
+                   uint64_t leaf_size, uint64_t cap_height, uint64_t hash_type, std::string &err);
+
+namespace {
+
+thread_local std::string g_last_error;
+
+RustError ok() { return RustError{0, nullptr}; }
+
+RustError fail(int code, const std::string &msg)
+{
+    RustError e;
+    e.code = code;
+    e.message = msg.empty() ? nullptr : strdup(msg.c_str());
+    return e;
+}
+
+template <class F>
+RustError guarded(F &&f)
+{
+    try {
+        f();
+        return ok();
+    } catch (const zk::arg_failure &e) {
+        return fail(e.code, e.what());
+    } catch (const zk::cuda_failure &e) {
+        return fail(e.code, e.what());
+    } catch (const std::bad_alloc &) {
+        return fail(-(int)cudaErrorMemoryAllocation, "host allocation failed");
+    } catch (const std::exception &e) {
+        return fail(-(int)cudaErrorUnknown, e.what());
+    }
+}
+
+void record_error(const char *fn, const std::string &msg)
+{
+    g_last_error = std::string(fn) + ": " + msg;
+    fprintf(stderr, "zeknox: %s\n", g_last_error.c_str());
+}
+
+// Device copy of `elems` words at `p`: the pointer itself when on_device,
+// otherwise a temporary filled from host memory (synchronously ordered on the
+// device stream).
+struct Staged {
+    zk::DevBuf buf;
+    uint64_t *dev = nullptr;
+    Staged(zk::DeviceCtx &c, void *p, uint64_t elems, bool on_device, bool copy_in)
+    {
+        if (on_device) {
+            dev = (uint64_t *)p;
+        } else {
+            buf.ctx = &c;
+            buf.p = elems ? c.alloc(elems * 8) : nullptr;
+            dev = buf.p;
+            if (copy_in && elems) ZK_CUDA(cudaMemcpyAsync(dev, p, elems * 8, cudaMemcpyHostToDevice, c.stream));
+        }
+    }
+};
+
+}  // namespace
+
+// ------------------------------------------------------------------ devices
+
+extern "C" RustError get_number_of_gpus(size_t *ngpus)
+{
+    return guarded([&] {
+        if (!ngpus) throw zk::arg_failure("null pointer");
+        *ngpus = (size_t)zk::device_count();
+    });
+}
+
+extern "C" RustError list_devices_info(void)
+{
+    return guarded([&] {
+        int n = zk::device_count();
+        for (int d = 0; d < n; d++) {
+            cudaDeviceProp p;
+            ZK_CUDA(cudaGetDeviceProperties(&p, d));
+            printf("GPU %d: %s, sm_%d%d, %d SMs, %.1f GiB, L2 %d MiB, smem/block opt-in %zu KiB\n", d, p.name, p.major,
+                   p.minor, p.multiProcessorCount, p.totalGlobalMem / 1073741824.0, p.l2CacheSize >> 20,
+                   p.sharedMemPerBlockOptin >> 10);
+            for (int q = 0; q < n; q++) {
+                if (q == d) continue;
+                int can = 0;
+                ZK_CUDA(cudaDeviceCanAccessPeer(&can, d, q));
+                printf("  peer %d -> %d: %s\n", d, q, can ? "yes" : "no");
+            }
+        }
+    });
+}
+
+extern "C" bool cuda_available(void) { return zk::device_count() > 0; }
+
+// ------------------------------------------------------------------- tables
+
+extern "C" RustError init_twiddle_factors(size_t device_id, size_t lg_n)
+{
+    return guarded([&] {
+        if (lg_n > 32) throw zk::arg_failure("lg_n above 32");
+        zk::DeviceCtx &c = zk::device(device_id);
+        std::lock_guard<std::recursive_mutex> lk(c.mu);
+        c.twiddles((uint32_t)lg_n, false);
+        c.twiddles((uint32_t)lg_n, true);
+        c.sync();
+    });
+}
+
+extern "C" RustError init_coset(size_t device_id, size_t lg_n, const uint64_t coset_gen)
+{
+    return guarded([&] {
+        if (lg_n > 32) throw zk::arg_failure("lg_n above 32");
+        zk::DeviceCtx &c = zk::device(device_id);
+        std::lock_guard<std::recursive_mutex> lk(c.mu);
+        c.set_coset((uint32_t)lg_n, coset_gen);
+        c.sync();
+    });
+}
+
+extern "C" void init_cuda_degree_and_generator(const uint32_t max_degree, const uint64_t group_generator)
+{
+    RustError e = guarded([&] {
+        int n = zk::device_count();
+        for (int d = 0; d < n; d++) {
+            zk::DeviceCtx &c = zk::device(d);
+            std::lock_guard<std::recursive_mutex> lk(c.mu);
+            c.set_coset(max_degree, group_generator);
+            for (uint32_t k = 1; k <= 12 && k <= max_degree; k++) {
+                c.twiddles(k, false);
+                c.twiddles(k, true);
+            }
+            c.sync();
+        }
+    });
+    if (e.code) {
+        record_error("init_cuda_degree_and_generator", e.message ? e.message : "error");
+        free(e.message);
+    }
+}
+
+extern "C" void init_cuda_degree(const uint32_t max_degree) { init_cuda_degree_and_generator(max_degree, ZK_GENERATOR); }
+
+extern "C" void init_cuda(void) { init_cuda_degree(24); }
+
+// --------------------------------------------------------------- transforms
+
+extern "C" RustError compute_batched_ntt(size_t device_id, void *inout, uint32_t lg_domain_size,
+                                         NTT_Direction ntt_direction, NTT_Config cfg)
+{
+    if (lg_domain_size == 0) return fail((int)cudaErrorInvalidValue, "lg_domain_size must be >= 1");
+    return guarded([&] {
+        if (lg_domain_size > 32) throw zk::arg_failure("lg_domain_size above 32");
+        if (cfg.are_inputs_on_device != cfg.are_outputs_on_device)
+            throw zk::arg_failure("in-place transform needs matching input/output placement");
+        if (!inout && cfg.batches) throw zk::arg_failure("null buffer");
+        zk::DeviceCtx &c = zk::device(device_id);
+        std::lock_guard<std::recursive_mutex> lk(c.mu);
+        const uint64_t total = (uint64_t)cfg.batches << lg_domain_size;
+        Staged s(c, inout, total, cfg.are_inputs_on_device, true);
+        zk::ntt_batch_device(c, s.dev, lg_domain_size, cfg.batches, ntt_direction == inverse, cfg.with_coset);
+        if (!cfg.are_outputs_on_device && total)
+            ZK_CUDA(cudaMemcpyAsync(inout, s.dev, total * 8, cudaMemcpyDeviceToHost, c.stream));
+        c.sync();
+    });
+}
+
+static void lde_on(zk::DeviceCtx &c, void *output, void *input, uint32_t lg_n, NTT_Direction dir, const NTT_Config &cfg)
+{
+    const uint64_t n = 1ULL << lg_n;
+    const uint32_t rate = cfg.extension_rate_bits;
+    const uint64_t N = n << rate;
+    const uint64_t in_total = n * cfg.batches;
+    const uint64_t out_total = N * ((uint64_t)cfg.batches + cfg.salt_size);
+    Staged si(c, input, in_total, cfg.are_inputs_on_device, true);
+    Staged so(c, output, out_total, cfg.are_outputs_on_device, false);
+    zk::lde_batch_device(c, so.dev, si.dev, lg_n, rate, cfg.batches, dir == inverse, cfg.with_coset);
+    if (cfg.salt_size) zk::salt_device(c, so.dev + N * cfg.batches, N * cfg.salt_size);
+    if (!cfg.are_outputs_on_device && out_total)
+        ZK_CUDA(cudaMemcpyAsync(output, so.dev, out_total * 8, cudaMemcpyDeviceToHost, c.stream));
+    c.sync();
+}
+
+extern "C" RustError compute_batched_lde(size_t device_id, void *output, void *input, uint32_t lg_domain_size,
+                                         NTT_Direction ntt_direction, NTT_Config cfg)
+{
+    if (lg_domain_size == 0 || cfg.extension_rate_bits < 1) return fail((int)cudaErrorInvalidValue, "invalid args");
+    return guarded([&] {
+        if (lg_domain_size + cfg.extension_rate_bits > 32) throw zk::arg_failure("extended size above 2^32");
+        if ((!input && cfg.batches) || (!output && (cfg.batches + cfg.salt_size))) throw zk::arg_failure("null buffer");
+        zk::DeviceCtx &c = zk::device(device_id);
+        std::lock_guard<std::recursive_mutex> lk(c.mu);
+        lde_on(c, output, input, lg_domain_size, ntt_direction, cfg);
+    });
+}
+
+extern "C" RustError compute_batched_lde_multi_gpu(void *output, void *input, uint32_t num_gpu,
+                                                   NTT_Direction ntt_direction, NTT_Config cfg,
+                                                   uint32_t lg_domain_size, size_t total_num_input_elements,
+                                                   size_t total_num_output_elements)
+{
+    if (total_num_input_elements == 0 || lg_domain_size == 0 || cfg.extension_rate_bits < 1)
+        return fail((int)cudaErrorInvalidValue, "invalid args");
+    return guarded([&] {
+        const uint32_t rate = cfg.extension_rate_bits;
+        if (lg_domain_size + rate > 32) throw zk::arg_failure("extended size above 2^32");
+        const uint64_t n = 1ULL << lg_domain_size, N = n << rate;
+        if (total_num_input_elements < n * cfg.batches || total_num_output_elements < N * cfg.batches)
+            throw zk::arg_failure("element counts smaller than batches x size");
+        int ngpu = zk::device_count();
+        uint32_t G = num_gpu == 0 ? 1 : num_gpu;
+        if ((int)G > ngpu) throw zk::arg_failure("num_gpu exceeds the GPUs present");
+        // columns split as in the reference: the first (batches % G) GPUs take one more
+        std::vector<uint64_t> take(G), first(G);
+        uint64_t acc = 0;
+        for (uint32_t g = 0; g < G; g++) {
+            take[g] = cfg.batches / G + (g < cfg.batches % G ? 1 : 0);
+            first[g] = acc;
+            acc += take[g];
+        }
+        NTT_Config sub = cfg;
+        sub.are_inputs_on_device = false;  // host input (ntt.cu:360-364)
+        sub.are_outputs_on_device = true;
+        sub.salt_size = 0;
+        for (uint32_t g = 0; g < G; g++) {
+            if (!take[g]) continue;
+            zk::DeviceCtx &c = zk::device(g);
+            std::lock_guard<std::recursive_mutex> lk(c.mu);
+            sub.batches = (uint32_t)take[g];
+            uint64_t *dst = (uint64_t *)output + first[g] * N;
+            if (g == 0) {
+                lde_on(c, dst, (uint64_t *)input + first[g] * n, lg_domain_size, ntt_direction, sub);
+            } else {
+                // compute on GPU g, then copy into GPU 0's output buffer
+                zk::DevBuf tmp(c, take[g] * N);
+                lde_on(c, tmp.p, (uint64_t *)input + first[g] * n, lg_domain_size, ntt_direction, sub);
+                ZK_CUDA(cudaMemcpyPeerAsync(dst, 0, tmp.p, g, take[g] * N * 8, c.stream));
+                c.sync();
+            }
+        }
+    });
+}
+
+static RustError transpose_impl(size_t device_id, void *output, void *input, uint32_t lg_n, NTT_TransposeConfig cfg)
+{
+    return guarded([&] {
+        if (lg_n > 32) throw zk::arg_failure("lg_n above 32");
+        if (cfg.batches && (!input || !output)) throw zk::arg_failure("null buffer");
+        zk::DeviceCtx &c = zk::device(device_id);
+        std::lock_guard<std::recursive_mutex> lk(c.mu);
+        const uint64_t total = (uint64_t)cfg.batches << lg_n;
+        Staged si(c, input, total, cfg.are_inputs_on_device, true);
+        Staged so(c, output, total, cfg.are_outputs_on_device, false);
+        zk::transpose_rev_device(c, so.dev, si.dev, lg_n, cfg.batches);
+        if (!cfg.are_outputs_on_device && total)
+            ZK_CUDA(cudaMemcpyAsync(output, so.dev, total * 8, cudaMemcpyDeviceToHost, c.stream));
+        c.sync();
+    });
+}
+
+extern "C" RustError compute_transpose_rev(size_t device_id, void *output, void *input, uint32_t lg_n,
+                                           NTT_TransposeConfig cfg)
+{
+    return transpose_impl(device_id, output, input, lg_n, cfg);
+}
+
+extern "C" RustError compute_naive_transpose_rev(size_t device_id, void *output, void *input, uint32_t lg_n,
+                                                 NTT_TransposeConfig cfg)
+{
+    return transpose_impl(device_id, output, input, lg_n, cfg);
+}
+
+// ------------------------------------------------------------------- Merkle
+
+extern "C" void fill_digests_buf_linear_gpu_with_gpu_ptr(void *digests_buf_gpu_ptr, void *cap_buf_gpu_ptr,
+                                                         void *leaves_buf_gpu_ptr, u64 digests_buf_size,
+                                                         u64 cap_buf_size, u64 leaves_buf_size, u64 leaf_size,
+                                                         u64 cap_height, u64 hash_type, u64 gpu_id)
+{
+    (void)gpu_id;  // the reference ignores it too: pointers are on the current device
+    std::string err;
+    if (!zk::merkle_device((uint64_t *)digests_buf_gpu_ptr, (uint64_t *)cap_buf_gpu_ptr,
+                           (const uint64_t *)leaves_buf_gpu_ptr, digests_buf_size, cap_buf_size, leaves_buf_size,
+                           leaf_size, cap_height, hash_type, cudaStreamLegacy, err))
+        record_error("fill_digests_buf_linear_gpu_with_gpu_ptr", err);
+}
+
+extern "C" void fill_digests_buf_linear_multigpu_with_gpu_ptr(void *digests_buf_gpu_ptr, void *cap_buf_gpu_ptr,
+                                                              void *leaves_buf_gpu_ptr, u64 digests_buf_size,
+                                                              u64 cap_buf_size, u64 leaves_buf_size, u64 leaf_size,
+                                                              u64 cap_height, u64 hash_type)
+{
+    std::string err;
+    if (!zk::merkle_geometry_ok(digests_buf_size, cap_buf_size, leaves_buf_size, cap_height, err)) {
+        record_error("fill_digests_buf_linear_multigpu_with_gpu_ptr", err);
+        return;
+    }
+    RustError e = guarded([&] {
+        int ngpu = zk::device_count();
+        // largest power of two of GPUs that divides the caps: each GPU builds a
+        // contiguous run of whole subtrees (merkle.cu:381-438 does one per GPU)
+        uint64_t G = 1;
+        while (G * 2 <= (uint64_t)ngpu && G * 2 <= cap_buf_size) G *= 2;
+        const uint64_t L = leaves_buf_size / cap_buf_size, D = 2 * L - 2;
+        const uint64_t caps_g = cap_buf_size / G;
+        uint32_t hg = 0;
+        while ((1ULL << hg) < caps_g) hg++;
+        if (G == 1) {
+            zk::DeviceCtx &c = zk::device(0);
+            std::lock_guard<std::recursive_mutex> lk(c.mu);
+            std::string e2;
+            if (!zk::merkle_device((uint64_t *)digests_buf_gpu_ptr, (uint64_t *)cap_buf_gpu_ptr,
+                                   (const uint64_t *)leaves_buf_gpu_ptr, digests_buf_size, cap_buf_size,
+                                   leaves_buf_size, leaf_size, cap_height, hash_type, c.stream, e2))
+                throw zk::arg_failure(e2);
+            c.sync();
+            return;
+        }
+        for (uint64_t g = 0; g < G; g++) {
+            zk::DeviceCtx &c = zk::device(g);
+            std::lock_guard<std::recursive_mutex> lk(c.mu);
+            const uint64_t leaves_g = caps_g * L, dig_g = caps_g * D;
+            const uint64_t *src_leaves = (const uint64_t *)leaves_buf_gpu_ptr + g * leaves_g * leaf_size;
+            uint64_t *dst_dig = (uint64_t *)digests_buf_gpu_ptr + g * dig_g * 4;
+            uint64_t *dst_cap = (uint64_t *)cap_buf_gpu_ptr + g * caps_g * 4;
+            zk::DevBuf lv(c, g ? leaves_g * leaf_size : 0), dg(c, g ? dig_g * 4 : 0), cp(c, g ? caps_g * 4 : 0);
+            const uint64_t *use_leaves = src_leaves;
+            uint64_t *use_dig = dst_dig, *use_cap = dst_cap;
+            if (g) {
+                // remote data lands in this GPU's memory before any kernel reads it
+                ZK_CUDA(cudaMemcpyPeerAsync(lv.p, (int)g, src_leaves, 0, leaves_g * leaf_size * 8, c.stream));
+                use_leaves = lv.p;
+                use_dig = dg.p;
+                use_cap = cp.p;
+            }
+            std::string e2;
+            if (!zk::merkle_device(use_dig, use_cap, use_leaves, dig_g, caps_g, leaves_g, leaf_size, hg, hash_type,
+                                   c.stream, e2))
+                throw zk::arg_failure(e2);
+            if (g) {
+                ZK_CUDA(cudaMemcpyPeerAsync(dst_dig, 0, dg.p, (int)g, dig_g * 32, c.stream));
+                ZK_CUDA(cudaMemcpyPeerAsync(dst_cap, 0, cp.p, (int)g, caps_g * 32, c.stream));
+            }
+            c.sync();
+        }
+    });
+    if (e.code) {
+        record_error("fill_digests_buf_linear_multigpu_with_gpu_ptr", e.message ? e.message : "error");
+        free(e.message);
+    }
+}
+
+extern "C" void fill_digests_buf_linear_cpu(void *digests_buf_ptr, void *cap_buf_ptr, const void *leaves_buf_ptr,
+                                            u64 digests_buf_size, u64 cap_buf_size, u64 leaves_buf_size, u64 leaf_size,
+                                            u64 cap_height, u64 hash_type)
+{
+    std::string err;
+    if (!digests_buf_ptr || !cap_buf_ptr || !leaves_buf_ptr) {
+        record_error("fill_digests_buf_linear_cpu", "null pointer");
+        return;
+    }
+    if (!zk_merkle_cpu(digests_buf_ptr, cap_buf_ptr, leaves_buf_ptr, digests_buf_size, cap_buf_size, leaves_buf_size,
+                       leaf_size, cap_height, hash_type, err))
+        record_error("fill_digests_buf_linear_cpu", err);
+}
+
+// -------------------------------------------------------------- extensions
+
+extern "C" const char *zeknox_last_error(void) { return g_last_error.empty() ? nullptr : g_last_error.c_str(); }
+
+static void check_job(const zk_commit_job &j)
+{
+    if (j.lg_n == 0 || j.rate_bits == 0 || j.cols == 0) throw zk::arg_failure("lg_n, rate_bits and cols must be >= 1");
+    if (j.lg_n + j.rate_bits > 32) throw zk::arg_failure("extended size above 2^32");
+    if (j.cap_height > j.lg_n + j.rate_bits) throw zk::arg_failure("cap_height above log2 of the leaf count");
+    if (!j.input || !j.leaves || !j.caps || (!j.digests && j.cap_height < j.lg_n + j.rate_bits))
+        throw zk::arg_failure("null buffer");
+    if (j.hash_type != 0 && j.hash_type != 1 && j.hash_type != 3 && j.hash_type != 4)
+        throw zk::arg_failure("unsupported hash_type");
+}
+
+extern "C" uint64_t zeknox_commit_scratch_words(const zk_commit_job *job)
+{
+    if (!job) return 0;
+    uint64_t n = 1ULL << job->lg_n;
+    uint64_t w = zk::lde_rows_scratch_elems(job->lg_n, job->rate_bits, job->cols);
+    if (job->input_is_values) w += 2 * n * job->cols;
+    return w;
+}
+
+static void commit_on(zk::DeviceCtx &c, const zk_commit_job &j, cudaStream_t s)
+{
+    const uint64_t n = 1ULL << j.lg_n;
+    const uint64_t N = n << j.rate_bits;
+    const uint64_t gen = j.coset_gen ? j.coset_gen : ZK_GENERATOR;
+    cudaStream_t keep = c.stream;
+    c.stream = s;  // run the whole job on the caller's stream
+    try {
+        const uint64_t *coeffs = j.input;
+        zk::DevBuf cf;
+        if (j.input_is_values) {
+            cf.ctx = &c;
+            cf.p = c.alloc(n * j.cols * 8);
+            ZK_CUDA(cudaMemcpyAsync(cf.p, j.input, n * j.cols * 8, cudaMemcpyDeviceToDevice, s));
+            zk::ntt_batch_device(c, cf.p, j.lg_n, j.cols, true, false);
+            coeffs = cf.p;
+        }
+        zk::lde_rows_device(c, j.leaves, coeffs, j.lg_n, j.rate_bits, j.cols, gen, nullptr);
+        std::string err;
+        const uint64_t n_caps = 1ULL << j.cap_height;
+        if (!zk::merkle_device(j.digests, j.caps, j.leaves, 2 * (N - n_caps), n_caps, N, j.cols, j.cap_height,
+                               j.hash_type, s, err))
+            throw zk::arg_failure(err);
+    } catch (...) {
+        c.stream = keep;
+        throw;
+    }
+    c.stream = keep;
+}
+
+extern "C" RustError zeknox_commit(size_t device_id, const zk_commit_job *job, void *stream)
+{
+    return guarded([&] {
+        if (!job) throw zk::arg_failure("null job");
+        check_job(*job);
+        zk::DeviceCtx &c = zk::device(device_id);
+        std::lock_guard<std::recursive_mutex> lk(c.mu);
+        cudaStream_t s = stream ? (cudaStream_t)stream : c.stream;
+        commit_on(c, *job, s);
+        if (!stream) c.sync();
+    });
+}
+
+extern "C" RustError zeknox_commit_batch(size_t device_id, const zk_commit_job *jobs, uint32_t njobs)
+{
+    return guarded([&] {
+        if (njobs && !jobs) throw zk::arg_failure("null jobs");
+        for (uint32_t i = 0; i < njobs; i++) check_job(jobs[i]);
+        zk::DeviceCtx &c = zk::device(device_id);
+        std::lock_guard<std::recursive_mutex> lk(c.mu);
+        for (uint32_t i = 0; i < njobs; i++) commit_on(c, jobs[i], c.stream);
+        c.sync();
+    });
+}
+
+// ------------------------------------------------------------- diagnostics
+
+extern "C" uint64_t zeknox_launch_count(void) { return zk::launch_count(); }
+
+extern "C" RustError zeknox_lde_rows(size_t device_id, uint64_t *rows, const uint64_t *coeffs, uint32_t lg_n,
+                                     uint32_t rate_bits, uint32_t cols, uint64_t coset_gen, void *stream)
+{
+    return guarded([&] {
+        if (lg_n == 0 || rate_bits == 0 || cols == 0) throw zk::arg_failure("lg_n, rate_bits and cols must be >= 1");
+        if (lg_n + rate_bits > 32) throw zk::arg_failure("extended size above 2^32");
+        if (!rows || !coeffs) throw zk::arg_failure("null buffer");
+        zk::DeviceCtx &c = zk::device(device_id);
+        std::lock_guard<std::recursive_mutex> lk(c.mu);
+        cudaStream_t keep = c.stream;
+        if (stream) c.stream = (cudaStream_t)stream;
+        try {
+            zk::lde_rows_device(c, rows, coeffs, lg_n, rate_bits, cols, coset_gen ? coset_gen : ZK_GENERATOR, nullptr);
+        } catch (...) {
+            c.stream = keep;
+            throw;
+        }
+        c.stream = keep;
+        if (!stream) c.sync();
+    });
+}
+
+// Register-resident Goldilocks multiply throughput: every thread runs 8
+// independent chains x <- x * y of `iters` multiplies.
+__global__ void mul_rate_kernel(uint64_t *out, uint64_t seed, uint32_t iters)
+{
+    uint64_t x[8], y[8];
+#pragma unroll
+    for (int i = 0; i < 8; i++) {
+        x[i] = (seed + threadIdx.x * 8 + i) * 0x9E3779B97F4A7C15ULL % zk::GL_P;
+        y[i] = (seed ^ (blockIdx.x * 131 + i)) * 0xBF58476D1CE4E5B9ULL % zk::GL_P;
+    }
+    for (uint32_t k = 0; k < iters; k++) {
+#pragma unroll
+        for (int i = 0; i < 8; i++) x[i] = zk::gl_mul(x[i], y[i]);
+    }
+    uint64_t acc = 0;
+#pragma unroll
+    for (int i = 0; i < 8; i++) acc ^= x[i];
+    out[blockIdx.x * blockDim.x + threadIdx.x] = acc;
+}
+
+extern "C" double zeknox_measure_mul_rate(size_t device_id)
+{
+    double rate = -1;
+    RustError e = guarded([&] {
+        zk::DeviceCtx &c = zk::device(device_id);
+        std::lock_guard<std::recursive_mutex> lk(c.mu);
+        const int blocks = c.sm_count * 8, threads = 256;
+        const uint32_t iters = 4096;
+        zk::DevBuf out(c, (size_t)blocks * threads);
+        cudaEvent_t a, b;
+        ZK_CUDA(cudaEventCreate(&a));
+        ZK_CUDA(cudaEventCreate(&b));
+        mul_rate_kernel<<<blocks, threads, 0, c.stream>>>(out.p, 1, 64);  // warm-up
+        ZK_CUDA(cudaEventRecord(a, c.stream));
+        mul_rate_kernel<<<blocks, threads, 0, c.stream>>>(out.p, 2, iters);
+        ZK_CUDA(cudaEventRecord(b, c.stream));
+        ZK_CUDA(cudaEventSynchronize(b));
+        float ms = 0;
+        ZK_CUDA(cudaEventElapsedTime(&ms, a, b));
+        cudaEventDestroy(a);
+        cudaEventDestroy(b);
+        rate = (double)blocks * threads * 8.0 * iters / (ms * 1e-3);
+    });
+    if (e.code) free(e.message);
+    return rate;
+}

@@ -1,0 +1,148 @@
+// gl64.cuh -- Goldilocks field arithmetic, p = 2^64 - 2^32 + 1.
+//
+// Replaces native/ff/gl64_t.cuh (device) and native/ff/goldilocks.hpp (host)
+// of zeknox.  Written from the field's structure:
+//     2^64 = 2^32 - 1 =: EPS (mod p)        2^96 = -1 (mod p)
+// so a 128-bit value  lo + 2^64 (h0 + 2^32 h1)  reduces to  lo + EPS*h0 - h1.
+// 2 has multiplicative order 192, so multiplying by 2^s is a shift followed by
+// that reduction; every 64th root of unity is a power of 2.
+//
+// All functions take and return canonical values (< p) unless their name says
+// otherwise.  They compile for host and device; the device path uses the
+// 64x64->128 multiply-high intrinsic, the host path unsigned __int128.
+#pragma once
+#include <stdint.h>
+
+#ifdef __CUDACC__
+#define ZK_HD __host__ __device__ __forceinline__
+#else
+#define ZK_HD inline
+#endif
+
+namespace zk {
+
+static constexpr uint64_t GL_P = 0xFFFFFFFF00000001ULL;
+static constexpr uint64_t GL_EPS = 0xFFFFFFFFULL;  // 2^64 mod p
+
+ZK_HD uint64_t mulhi64(uint64_t a, uint64_t b)
+{
+#ifdef __CUDA_ARCH__
+    return __umul64hi(a, b);
+#else
+    return (uint64_t)(((unsigned __int128)a * b) >> 64);
+#endif
+}
+
+// a + b for canonical a, b.  If the 64-bit sum wraps, the true sum minus p is
+// sum + EPS (no second wrap); otherwise subtract p when sum >= p, which is
+// exactly when sum + EPS wraps.
+ZK_HD uint64_t gl_add(uint64_t a, uint64_t b)
+{
+    uint64_t s = a + b;
+    uint64_t t = s + GL_EPS;
+    bool c1 = s < a;
+    bool c2 = t < s;
+    return (c1 | c2) ? t : s;
+}
+
+// a - b for canonical a, b: a borrow means a - b + 2^64, fix by subtracting EPS.
+ZK_HD uint64_t gl_sub(uint64_t a, uint64_t b)
+{
+    uint64_t d = a - b;
+    return (a < b) ? d - GL_EPS : d;
+}
+
+ZK_HD uint64_t gl_neg(uint64_t a) { return a ? GL_P - a : 0; }
+
+ZK_HD uint64_t gl_canon(uint64_t a) { return a >= GL_P ? a - GL_P : a; }
+
+// Reduce lo + 2^64*hi (any 128-bit value) to a canonical element.
+ZK_HD uint64_t gl_reduce128(uint64_t lo, uint64_t hi)
+{
+    uint64_t h1 = hi >> 32;
+    uint64_t h0 = hi & GL_EPS;
+    uint64_t t0 = lo - h1;
+    if (lo < h1) t0 -= GL_EPS;                  // lo - h1 + p, already < p
+    uint64_t t1 = (h0 << 32) - h0;              // h0 * EPS < p
+    uint64_t t2 = t0 + t1;
+    if (t2 < t1) t2 += GL_EPS;                  // wrapped: t0 + t1 - p < 2^64
+    return gl_canon(t2);
+}
+
+// Reduce lo + 2^64*hi with hi < 2^32 (a "u96" value).
+ZK_HD uint64_t gl_reduce96(uint64_t lo, uint64_t hi)
+{
+    uint64_t t1 = (hi << 32) - hi;              // hi * EPS
+    uint64_t t2 = lo + t1;
+    if (t2 < t1) t2 += GL_EPS;
+    return gl_canon(t2);
+}
+
+ZK_HD uint64_t gl_mul(uint64_t a, uint64_t b) { return gl_reduce128(a * b, mulhi64(a, b)); }
+
+ZK_HD uint64_t gl_sqr(uint64_t a) { return gl_mul(a, a); }
+
+// a * 2^s for 0 <= s < 64: the 128-bit shift then the special reduction.
+ZK_HD uint64_t gl_mul_pow2_lt64(uint64_t a, unsigned s)
+{
+    if (s == 0) return a;
+    return gl_reduce128(a << s, a >> (64 - s));
+}
+
+// a * 2^s for any s (taken mod 192, the order of 2).  2^96 = -1 turns
+// s >= 96 into a negation; for 64 <= s < 96, 2^s = 2^(s-32) - 2^(s-64)
+// because 2^64 = 2^32 - 1.
+ZK_HD uint64_t gl_mul_pow2(uint64_t a, unsigned s)
+{
+    s %= 192;
+    bool neg = s >= 96;
+    if (neg) s -= 96;
+    uint64_t r = s < 64 ? gl_mul_pow2_lt64(a, s) : gl_sub(gl_mul_pow2_lt64(a, s - 32), gl_mul_pow2_lt64(a, s - 64));
+    return neg ? gl_neg(r) : r;
+}
+
+ZK_HD uint64_t gl_pow(uint64_t a, uint64_t e)
+{
+    uint64_t r = 1;
+    while (e) {
+        if (e & 1) r = gl_mul(r, a);
+        a = gl_mul(a, a);
+        e >>= 1;
+    }
+    return r;
+}
+
+ZK_HD uint64_t gl_inv(uint64_t a) { return gl_pow(a, GL_P - 2); }
+
+// x^7, the Poseidon/Poseidon2 S-box: x^2, x^4, x^3 = x^2 * x, x^7 = x^3 * x^4.
+ZK_HD uint64_t gl_sbox7(uint64_t x)
+{
+    uint64_t x2 = gl_sqr(x);
+    uint64_t x4 = gl_sqr(x2);
+    uint64_t x3 = gl_mul(x2, x);
+    return gl_mul(x3, x4);
+}
+
+ZK_HD uint32_t bitrev32(uint32_t x, unsigned bits)
+{
+#ifdef __CUDA_ARCH__
+    return bits ? __brev(x) >> (32 - bits) : 0;
+#else
+    uint32_t r = 0;
+    for (unsigned i = 0; i < bits; i++) r |= ((x >> i) & 1u) << (bits - 1 - i);
+    return r;
+#endif
+}
+
+ZK_HD uint64_t bitrev64(uint64_t x, unsigned bits)
+{
+#ifdef __CUDA_ARCH__
+    return bits ? __brevll(x) >> (64 - bits) : 0;
+#else
+    uint64_t r = 0;
+    for (unsigned i = 0; i < bits; i++) r |= ((x >> i) & 1ULL) << (bits - 1 - i);
+    return r;
+#endif
+}
+
+}  // namespace zk

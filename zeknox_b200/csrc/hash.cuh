@@ -1,0 +1,438 @@
+// hash.cuh -- width-12 Goldilocks permutations and the Plonky2 sponge.
+//
+// Replaces zeknox's native/poseidon (Plonky2 Poseidon), native/poseidon2,
+// native/monolith and native/keccak hashers.  State is 12 uint64_t in
+// registers; every loop is fully unrolled so round constants become
+// constant-bank operands (device) or immediates.  The same code runs on the
+// host (for the exported CPU Merkle builder) and on the device.
+#pragma once
+#include <stdint.h>
+#include <string.h>
+
+#include "gl64.cuh"
+#include "zk_constants.h"
+
+namespace zk {
+
+enum HashKind : int { HASH_POSEIDON = 0, HASH_KECCAK = 1, HASH_POSEIDON_BN128 = 2, HASH_POSEIDON2 = 3, HASH_MONOLITH = 4 };
+
+#ifdef __CUDA_ARCH__
+#define ZKC(name) d_##name
+#else
+#define ZKC(name) h_##name
+#endif
+
+#ifdef __CUDACC__
+#define ZK_CONST_TABLE(type, name, n, list) \
+    static __constant__ type d_##name[n] = {list}; \
+    static const type h_##name[n] = {list};
+#else
+#define ZK_CONST_TABLE(type, name, n, list) static const type h_##name[n] = {list};
+#endif
+
+ZK_CONST_TABLE(uint64_t, POSEIDON_RC, 360, ZK_POSEIDON_RC_LIST)
+ZK_CONST_TABLE(uint64_t, POSEIDON2_RC, 360, ZK_POSEIDON2_RC_LIST)
+ZK_CONST_TABLE(uint64_t, POSEIDON2_DIAG, 12, ZK_POSEIDON2_DIAG_LIST)
+ZK_CONST_TABLE(uint64_t, MONOLITH_RC, 84, ZK_MONOLITH_RC_LIST)
+ZK_CONST_TABLE(uint64_t, KECCAK_RNDC, 24, ZK_KECCAK_RNDC_LIST)
+
+// Small circulant rows and the Keccak lane tables are compile-time constants
+// (folded into the code once the loops are unrolled).
+#ifdef __CUDACC__
+#define ZK_CX __host__ __device__ constexpr
+#else
+#define ZK_CX constexpr
+#endif
+ZK_CX uint32_t poseidon_circ(int i)
+{
+    constexpr uint32_t c[12] = {ZK_POSEIDON_CIRC_LIST};
+    return c[i];
+}
+ZK_CX uint32_t monolith_circ(int i)
+{
+    constexpr uint32_t c[12] = {ZK_MONOLITH_CIRC_LIST};
+    return c[i];
+}
+ZK_CX int keccak_rot(int t)
+{
+    constexpr int r[24] = {ZK_KECCAK_ROTC_LIST};
+    return r[t];
+}
+ZK_CX int keccak_pi(int t)
+{
+    constexpr int p[24] = {ZK_KECCAK_PILN_LIST};
+    return p[t];
+}
+
+// ------------------------------------------------------------- small dot product
+//
+// sum_i x_i * c_i with x_i < 2^64 and small c_i, accumulated exactly as two
+// 64-bit sums over the 32-bit halves of x (each < 2^32 * 12 * 64 < 2^42), then
+// recombined into a < 2^80 value and reduced once.
+struct Acc96 {
+    uint64_t lo, hi;  // sum of low halves * c, sum of high halves * c
+    ZK_HD void zero() { lo = hi = 0; }
+    ZK_HD void mac(uint64_t x, uint32_t c)
+    {
+        lo += (x & 0xFFFFFFFFULL) * c;
+        hi += (x >> 32) * c;
+    }
+    ZK_HD void add(uint64_t x) { lo += x & 0xFFFFFFFFULL; hi += x >> 32; }
+    ZK_HD uint64_t reduce() const
+    {
+        uint64_t l = lo + (hi << 32);
+        uint64_t h = (hi >> 32) + (l < lo);
+        return gl_reduce96(l, h);
+    }
+};
+
+// ----------------------------------------------------------------- Poseidon
+//
+// Plonky2 Poseidon in the round-by-round ("naive") form of
+// native/poseidon/poseidon.cu:771-780 / poseidon.cpp:94-105: 4 full rounds,
+// 22 partial rounds (S-box on lane 0 only), 4 full rounds; each round adds the
+// 12 round constants of that round, applies the S-box layer, then the MDS
+// matrix circ(17,15,41,16,2,28,13,13,39,18,34,20) + diag(8,0,...).
+ZK_HD void poseidon_mds(uint64_t s[12])
+{
+    uint64_t t[12];
+#pragma unroll
+    for (int r = 0; r < 12; r++) {
+        Acc96 a;
+        a.zero();
+#pragma unroll
+        for (int i = 0; i < 12; i++) a.mac(s[(i + r) % 12], poseidon_circ(i));
+        if (r == 0) a.mac(s[0], ZK_POSEIDON_DIAG0);
+        t[r] = a.reduce();
+    }
+#pragma unroll
+    for (int i = 0; i < 12; i++) s[i] = t[i];
+}
+
+ZK_HD void poseidon_permute(uint64_t s[12])
+{
+#pragma unroll
+    for (int r = 0; r < 4; r++) {
+#pragma unroll
+        for (int i = 0; i < 12; i++) s[i] = gl_sbox7(gl_add(s[i], ZKC(POSEIDON_RC)[12 * r + i]));
+        poseidon_mds(s);
+    }
+#pragma unroll 2
+    for (int r = 4; r < 26; r++) {
+        s[0] = gl_sbox7(gl_add(s[0], ZKC(POSEIDON_RC)[12 * r]));
+#pragma unroll
+        for (int i = 1; i < 12; i++) s[i] = gl_add(s[i], ZKC(POSEIDON_RC)[12 * r + i]);
+        poseidon_mds(s);
+    }
+#pragma unroll
+    for (int r = 26; r < 30; r++) {
+#pragma unroll
+        for (int i = 0; i < 12; i++) s[i] = gl_sbox7(gl_add(s[i], ZKC(POSEIDON_RC)[12 * r + i]));
+        poseidon_mds(s);
+    }
+}
+
+// ----------------------------------------------------------------- Poseidon2
+//
+// native/poseidon2/poseidon2.cu:65-209.  External layer: the 4x4 block
+// M4 = [[5,7,1,3],[4,6,1,1],[1,3,5,7],[1,1,4,6]] on each of the three lane
+// groups, then every lane adds the sum of its column across the groups -- so
+// lane 4g+k ends as  sum_j (1 + [g'==g]) * (M4 x_g')_k.  Internal layer:
+// s_i <- s_i * diag_i + sum(s).
+ZK_HD void p2_external(uint64_t s[12])
+{
+    // M4 rows expanded; each output is a small-coefficient combination, so
+    // accumulate the whole layer exactly and reduce once per lane.
+    uint64_t y[12];
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+        // coefficient of x_{4g'+j} in lane 4g+k: M4[k][j] * (1 + [g'==g])
+        constexpr uint32_t M4[4][4] = {{5, 7, 1, 3}, {4, 6, 1, 1}, {1, 3, 5, 7}, {1, 1, 4, 6}};
+        Acc96 col;
+        col.zero();
+#pragma unroll
+        for (int g = 0; g < 3; g++)
+#pragma unroll
+            for (int j = 0; j < 4; j++) col.mac(s[4 * g + j], M4[k][j]);
+#pragma unroll
+        for (int g = 0; g < 3; g++) {
+            Acc96 a = col;
+#pragma unroll
+            for (int j = 0; j < 4; j++) a.mac(s[4 * g + j], M4[k][j]);
+            y[4 * g + k] = a.reduce();
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < 12; i++) s[i] = y[i];
+}
+
+ZK_HD void poseidon2_permute(uint64_t s[12])
+{
+    p2_external(s);
+#pragma unroll
+    for (int r = 0; r < 4; r++) {
+#pragma unroll
+        for (int i = 0; i < 12; i++) s[i] = gl_sbox7(gl_add(s[i], ZKC(POSEIDON2_RC)[12 * r + i]));
+        p2_external(s);
+    }
+#pragma unroll 2
+    for (int r = 4; r < 26; r++) {
+        s[0] = gl_sbox7(gl_add(s[0], ZKC(POSEIDON2_RC)[12 * r]));
+        uint64_t sum = s[0];
+#pragma unroll
+        for (int i = 1; i < 12; i++) sum = gl_add(sum, s[i]);
+        // s_i * d_i + sum as one 128-bit value, reduced once
+#pragma unroll
+        for (int i = 0; i < 12; i++) {
+            uint64_t d = ZKC(POSEIDON2_DIAG)[i];
+            uint64_t lo = s[i] * d, hi = mulhi64(s[i], d);
+            lo += sum;
+            hi += lo < sum;
+            s[i] = gl_reduce128(lo, hi);
+        }
+    }
+#pragma unroll
+    for (int r = 26; r < 30; r++) {
+#pragma unroll
+        for (int i = 0; i < 12; i++) s[i] = gl_sbox7(gl_add(s[i], ZKC(POSEIDON2_RC)[12 * r + i]));
+        p2_external(s);
+    }
+}
+
+// ----------------------------------------------------------------- Monolith
+//
+// Monolith-64 (native/monolith/monolith.cu:114-236): Concrete with round
+// constants row 0, then 6 x [Bars on lanes 0..3, Bricks, Concrete(row r)].
+//   Bar (per byte b):  rotl1(b ^ (rotl1(~b) & rotl2(b) & rotl3(b)))
+//   Bricks: s_i += s_{i-1}^2 for i = 11..1 (old values), with the 65th bit kept
+//   Concrete: circulant product of the 65-bit lanes plus the round constant.
+ZK_HD uint64_t mono_bar(uint64_t x)
+{
+    const uint64_t H1 = 0x8080808080808080ULL, L7 = 0x7F7F7F7F7F7F7F7FULL;
+    const uint64_t H2 = 0xC0C0C0C0C0C0C0C0ULL, L6 = 0x3F3F3F3F3F3F3F3FULL;
+    const uint64_t H3 = 0xE0E0E0E0E0E0E0E0ULL, L5 = 0x1F1F1F1F1F1F1F1FULL;
+    uint64_t nx = ~x;
+    uint64_t r1 = ((nx & H1) >> 7) | ((nx & L7) << 1);
+    uint64_t r2 = ((x & H2) >> 6) | ((x & L6) << 2);
+    uint64_t r3 = ((x & H3) >> 5) | ((x & L5) << 3);
+    uint64_t t = x ^ (r1 & r2 & r3);
+    return ((t & H1) >> 7) | ((t & L7) << 1);
+}
+
+ZK_HD void mono_concrete(uint64_t s[12], const uint32_t hi[12], int round)
+{
+    uint64_t t[12];
+#pragma unroll
+    for (int r = 0; r < 12; r++) {
+        Acc96 a;
+        a.zero();
+        uint64_t top = 0;
+#pragma unroll
+        for (int c = 0; c < 12; c++) {
+            a.mac(s[c], monolith_circ((c - r + 12) % 12));
+            top += (uint64_t)hi[c] * monolith_circ((c - r + 12) % 12);
+        }
+        a.add(ZKC(MONOLITH_RC)[12 * round + r]);
+        // value = lo + 2^32*hi + 2^64*top
+        uint64_t l = a.lo + (a.hi << 32);
+        uint64_t h = (a.hi >> 32) + (l < a.lo) + top;
+        t[r] = gl_reduce96(l, h);
+    }
+#pragma unroll
+    for (int i = 0; i < 12; i++) s[i] = t[i];
+}
+
+ZK_HD void monolith_permute(uint64_t s[12])
+{
+    uint32_t hi[12];
+#pragma unroll
+    for (int i = 0; i < 12; i++) hi[i] = 0;
+    mono_concrete(s, hi, 0);
+#pragma unroll 1
+    for (int r = 1; r <= 6; r++) {
+#pragma unroll
+        for (int i = 0; i < 4; i++) s[i] = mono_bar(s[i]);
+        uint64_t sq[11];
+#pragma unroll
+        for (int i = 0; i < 11; i++) sq[i] = gl_sqr(gl_canon(s[i]));
+        hi[0] = 0;
+#pragma unroll
+        for (int i = 1; i < 12; i++) {
+            uint64_t v = s[i] + sq[i - 1];
+            hi[i] = v < sq[i - 1];
+            s[i] = v;
+        }
+        mono_concrete(s, hi, r);
+    }
+}
+
+// ------------------------------------------------------------------- Keccak
+//
+// Keccak-f[1600] (Keccak reference; zeknox uses Saarinen's formulation,
+// native/keccak/keccak.cu:42-79), 24 rounds over 25 lanes.
+ZK_HD uint64_t rotl64(uint64_t x, int k) { return k == 0 ? x : (x << k) | (x >> (64 - k)); }
+
+ZK_HD void keccak_f(uint64_t st[25])
+{
+#pragma unroll 1
+    for (int round = 0; round < 24; round++) {
+        uint64_t c[5];
+#pragma unroll
+        for (int x = 0; x < 5; x++) c[x] = st[x] ^ st[x + 5] ^ st[x + 10] ^ st[x + 15] ^ st[x + 20];
+#pragma unroll
+        for (int x = 0; x < 5; x++) {
+            uint64_t d = c[(x + 4) % 5] ^ rotl64(c[(x + 1) % 5], 1);
+#pragma unroll
+            for (int y = 0; y < 25; y += 5) st[y + x] ^= d;
+        }
+        uint64_t cur = st[1];
+#pragma unroll
+        for (int t = 0; t < 24; t++) {
+            int j = keccak_pi(t);
+            uint64_t nxt = st[j];
+            st[j] = rotl64(cur, keccak_rot(t));
+            cur = nxt;
+        }
+#pragma unroll
+        for (int y = 0; y < 25; y += 5) {
+            uint64_t r0 = st[y], r1 = st[y + 1], r2 = st[y + 2], r3 = st[y + 3], r4 = st[y + 4];
+            st[y] = r0 ^ (~r1 & r2);
+            st[y + 1] = r1 ^ (~r2 & r3);
+            st[y + 2] = r2 ^ (~r3 & r4);
+            st[y + 3] = r3 ^ (~r4 & r0);
+            st[y + 4] = r4 ^ (~r0 & r1);
+        }
+        st[0] ^= ZKC(KECCAK_RNDC)[round];
+    }
+}
+
+// ------------------------------------------------------------------ sponges
+
+template <int H>
+ZK_HD void permute(uint64_t s[12])
+{
+    if (H == HASH_POSEIDON) poseidon_permute(s);
+    else if (H == HASH_POSEIDON2) poseidon2_permute(s);
+    else monolith_permute(s);
+}
+
+// Plonky2 overwrite-mode sponge over a strided element source (element i at
+// src[i * stride]); rate 8, capacity 4, zero initial state.  Inputs of <= 4
+// elements are the digest themselves, zero padded
+// (native/poseidon/poseidon_permutation.cuh:84-120).
+template <int H>
+ZK_HD void sponge_hash_one(const uint64_t *src, uint64_t len, uint64_t out[4])
+{
+    if (len <= 4) {
+#pragma unroll
+        for (int i = 0; i < 4; i++) out[i] = (uint64_t)i < len ? src[i] : 0;
+        return;
+    }
+    uint64_t s[12];
+#pragma unroll
+    for (int i = 0; i < 12; i++) s[i] = 0;
+    for (uint64_t idx = 0; idx < len; idx += 8) {
+        uint64_t k = len - idx;
+        if (k >= 8) {
+#pragma unroll
+            for (int i = 0; i < 8; i++) s[i] = src[idx + i];
+        } else {
+            // last partial chunk overwrites only its k < 8 lanes
+#pragma unroll
+            for (int i = 0; i < 8; i++)
+                if ((uint64_t)i < k) s[i] = src[idx + i];
+        }
+        permute<H>(s);
+    }
+#pragma unroll
+    for (int i = 0; i < 4; i++) out[i] = gl_canon(s[i]);
+}
+
+template <int H>
+ZK_HD void sponge_hash_two(const uint64_t l[4], const uint64_t r[4], uint64_t out[4])
+{
+    uint64_t s[12];
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+        s[i] = l[i];
+        s[4 + i] = r[i];
+        s[8 + i] = 0;
+    }
+    permute<H>(s);
+#pragma unroll
+    for (int i = 0; i < 4; i++) out[i] = gl_canon(s[i]);
+}
+
+// Keccak-256 (rate 136 bytes, 0x01 ... 0x80 padding) of len 8-byte words, the
+// 32-byte digest with limb 3 truncated to one byte (native/keccak/keccak.cu:116-124).
+// Fewer than 4 words are copied through (the remaining limbs are not written).
+ZK_HD void keccak_hash_one(const uint64_t *src, uint64_t len, uint64_t out[4])
+{
+    if (len < 4) {
+#pragma unroll
+        for (int i = 0; i < 3; i++)
+            if ((uint64_t)i < len) out[i] = src[i];
+        return;
+    }
+    uint64_t st[25];
+#pragma unroll
+    for (int i = 0; i < 25; i++) st[i] = 0;
+    uint64_t idx = 0;
+    for (; len - idx >= 17; idx += 17) {
+#pragma unroll
+        for (int i = 0; i < 17; i++) st[i] ^= src[idx + i];
+        keccak_f(st);
+    }
+    uint64_t rem = len - idx;
+    // tail words, then the pad byte 0x01 right after the message and 0x80 into
+    // the last byte of the 136-byte block
+#pragma unroll
+    for (int i = 0; i < 17; i++) {
+        if ((uint64_t)i < rem) st[i] ^= src[idx + i];
+        if ((uint64_t)i == rem) st[i] ^= 0x01ULL;
+    }
+    st[16] ^= 0x8000000000000000ULL;
+    keccak_f(st);
+    out[0] = st[0];
+    out[1] = st[1];
+    out[2] = st[2];
+    out[3] = st[3] & 0xFF;
+}
+
+// Keccak-256 of 25 bytes of l followed by 25 bytes of r (native/keccak/keccak.cu:126-135).
+ZK_HD void keccak_hash_two(const uint64_t l[4], const uint64_t r[4], uint64_t out[4])
+{
+    uint64_t st[25];
+#pragma unroll
+    for (int i = 0; i < 25; i++) st[i] = 0;
+    uint64_t r3 = r[3] & 0xFF;
+    st[0] = l[0];
+    st[1] = l[1];
+    st[2] = l[2];
+    st[3] = (l[3] & 0xFF) | (r[0] << 8);
+    st[4] = (r[0] >> 56) | (r[1] << 8);
+    st[5] = (r[1] >> 56) | (r[2] << 8);
+    st[6] = (r[2] >> 56) | (r3 << 8) | (0x01ULL << 16);
+    st[16] = 0x8000000000000000ULL;
+    keccak_f(st);
+    out[0] = st[0];
+    out[1] = st[1];
+    out[2] = st[2];
+    out[3] = st[3] & 0xFF;
+}
+
+template <int H>
+ZK_HD void hash_one(const uint64_t *src, uint64_t len, uint64_t out[4])
+{
+    if (H == HASH_KECCAK) keccak_hash_one(src, len, out);
+    else sponge_hash_one<H>(src, len, out);
+}
+
+template <int H>
+ZK_HD void hash_two(const uint64_t l[4], const uint64_t r[4], uint64_t out[4])
+{
+    if (H == HASH_KECCAK) keccak_hash_two(l, r, out);
+    else sponge_hash_two<H>(l, r, out);
+}
+
+}  // namespace zk

@@ -1,0 +1,80 @@
+// merkle.cu -- host driver of the Merkle forest builder.
+//
+// Follows native/merkle/merkle.cu:166-280 of zeknox for the layout and the
+// special cases (caps == leaves; subtrees of 1 or 2 leaves); launches a leaf
+// kernel that also folds the lower levels, then (for subtrees larger than a
+// CTA) a tail kernel per subtree -- 1 or 2 launches instead of one per level.
+#include <cstdio>
+#include <string>
+
+#include "geom.h"
+#include "merkle.cuh"
+#include "ntt_api.cuh"
+#include "runtime.cuh"
+
+namespace zk {
+
+static constexpr int LEAF_T = 128;     // leaves (threads) per CTA
+static constexpr int TAIL_MAXM = 1024; // nodes a tail CTA can take
+
+bool merkle_geometry_ok(uint64_t n_digests, uint64_t n_caps, uint64_t n_leaves, uint64_t cap_height, std::string &err)
+{
+    return merkle_geometry_check(n_digests, n_caps, n_leaves, cap_height, err);
+}
+
+template <int H>
+static void merkle_launch(uint64_t *digests, uint64_t *caps, const uint64_t *leaves, const MerkleGeom &g, cudaStream_t s)
+{
+    uint64_t blocks = (g.n_leaves + LEAF_T - 1) / LEAF_T;
+    merkle_leaf_kernel<H, LEAF_T><<<(unsigned)blocks, LEAF_T, 0, s>>>(leaves, digests, caps, g);
+    note_launch();
+    if (g.sub_leaves <= (uint64_t)LEAF_T) return;  // caps written by the leaf kernel
+    // heights folded by the leaf kernel
+    uint32_t u0 = 0;
+    while ((1u << (u0 + 1)) <= (uint32_t)LEAF_T && u0 + 1 <= g.log_sub - 1) u0++;
+    while ((g.sub_leaves >> u0) > (uint64_t)TAIL_MAXM) {
+        u0++;
+        uint64_t total = (g.sub_leaves >> u0) * g.n_caps;
+        uint64_t nb = (total + 255) / 256;
+        if (nb > 65535) nb = 65535;
+        merkle_level_kernel<H><<<(unsigned)nb, 256, 0, s>>>(digests, g, u0);
+        note_launch();
+    }
+    merkle_tail_kernel<H, TAIL_MAXM><<<g.n_caps, 256, 0, s>>>(digests, caps, g, u0);
+    note_launch();
+}
+
+bool merkle_device(uint64_t *digests, uint64_t *caps, const uint64_t *leaves, uint64_t n_digests, uint64_t n_caps,
+                   uint64_t n_leaves, uint64_t leaf_size, uint64_t cap_height, uint64_t hash_type, cudaStream_t stream,
+                   std::string &err)
+{
+    if (!merkle_geometry_ok(n_digests, n_caps, n_leaves, cap_height, err)) return false;
+    if (n_caps > 0xFFFFFFFFULL) {
+        err = "too many caps";
+        return false;
+    }
+    MerkleGeom g;
+    g.n_leaves = n_leaves;
+    g.leaf_size = leaf_size;
+    g.sub_leaves = n_leaves / n_caps;
+    g.sub_digests = 2 * g.sub_leaves - 2;
+    g.log_sub = ilog2_exact(g.sub_leaves);
+    g.n_caps = (uint32_t)n_caps;
+    switch (hash_type) {
+    case HASH_POSEIDON: merkle_launch<HASH_POSEIDON>(digests, caps, leaves, g, stream); break;
+    case HASH_KECCAK: merkle_launch<HASH_KECCAK>(digests, caps, leaves, g, stream); break;
+    case HASH_POSEIDON2: merkle_launch<HASH_POSEIDON2>(digests, caps, leaves, g, stream); break;
+    case HASH_MONOLITH: merkle_launch<HASH_MONOLITH>(digests, caps, leaves, g, stream); break;
+    default:
+        err = "unsupported hash_type " + std::to_string(hash_type) + " (Poseidon-BN128 is not built)";
+        return false;
+    }
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) {
+        err = cudaGetErrorString(e);
+        return false;
+    }
+    return true;
+}
+
+}  // namespace zk

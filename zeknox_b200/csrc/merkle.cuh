@@ -1,0 +1,181 @@
+// merkle.cuh -- linear-layout Merkle forest builder (device side).
+//
+// Replaces native/merkle/merkle.cu:24-280 of zeknox.  Layout (unchanged, it is
+// the ABI): 2^cap_height subtrees of L leaves; subtree k owns digests
+// [k(2L-2), (k+1)(2L-2)); in it the level with 2^r nodes starts at 2^r - 2,
+// node i of a level has children 2(i+1)+start and 2(i+1)+1+start of the level
+// below, leaf digests start at L-2, and the subtree root H2(d[0], d[1]) is
+// cap[k].
+//
+// Kernel structure (B200-first instead of one launch per level):
+//   * leaf kernel: one thread per leaf runs the sponge with the state in
+//     registers; the CTA then folds its own T leaves log2(T) levels up in
+//     shared memory, writing every node it produces, and when whole subtrees
+//     fit in the CTA it also writes their caps;
+//   * tail kernel: one CTA per subtree folds the remaining levels in shared
+//     memory and writes the cap (only when L > T).
+#pragma once
+#include <stdint.h>
+
+#include "hash.cuh"
+
+namespace zk {
+
+struct MerkleGeom {
+    uint64_t n_leaves;
+    uint64_t leaf_size;
+    uint64_t sub_leaves;   // L
+    uint64_t sub_digests;  // 2L - 2
+    uint32_t log_sub;      // log2 L
+    uint32_t n_caps;
+};
+
+__device__ __forceinline__ uint64_t merkle_node_index(const MerkleGeom &g, uint64_t first_leaf, uint32_t level_u)
+{
+    // node at height level_u (leaves are height 0) covering leaves starting at first_leaf
+    uint64_t k = first_leaf >> g.log_sub;
+    uint64_t in_sub = first_leaf & (g.sub_leaves - 1);
+    uint64_t level_nodes = g.sub_leaves >> level_u;
+    return k * g.sub_digests + (level_nodes - 2) + (in_sub >> level_u);
+}
+
+template <int H>
+__device__ __forceinline__ void leaf_hash(const uint64_t *__restrict__ row, uint64_t len, uint64_t out[4])
+{
+    hash_one<H>(row, len, out);
+}
+
+// T threads per CTA, T a power of two.  smem: T digests.
+template <int H, int T>
+__global__ void __launch_bounds__(T) merkle_leaf_kernel(const uint64_t *__restrict__ leaves, uint64_t *__restrict__ digests,
+                                                        uint64_t *__restrict__ caps, MerkleGeom g)
+{
+    __shared__ uint64_t node[T][4];
+    const uint64_t i0 = (uint64_t)blockIdx.x * T;
+    const uint32_t t = threadIdx.x;
+    const uint64_t i = i0 + t;
+    uint64_t d[4];
+    if (i < g.n_leaves) {
+        leaf_hash<H>(leaves + i * g.leaf_size, g.leaf_size, d);
+        if (g.sub_leaves == 1) {
+            // caps == leaves: the leaf hashes are the caps, digests untouched
+#pragma unroll
+            for (int q = 0; q < 4; q++) caps[4 * i + q] = d[q];
+            return;
+        }
+        uint64_t di = merkle_node_index(g, i, 0);
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            digests[4 * di + q] = d[q];
+            node[t][q] = d[q];
+        }
+    }
+    if (g.sub_leaves == 1) return;
+    // Levels fully inside this CTA: height u has (L >> u) >= 2 nodes per subtree.
+    uint32_t top = g.log_sub - 1;  // highest stored height
+    uint32_t U = 0;
+    while ((1u << (U + 1)) <= T && U + 1 <= top) U++;
+    const uint64_t cta_leaves = g.n_leaves - i0 < (uint64_t)T ? g.n_leaves - i0 : (uint64_t)T;
+    for (uint32_t u = 1; u <= U; u++) {
+        __syncthreads();
+        uint32_t nodes = T >> u;
+        uint64_t h[4];
+        bool act = t < nodes && ((uint64_t)t << u) < cta_leaves;
+        if (act) {
+            uint64_t l[4], r[4];
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+                l[q] = node[2 * t][q];
+                r[q] = node[2 * t + 1][q];
+            }
+            hash_two<H>(l, r, h);
+            uint64_t di = merkle_node_index(g, i0 + ((uint64_t)t << u), u);
+#pragma unroll
+            for (int q = 0; q < 4; q++) digests[4 * di + q] = h[q];
+        }
+        __syncthreads();
+        if (act) {
+#pragma unroll
+            for (int q = 0; q < 4; q++) node[t][q] = h[q];
+        }
+    }
+    // Whole subtrees inside the CTA: their caps come from the two top nodes.
+    if (U == top && g.sub_leaves <= (uint64_t)T) {
+        __syncthreads();
+        uint32_t subs = (uint32_t)((cta_leaves + g.sub_leaves - 1) >> g.log_sub);
+        if (t < subs) {
+            uint64_t l[4], r[4], h[4];
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+                l[q] = node[2 * t][q];
+                r[q] = node[2 * t + 1][q];
+            }
+            hash_two<H>(l, r, h);
+            uint64_t k = (i0 >> g.log_sub) + t;
+#pragma unroll
+            for (int q = 0; q < 4; q++) caps[4 * k + q] = h[q];
+        }
+    }
+}
+
+// One CTA per subtree: starting from the stored level of height u0 (m nodes per
+// subtree, 2 < m <= MAXM), fold to 2 nodes and write the cap.  Two shared
+// buffers (MAXM and MAXM/2 digests) alternate between levels.
+template <int H, int MAXM>
+__global__ void __launch_bounds__(256) merkle_tail_kernel(uint64_t *__restrict__ digests, uint64_t *__restrict__ caps,
+                                                          MerkleGeom g, uint32_t u0)
+{
+    __shared__ uint64_t bufa[MAXM][4];
+    __shared__ uint64_t bufb[MAXM / 2][4];
+    const uint64_t k = blockIdx.x;
+    uint64_t *sub = digests + k * g.sub_digests * 4;
+    uint32_t m = (uint32_t)(g.sub_leaves >> u0);
+    for (uint32_t j = threadIdx.x; j < m; j += blockDim.x)
+#pragma unroll
+        for (int q = 0; q < 4; q++) bufa[j][q] = sub[4 * (m - 2 + j) + q];
+    uint64_t(*src)[4] = bufa;
+    uint64_t(*dst)[4] = bufb;
+    while (m > 2) {
+        __syncthreads();
+        uint32_t half = m / 2;
+        for (uint32_t j = threadIdx.x; j < half; j += blockDim.x) {
+            uint64_t h[4];
+            hash_two<H>(src[2 * j], src[2 * j + 1], h);
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+                sub[4 * (half - 2 + j) + q] = h[q];
+                dst[j][q] = h[q];
+            }
+        }
+        uint64_t(*tmp)[4] = src;
+        src = dst;
+        dst = tmp;
+        m = half;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint64_t h[4];
+        hash_two<H>(src[0], src[1], h);
+#pragma unroll
+        for (int q = 0; q < 4; q++) caps[4 * k + q] = h[q];
+    }
+}
+
+// One level, node-parallel, for very large subtrees (m > tail capacity).
+template <int H>
+__global__ void merkle_level_kernel(uint64_t *__restrict__ digests, MerkleGeom g, uint32_t u)
+{
+    uint64_t per_sub = g.sub_leaves >> u;
+    uint64_t total = per_sub * g.n_caps;
+    for (uint64_t x = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; x < total; x += (uint64_t)gridDim.x * blockDim.x) {
+        uint64_t k = x / per_sub, j = x % per_sub;
+        uint64_t *sub = digests + k * g.sub_digests * 4;
+        uint64_t start = per_sub - 2, child = 2 * per_sub - 2;
+        uint64_t h[4];
+        hash_two<H>(sub + 4 * (child + 2 * j), sub + 4 * (child + 2 * j + 1), h);
+#pragma unroll
+        for (int q = 0; q < 4; q++) sub[4 * (start + j) + q] = h[q];
+    }
+}
+
+}  // namespace zk

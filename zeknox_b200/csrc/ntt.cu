@@ -1,0 +1,327 @@
+// ntt.cu -- host drivers of the batched NTT / LDE / transpose.
+//
+// Semantics follow zeknox native/ntt/ntt.cu (batch_ntt :253-309, batch_lde
+// :477-564, compute_transpose_rev :182-226); the execution plan is this
+// project's: a handful of multi-stage DIF passes (ntt.cuh) plus one tiled
+// reorder, instead of one HBM pass per radix-2 stage.
+#include <algorithm>
+#include <chrono>
+#include <cstdlib>
+#include <cstring>
+
+#include "ntt.cuh"
+#include "ntt_api.cuh"
+#include "runtime.cuh"
+#include "zk_constants.h"
+
+namespace zk {
+
+static const uint64_t H_SIZE_INV[33] = {ZK_DOMAIN_SIZE_INV_LIST};
+static const uint64_t H_OMEGA_N[33] = {ZK_OMEGA_LIST};
+
+static constexpr int PASS_NT = 512;
+static constexpr int PASS_TILE = 8192;
+
+// ------------------------------------------------------------- pass dispatch
+
+template <int LOGR, int INV, int LOADM, int STOREM>
+static void launch_one(const NttPassArgs &a, uint64_t grid, uint32_t smem, cudaStream_t s)
+{
+    auto k = ntt_pass_kernel<LOGR, INV, PASS_NT, PASS_TILE, LOADM, STOREM>;
+    static bool attr = false;
+    if (!attr) {
+        ZK_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, PASS_TILE * 8));
+        attr = true;
+    }
+    k<<<(unsigned)grid, PASS_NT, smem, s>>>(a);
+    note_launch();
+}
+
+template <int INV, int LOADM, int STOREM>
+static void launch_pass(uint32_t logr, const NttPassArgs &a, uint64_t grid, uint32_t smem, cudaStream_t s)
+{
+#define ZK_CASE(r) \
+    case r: launch_one<(STOREM == STORE_ROWS && r > 9) ? 9 : r, INV, LOADM, STOREM>(a, grid, smem, s); break;
+    switch (logr) {
+        ZK_CASE(1) ZK_CASE(2) ZK_CASE(3) ZK_CASE(4) ZK_CASE(5) ZK_CASE(6)
+        ZK_CASE(7) ZK_CASE(8) ZK_CASE(9) ZK_CASE(10) ZK_CASE(11) ZK_CASE(12)
+    default: throw arg_failure("bad pass radix");
+    }
+#undef ZK_CASE
+}
+
+struct Pass {
+    uint32_t s_lo, logr;
+};
+
+// Split L stages into passes of at most 12 (the last at most 9 for row output).
+static std::vector<Pass> plan_passes(uint32_t L, bool rows)
+{
+    std::vector<uint32_t> sizes;
+    const uint32_t last_max = rows ? 9 : 12;
+    if (L <= last_max) {
+        sizes.push_back(L);
+    } else if (!rows) {
+        uint32_t np = (L + 11) / 12;
+        for (uint32_t i = 0; i < np; i++) sizes.push_back(L / np + (i < L % np ? 1 : 0));
+    } else {
+        uint32_t rem = L - 9;
+        uint32_t np = (rem + 11) / 12;
+        for (uint32_t i = 0; i < np; i++) sizes.push_back(rem / np + (i < rem % np ? 1 : 0));
+        sizes.push_back(9);
+    }
+    std::vector<Pass> p;
+    uint32_t hi = L;
+    for (uint32_t k : sizes) {
+        hi -= k;
+        p.push_back({hi, k});
+    }
+    return p;
+}
+
+// Batched DIF over `vcols` virtual columns of size 2^L; output in bit-reversed
+// order, either in vcol-major layout at dst (stride dst_stride) or, for
+// rows=true, as leaf rows (see STORE_ROWS).  `scratch` (vcols * 2^L words) is
+// needed only when rows=true and there is more than one pass.
+struct DifJob {
+    const uint64_t *src;
+    uint64_t src_stride;
+    int load;                 // NttLoad of the first pass
+    const uint64_t *tab;
+    uint64_t n_src;
+    uint64_t *dst;
+    uint64_t dst_stride;
+    uint64_t vcols;
+    uint32_t L;
+    uint32_t rate;
+    uint32_t cols;
+    bool rows;
+    bool inverse;
+    uint64_t *scratch;
+};
+
+static void run_dif(DeviceCtx &c, const DifJob &j)
+{
+    if (j.L == 0) {
+        // size-1 transform: copy (with scaling) -- handled by the caller's reorder
+        throw arg_failure("zero-size transform");
+    }
+    auto passes = plan_passes(j.L, j.rows);
+    const uint64_t n = 1ULL << j.L;
+    const uint64_t *tw_small = c.twiddles(12, j.inverse);
+    for (size_t pi = 0; pi < passes.size(); pi++) {
+        const Pass &ps = passes[pi];
+        const bool first = pi == 0, last = pi + 1 == passes.size();
+        NttPassArgs a{};
+        a.src = first ? j.src : (j.rows ? j.scratch : j.dst);
+        a.src_stride = first ? j.src_stride : (j.rows ? n : j.dst_stride);
+        a.tab = j.tab;
+        a.n_src = j.n_src;
+        a.tw_small = tw_small;
+        a.tw_pass = ps.s_lo ? c.twiddles(ps.s_lo + ps.logr, j.inverse) : nullptr;
+        a.vcols = j.vcols;
+        a.L = j.L;
+        a.s_lo = ps.s_lo;
+        a.rate = j.rate;
+        a.cols = j.cols;
+        const bool store_rows = j.rows && last;
+        if (store_rows) {
+            a.dst = j.dst;
+            a.dst_stride = 0;
+        } else {
+            a.dst = j.rows ? j.scratch : j.dst;
+            a.dst_stride = j.rows ? n : j.dst_stride;
+        }
+        const int load = first ? j.load : LOAD_PLAIN;
+        if (store_rows && ps.logr > 9) throw arg_failure("row-output pass radix above 2^9");
+        uint64_t grid;
+        uint32_t tile;
+        if (store_rows) {
+            uint32_t W = (uint32_t)std::min<uint64_t>(n, PASS_TILE / 16);
+            tile = 16 * W;
+            uint64_t ncg = (j.cols + 15) / 16;
+            grid = (n / W) * ncg * (1ULL << j.rate);
+        } else {
+            tile = (uint32_t)std::min<uint64_t>(n, PASS_TILE);
+            grid = j.vcols * (n / tile);
+        }
+        if (grid == 0) continue;
+        if (grid > 0x7FFFFFFFULL) throw arg_failure("transform batch too large for one launch");
+        const uint32_t smem = tile * 8;
+        if (!j.inverse) {
+            if (store_rows) {
+                if (load == LOAD_COSETS) launch_pass<0, LOAD_COSETS, STORE_ROWS>(ps.logr, a, grid, smem, c.stream);
+                else launch_pass<0, LOAD_PLAIN, STORE_ROWS>(ps.logr, a, grid, smem, c.stream);
+            } else {
+                if (load == LOAD_COSETS) launch_pass<0, LOAD_COSETS, STORE_SAME>(ps.logr, a, grid, smem, c.stream);
+                else if (load == LOAD_SCALE) launch_pass<0, LOAD_SCALE, STORE_SAME>(ps.logr, a, grid, smem, c.stream);
+                else launch_pass<0, LOAD_PLAIN, STORE_SAME>(ps.logr, a, grid, smem, c.stream);
+            }
+        } else {
+            if (store_rows) throw arg_failure("inverse transform with row output is not supported");
+            if (load == LOAD_EXTEND) launch_pass<1, LOAD_EXTEND, STORE_SAME>(ps.logr, a, grid, smem, c.stream);
+            else launch_pass<1, LOAD_PLAIN, STORE_SAME>(ps.logr, a, grid, smem, c.stream);
+        }
+        ZK_CUDA(cudaGetLastError());
+    }
+}
+
+// bit-reversed (per virtual column) -> natural, with factor mul and optional table
+static void reorder(DeviceCtx &c, const uint64_t *src, uint64_t src_stride, uint64_t *dst, uint64_t dst_stride,
+                    uint32_t lg_t, uint32_t rate, uint64_t cols, uint64_t mul, const uint64_t *tab)
+{
+    const uint32_t a = lg_t >= 10 ? 5 : lg_t / 2;
+    const uint64_t blocks = cols * (1ULL << (lg_t - 2 * a)) * (1ULL << rate);
+    if (blocks > 0x7FFFFFFFULL) throw arg_failure("reorder too large for one launch");
+    bitrev_reorder_kernel<<<(unsigned)blocks, 256, 0, c.stream>>>(src, dst, src_stride, dst_stride, lg_t, rate, cols, mul,
+                                                                  tab);
+    note_launch();
+    ZK_CUDA(cudaGetLastError());
+}
+
+// --------------------------------------------------------------- public ops
+
+void ntt_batch_device(DeviceCtx &c, uint64_t *inout, uint32_t lg, uint64_t batches, bool inverse, bool with_coset)
+{
+    const uint64_t n = 1ULL << lg;
+    if (batches == 0) return;
+    DevBuf tmp(c, n * batches);
+    if (!inverse) {
+        DifJob j{};
+        j.src = inout;
+        j.src_stride = n;
+        j.load = with_coset ? LOAD_SCALE : LOAD_PLAIN;
+        j.tab = with_coset ? c.coset_powers(lg) : nullptr;
+        j.dst = tmp.p;
+        j.dst_stride = n;
+        j.vcols = batches;
+        j.L = lg;
+        run_dif(c, j);
+        reorder(c, tmp.p, n, inout, n, lg, 0, batches, 1, nullptr);
+    } else {
+        DifJob j{};
+        j.src = inout;
+        j.src_stride = n;
+        j.load = LOAD_PLAIN;
+        j.dst = tmp.p;
+        j.dst_stride = n;
+        j.vcols = batches;
+        j.L = lg;
+        j.inverse = true;
+        run_dif(c, j);
+        // reference order: coset multiply (forward powers) then n^-1 (ntt.cu:137-143)
+        reorder(c, tmp.p, n, inout, n, lg, 0, batches, H_SIZE_INV[lg], with_coset ? c.coset_powers(lg) : nullptr);
+    }
+}
+
+void lde_batch_device(DeviceCtx &c, uint64_t *out, const uint64_t *in, uint32_t lg_n, uint32_t rate, uint64_t batches,
+                      bool inverse, bool with_coset)
+{
+    const uint64_t n = 1ULL << lg_n;
+    const uint32_t lgN = lg_n + rate;
+    const uint64_t N = 1ULL << lgN;
+    if (batches == 0) return;
+    DevBuf tmp(c, N * batches);
+    if (!inverse) {
+        // coset c of column b is virtual column b*2^rate + c of size n
+        const uint64_t g = with_coset ? (c.coset_powers(0), c.coset_gen) : 1;
+        DifJob j{};
+        j.src = in;
+        j.src_stride = n;
+        j.load = LOAD_COSETS;
+        j.tab = c.lde_table(lg_n, rate, g);
+        j.dst = tmp.p;
+        j.dst_stride = n;
+        j.vcols = batches << rate;
+        j.L = lg_n;
+        j.rate = rate;
+        run_dif(c, j);
+        reorder(c, tmp.p, n, out, N, lg_n, rate, batches, 1, nullptr);
+    } else {
+        // zero-extended inverse transform of size N (ntt.cu:529-535)
+        DifJob j{};
+        j.src = in;
+        j.src_stride = n;
+        j.load = LOAD_EXTEND;
+        j.n_src = n;
+        j.dst = tmp.p;
+        j.dst_stride = N;
+        j.vcols = batches;
+        j.L = lgN;
+        j.inverse = true;
+        run_dif(c, j);
+        reorder(c, tmp.p, N, out, N, lgN, 0, batches, H_SIZE_INV[lgN], with_coset ? c.coset_powers(lgN) : nullptr);
+    }
+}
+
+void lde_rows_device(DeviceCtx &c, uint64_t *rows, const uint64_t *coeffs, uint32_t lg_n, uint32_t rate, uint64_t cols,
+                     uint64_t coset_gen, uint64_t *scratch)
+{
+    const uint64_t n = 1ULL << lg_n;
+    if (cols == 0) return;
+    DifJob j{};
+    j.src = coeffs;
+    j.src_stride = n;
+    j.load = LOAD_COSETS;
+    j.tab = c.lde_table(lg_n, rate, coset_gen % GL_P);
+    j.dst = rows;
+    j.vcols = cols << rate;
+    j.L = lg_n;
+    j.rate = rate;
+    j.cols = (uint32_t)cols;
+    j.rows = true;
+    DevBuf tmp;
+    if (plan_passes(lg_n, true).size() > 1) {
+        if (!scratch) {
+            tmp.ctx = &c;
+            tmp.p = c.alloc((n << rate) * cols * 8);
+            scratch = tmp.p;
+        }
+        j.scratch = scratch;
+    }
+    run_dif(c, j);
+}
+
+uint64_t lde_rows_scratch_elems(uint32_t lg_n, uint32_t rate, uint64_t cols)
+{
+    return plan_passes(lg_n, true).size() > 1 ? ((1ULL << (lg_n + rate)) * cols) : 0;
+}
+
+void transpose_rev_device(DeviceCtx &c, uint64_t *out, const uint64_t *in, uint32_t lg, uint64_t cols)
+{
+    const uint64_t n = 1ULL << lg;
+    if (cols == 0) return;
+    dim3 grid((unsigned)((n + 31) / 32), (unsigned)((cols + 31) / 32));
+    if (grid.y > 65535) throw arg_failure("too many columns for transpose");
+    transpose_rev_kernel<<<grid, 256, 0, c.stream>>>(in, out, lg, cols);
+    note_launch();
+    ZK_CUDA(cudaGetLastError());
+}
+
+// salt columns: seeded counter-based values in [0, p) (the reference draws
+// curand numbers seeded with time(NULL), native/ntt/ntt.cu:541-546)
+__global__ void salt_kernel(uint64_t *out, uint64_t count, uint64_t seed)
+{
+    for (uint64_t k = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; k < count; k += (uint64_t)gridDim.x * blockDim.x) {
+        uint64_t z = seed + (k + 1) * 0x9E3779B97F4A7C15ULL;
+        z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
+        z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
+        z ^= z >> 31;
+        out[k] = z >= GL_P ? z - GL_P : z;
+    }
+}
+
+void salt_device(DeviceCtx &c, uint64_t *out, uint64_t count)
+{
+    uint64_t seed;
+    const char *env = getenv("ZEKNOX_SALT_SEED");
+    if (env) seed = strtoull(env, nullptr, 0);
+    else seed = (uint64_t)std::chrono::steady_clock::now().time_since_epoch().count();
+    uint64_t blocks = std::min<uint64_t>((count + 255) / 256, (uint64_t)c.sm_count * 8);
+    if (blocks == 0) return;
+    salt_kernel<<<(unsigned)blocks, 256, 0, c.stream>>>(out, count, seed);
+    note_launch();
+    ZK_CUDA(cudaGetLastError());
+}
+
+}  // namespace zk

@@ -1,0 +1,364 @@
+// ntt.cuh -- batched Goldilocks NTT passes (device side).
+//
+// Replaces the radix-2 stage kernels of zeknox native/ntt/kernels.cu:160-392
+// (one global pass per stage) with a multi-pass decimation-in-frequency
+// engine: each pass applies k = LOGR consecutive DIF stages to every group of
+// R = 2^k elements spaced S = 2^s_lo apart, through shared memory, so a 2^L
+// transform costs ceil(L / k) passes over HBM instead of L.
+//
+// Math.  For a block of M = R*S elements viewed as x[m*S + o] (m < R, o < S),
+// the first k DIF stages leave, at position m'*S + o,
+//     w_M^(o * f) * sum_m x[m*S + o] * w_R^(m * f),     f = rev_k(m'),
+// after which every run of S contiguous positions is an independent DIF of
+// size S.  The R-point transform inside a pass is itself split the same way
+// into register-resident E-point DIFs (E <= 16) whose twiddles are powers of
+// w_E, i.e. powers of 2 (w_64 = 2^39 for zeknox's roots), so they cost a shift
+// and a reduction instead of a multiplication.  After the last pass position
+// j of each transform holds X[rev_L(j)] (bit-reversed order).
+//
+// A "virtual column" is one independent transform.  For a low-degree
+// extension of rate 2^rate, coset c of input column b is its own virtual
+// column: coefficient j is scaled by (g * w_N^c)^j and transformed at size n,
+// and its bit-reversed output is exactly rows [rev_rate(c)*n, (rev_rate(c)+1)*n)
+// of the bit-reversed size-N evaluation -- zero-extension never touches memory.
+#pragma once
+#include <stdint.h>
+
+#include "gl64.cuh"
+
+namespace zk {
+
+// w_{2^h} = 2^EXP for the reference's roots (h = 1..6), forward and inverse.
+__host__ __device__ constexpr unsigned root_exp(int h, int inv)
+{
+    return inv ? (h == 1 ? 96 : h == 2 ? 144 : h == 3 ? 72 : h == 4 ? 36 : h == 5 ? 114 : 153)
+               : (h == 1 ? 96 : h == 2 ? 48 : h == 3 ? 120 : h == 4 ? 156 : h == 5 ? 78 : 39);
+}
+
+// In-register DIF on E = 2^LOGE values: natural input, bit-reversed output.
+template <int LOGE, int INV>
+__device__ __forceinline__ void dif_regs(uint64_t *x)
+{
+    constexpr int E = 1 << LOGE;
+#pragma unroll
+    for (int h = LOGE; h >= 1; h--) {
+        const int span = 1 << (h - 1);
+#pragma unroll
+        for (int blk = 0; blk < E; blk += 2 * span) {
+#pragma unroll
+            for (int i = 0; i < span; i++) {
+                uint64_t u = x[blk + i], v = x[blk + i + span];
+                x[blk + i] = gl_add(u, v);
+                uint64_t d = gl_sub(u, v);
+                x[blk + i + span] = i == 0 ? d : gl_mul_pow2(d, (root_exp(h, INV) * (unsigned)i) % 192u);
+            }
+        }
+    }
+}
+
+// XOR-fold swizzle of a shared-memory word index (8-byte words): every
+// power-of-two access stride used below hits 16 distinct 8-byte banks.
+__device__ __forceinline__ uint32_t swz(uint32_t w) { return w ^ (((w >> 4) ^ (w >> 8) ^ (w >> 12)) & 15u); }
+
+enum NttLoad : int {
+    LOAD_PLAIN = 0,      // src[v * src_stride + j]
+    LOAD_SCALE = 1,      // src[v * src_stride + j] * tab[j]              (coset powers g^j)
+    LOAD_COSETS = 2,     // src[(v >> rate) * src_stride + j] * tab[(v & (2^rate-1)) * n + j]
+    LOAD_EXTEND = 3,     // j < n_src ? src[v * src_stride + j] : 0        (zero-extended transform)
+};
+
+enum NttStore : int {
+    STORE_SAME = 0,      // dst[v * dst_stride + position]
+    STORE_ROWS = 1,      // leaf-major: dst[(rev_rate(v & mask) * n + position) * cols + (v >> rate)]
+};
+
+struct NttPassArgs {
+    const uint64_t *src;
+    uint64_t *dst;
+    const uint64_t *tab;      // LOAD_SCALE / LOAD_COSETS / LOAD_EXTEND_SCALE table
+    const uint64_t *tw_pass;  // w_M^t, t < M   (M = R * S); unused when S == 1
+    const uint64_t *tw_small; // w_4096^t, t < 4096 (inverse roots for INV)
+    uint64_t src_stride;      // elements between consecutive source columns
+    uint64_t dst_stride;
+    uint64_t n_src;           // LOAD_EXTEND: nonzero prefix length
+    uint64_t vcols;           // virtual columns
+    uint32_t L;               // log2 transform size
+    uint32_t s_lo;            // lowest stage of this pass
+    uint32_t rate;            // LOAD_COSETS / STORE_ROWS: log2 cosets per column
+    uint32_t cols;            // STORE_ROWS: real columns (row length of the output)
+};
+
+// Sub-step of the in-CTA R-point DIF: every task owns E elements spaced Q apart
+// inside a block of size R_cur = E * Q.
+template <int LOGE, int INV, int NT>
+__device__ __forceinline__ void dif_substep(uint64_t *sm, uint32_t tile_elems, uint32_t log_rcur,
+                                            const uint64_t *__restrict__ tw_small)
+{
+    constexpr int E = 1 << LOGE;
+    const uint32_t R_cur = 1u << log_rcur;
+    const uint32_t Q = R_cur >> LOGE;
+    const uint32_t tasks = tile_elems >> LOGE;
+    for (uint32_t t = threadIdx.x; t < tasks; t += NT) {
+        uint32_t m_lo = t & (Q - 1);
+        uint32_t blk = t >> (log_rcur - LOGE);  // block of R_cur (across groups)
+        uint32_t base = blk * R_cur + m_lo;
+        uint64_t x[E];
+#pragma unroll
+        for (int e = 0; e < E; e++) x[e] = sm[swz(base + e * Q)];
+        dif_regs<LOGE, INV>(x);
+        if (Q > 1) {
+            // position p gets w_{R_cur}^(m_lo * rev_e(p)); w_{R_cur} = w_4096^(4096 / R_cur)
+            uint32_t step = (uint32_t)m_lo << (12 - log_rcur);
+#pragma unroll
+            for (int p = 1; p < E; p++) {
+                uint32_t f = bitrev32((uint32_t)p, LOGE);
+                x[p] = gl_mul(x[p], __ldg(tw_small + ((step * f) & 4095u)));
+            }
+        }
+#pragma unroll
+        for (int e = 0; e < E; e++) sm[swz(base + e * Q)] = x[e];
+    }
+}
+
+// One pass: LOGR stages on groups of R = 2^LOGR elements; at most TILE
+// elements per CTA (dynamic shared memory of TILE words).
+//   STORE_SAME tiles: min(TILE, n) positions of one virtual column; when the
+//     group spacing S is at least the number of groups per tile the rows of a
+//     tile are runs of consecutive offsets, otherwise the tile is one
+//     contiguous span of whole blocks.
+//   STORE_ROWS tiles (last pass, S == 1): 16 virtual columns of one coset and
+//     consecutive source columns x W positions, so every output leaf row gets
+//     16 consecutive 8-byte words.
+template <int LOGR, int INV, int NT, int TILE, int LOADM, int STOREM>
+__global__ void __launch_bounds__(NT) ntt_pass_kernel(NttPassArgs a)
+{
+    extern __shared__ uint64_t sm[];
+    constexpr uint32_t R = 1u << LOGR;
+    constexpr uint32_t CW = 16;
+    const uint32_t S = 1u << a.s_lo;
+    const uint64_t n = 1ULL << a.L;
+    const uint64_t M = (uint64_t)R << a.s_lo;
+    const uint32_t rmask = (1u << a.rate) - 1;
+    const uint32_t W = (STOREM == STORE_ROWS) ? (uint32_t)(n < TILE / CW ? n : TILE / CW) : 0;
+    const uint32_t tile = (STOREM == STORE_ROWS) ? CW * W : (uint32_t)(n < TILE ? n : TILE);
+    const uint32_t G = tile / R;    // groups per tile
+    const uint32_t GW = W / R;      // groups per virtual column (row tiles)
+
+    uint64_t v0, pos0;
+    if (STOREM == STORE_ROWS) {
+        const uint64_t per_v = n / W;
+        const uint64_t t = blockIdx.x;
+        const uint64_t posblk = t % per_v, cg = t / per_v;
+        const uint64_t ncg = (a.cols + CW - 1) / CW;
+        const uint64_t coset = cg / ncg, colg = cg % ncg;
+        v0 = ((colg * CW) << a.rate) | coset;
+        pos0 = posblk * W;
+    } else {
+        const uint64_t tiles_per_v = n / tile;
+        v0 = blockIdx.x / tiles_per_v;
+        pos0 = (blockIdx.x % tiles_per_v) * tile;
+    }
+
+    // tile element (group g, member m) -> (virtual column, position)
+    auto gpos = [&](uint32_t g, uint32_t m, uint64_t &vcol, uint64_t &pos) {
+        if (STOREM == STORE_ROWS) {
+            const uint32_t c = g / GW, gg = g % GW;
+            vcol = v0 + ((uint64_t)c << a.rate);
+            pos = pos0 + (uint64_t)gg * R + m;
+        } else {
+            vcol = v0;
+            const uint64_t gid = pos0 / R + g;
+            pos = (gid >> a.s_lo) * M + (uint64_t)m * S + (gid & (S - 1));
+        }
+    };
+    // linear index e -> (g, m) so that consecutive e are consecutive addresses
+    auto split_in = [&](uint32_t e, uint32_t &g, uint32_t &m) {
+        if (STOREM == STORE_ROWS) {
+            const uint32_t c = e / W, w = e % W;
+            g = c * GW + w / R;
+            m = w % R;
+        } else if (S >= G) {
+            g = e % G;
+            m = e / G;
+        } else {
+            const uint32_t blk = e / (uint32_t)M, rem = e % (uint32_t)M;
+            m = rem >> a.s_lo;
+            g = blk * S + (rem & (S - 1));
+        }
+    };
+
+    // ---- load
+    for (uint32_t e = threadIdx.x; e < tile; e += NT) {
+        uint32_t g, m;
+        split_in(e, g, m);
+        uint64_t vcol, pos;
+        gpos(g, m, vcol, pos);
+        uint64_t val = 0;
+        const bool ok = (STOREM == STORE_ROWS) ? ((vcol >> a.rate) < a.cols) : (vcol < a.vcols);
+        if (ok) {
+            if (LOADM == LOAD_PLAIN) {
+                val = a.src[vcol * a.src_stride + pos];
+            } else if (LOADM == LOAD_SCALE) {
+                val = gl_mul(a.src[vcol * a.src_stride + pos], __ldg(a.tab + pos));
+            } else if (LOADM == LOAD_COSETS) {
+                val = gl_mul(a.src[(vcol >> a.rate) * a.src_stride + pos], __ldg(a.tab + (vcol & rmask) * n + pos));
+            } else {  // LOAD_EXTEND
+                val = pos < a.n_src ? a.src[vcol * a.src_stride + pos] : 0;
+            }
+        }
+        sm[swz(g * R + m)] = val;
+    }
+    __syncthreads();
+
+    // ---- R-point DIF in sub-steps of up to 16 points
+    constexpr int NSTEP = (LOGR + 3) / 4;
+#pragma unroll
+    for (int st = 0; st < NSTEP; st++) {
+        const uint32_t log_rcur = LOGR - 4 * st;
+        if (log_rcur >= 4) dif_substep<4, INV, NT>(sm, tile, log_rcur, a.tw_small);
+        else if (log_rcur == 3) dif_substep<3, INV, NT>(sm, tile, 3, a.tw_small);
+        else if (log_rcur == 2) dif_substep<2, INV, NT>(sm, tile, 2, a.tw_small);
+        else dif_substep<1, INV, NT>(sm, tile, 1, a.tw_small);
+        __syncthreads();
+    }
+
+    // ---- pass twiddle + store
+    for (uint32_t e = threadIdx.x; e < tile; e += NT) {
+        uint32_t g, m;
+        if (STOREM == STORE_ROWS) {
+            const uint32_t w = e / CW, c = e % CW;  // consecutive e -> consecutive columns of one row
+            g = c * GW + w / R;
+            m = w % R;
+        } else {
+            split_in(e, g, m);
+        }
+        uint64_t vcol, pos;
+        gpos(g, m, vcol, pos);
+        uint64_t val = sm[swz(g * R + m)];
+        if (S > 1) {
+            const uint64_t o = pos & (S - 1);
+            const uint64_t f = bitrev32(m, LOGR);
+            val = gl_mul(val, __ldg(a.tw_pass + o * f));
+        }
+        if (STOREM == STORE_ROWS) {
+            const uint64_t b = vcol >> a.rate;
+            if (b < a.cols) {
+                const uint64_t row = ((uint64_t)bitrev32((uint32_t)(vcol & rmask), a.rate) << a.L) + pos;
+                a.dst[row * a.cols + b] = val;
+            }
+        } else if (vcol < a.vcols) {
+            a.dst[vcol * a.dst_stride + pos] = val;
+        }
+    }
+}
+
+// ------------------------------------------------------------------ reorders
+
+// Bit-reversed -> natural order with optional per-element factor:
+//   dst[v * dst_stride + i] = src[v * src_stride + rev_L(i)] * scale(i)
+// where scale(i) = mul (a constant, e.g. n^-1), times tab[i] when tab != null.
+// For the LDE interleave (rate > 0): natural index i = c + 2^rate * t takes
+// virtual column v * 2^rate + c at bit-reversed position t.
+// Tiles of 32 x 32 through shared memory so both sides are coalesced.
+static __global__ void __launch_bounds__(256) bitrev_reorder_kernel(const uint64_t *__restrict__ src, uint64_t *__restrict__ dst,
+                                                             uint64_t src_stride, uint64_t dst_stride, uint32_t lg_t,
+                                                             uint32_t rate, uint64_t cols, uint64_t mul,
+                                                             const uint64_t *__restrict__ tab)
+{
+    // Natural output index i = c + 2^rate * t, t < 2^lg_t, c < 2^rate.
+    // Source: virtual column (v << rate) + c, position rev(t).
+    // Split t = hi * 2^(lg_t - a) + mid * 2^a + lo with a = min(5, lg_t / 2).
+    __shared__ uint64_t tile[32][33];
+    const uint32_t a = lg_t >= 10 ? 5 : lg_t / 2;
+    const uint32_t A = 1u << a;
+    const uint32_t mid_bits = lg_t - 2 * a;
+    const uint64_t n_mid = 1ULL << mid_bits;
+    const uint64_t per_col = n_mid << rate;  // (mid, c) tiles per column
+    uint64_t blk = blockIdx.x;
+    uint64_t v = blk / per_col;
+    uint64_t rem = blk % per_col;
+    uint32_t c = (uint32_t)(rem % (1u << rate));
+    uint64_t mid = rem >> rate;
+    if (v >= cols) return;
+    const uint32_t tx = threadIdx.x & 31, ty = threadIdx.x >> 5;  // 32 x 8
+    const uint64_t *s = src + ((v << rate) + c) * src_stride;
+    // read: source position q = rev(t) = rev(lo) * 2^(lg_t-a) + rev(mid) * 2^a + rev(hi)
+    // fix lo (row ry), vary hi (tx) -> contiguous source positions rev(hi)
+    uint64_t rmid = bitrev64(mid, mid_bits);
+    for (uint32_t ry = ty; ry < A; ry += 8) {
+        if (tx < A) {
+            uint64_t q = ((uint64_t)bitrev32(ry, a) << (lg_t - a)) + (rmid << a) + tx;
+            // tx = rev(hi) -> hi = rev(tx)
+            tile[ry][bitrev32(tx, a)] = s[q];
+        }
+    }
+    __syncthreads();
+    // write: t = hi * 2^(lg_t-a) + mid * 2^a + lo; fix hi (row), vary lo (tx) -> contiguous t
+    uint64_t *d = dst + v * dst_stride;
+    for (uint32_t hy = ty; hy < A; hy += 8) {
+        if (tx < A) {
+            uint64_t t = ((uint64_t)hy << (lg_t - a)) + (mid << a) + tx;
+            uint64_t i = (t << rate) + c;
+            uint64_t val = tile[tx][hy];
+            if (mul != 1) val = gl_mul(val, mul);
+            if (tab) val = gl_mul(val, __ldg(tab + i));
+            d[i] = val;
+        }
+    }
+}
+
+// compute_transpose_rev: out[rev_lg(i) * cols + b] = in[b * n + i].
+// Tile: 32 positions x 32 columns, 8 rows of threads.
+static __global__ void __launch_bounds__(256) transpose_rev_kernel(const uint64_t *__restrict__ in, uint64_t *__restrict__ out,
+                                                            uint32_t lg, uint64_t cols)
+{
+    __shared__ uint64_t tile[32][33];
+    const uint64_t n = 1ULL << lg;
+    const uint64_t i0 = (uint64_t)blockIdx.x * 32;
+    const uint64_t b0 = (uint64_t)blockIdx.y * 32;
+    const uint32_t tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+    for (uint32_t r = ty; r < 32; r += 8) {
+        uint64_t b = b0 + r, i = i0 + tx;
+        if (b < cols && i < n) tile[r][tx] = in[b * n + i];
+    }
+    __syncthreads();
+    for (uint32_t r = ty; r < 32; r += 8) {
+        uint64_t i = i0 + r, b = b0 + tx;
+        if (b < cols && i < n) out[bitrev64(i, lg) * cols + b] = tile[tx][r];
+    }
+}
+
+// Multiply every element of a batch of columns by mul (e.g. n^-1) and, when
+// tab != null, by tab[i] (i = index within the column).  Used for transforms
+// too small for the tiled reorder.
+static __global__ void scale_kernel(uint64_t *x, uint64_t n, uint64_t cols, uint64_t mul, const uint64_t *__restrict__ tab)
+{
+    uint64_t total = n * cols;
+    for (uint64_t k = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; k < total; k += (uint64_t)gridDim.x * blockDim.x) {
+        uint64_t i = k % n;
+        uint64_t v = x[k];
+        if (mul != 1) v = gl_mul(v, mul);
+        if (tab) v = gl_mul(v, __ldg(tab + i));
+        x[k] = v;
+    }
+}
+
+// tab[t] = w^t for t < count (one square-and-multiply per entry).
+static __global__ void powers_kernel(uint64_t *tab, uint64_t count, uint64_t w)
+{
+    for (uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; t < count; t += (uint64_t)gridDim.x * blockDim.x)
+        tab[t] = gl_pow(w, t);
+}
+
+// LDE coset table: tab[c * n + j] = (g * w_N^c)^j for c < 2^rate, j < n.
+static __global__ void coset_powers_kernel(uint64_t *tab, uint64_t n, uint32_t cosets, uint64_t g, uint64_t wN)
+{
+    uint64_t total = n * cosets;
+    for (uint64_t k = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; k < total; k += (uint64_t)gridDim.x * blockDim.x) {
+        uint64_t c = k / n, j = k % n;
+        uint64_t base = gl_mul(g, gl_pow(wN, c));
+        tab[k] = gl_pow(base, j);
+    }
+}
+
+}  // namespace zk

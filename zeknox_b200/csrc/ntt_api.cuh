@@ -1,0 +1,35 @@
+// ntt_api.cuh -- host-side entry points of the NTT engine (used by abi.cu).
+#pragma once
+#include <stdint.h>
+
+#include "runtime.cuh"
+
+namespace zk {
+
+// compute_batched_ntt on device memory: natural order in and out, in place.
+void ntt_batch_device(DeviceCtx &c, uint64_t *inout, uint32_t lg, uint64_t batches, bool inverse, bool with_coset);
+
+// compute_batched_lde on device memory: column-major natural-order evaluations.
+void lde_batch_device(DeviceCtx &c, uint64_t *out, const uint64_t *in, uint32_t lg_n, uint32_t rate, uint64_t batches,
+                      bool inverse, bool with_coset);
+
+// Fused LDE + bit-reverse + transpose: rows[r * cols + b] = LDE_b[rev_{lg_n+rate}(r)]
+// (the leaf-major matrix compute_transpose_rev would produce).  `scratch` may
+// be null (allocated on the stream) or hold lde_rows_scratch_elems() words.
+void lde_rows_device(DeviceCtx &c, uint64_t *rows, const uint64_t *coeffs, uint32_t lg_n, uint32_t rate, uint64_t cols,
+                     uint64_t coset_gen, uint64_t *scratch);
+uint64_t lde_rows_scratch_elems(uint32_t lg_n, uint32_t rate, uint64_t cols);
+
+void transpose_rev_device(DeviceCtx &c, uint64_t *out, const uint64_t *in, uint32_t lg, uint64_t cols);
+
+void salt_device(DeviceCtx &c, uint64_t *out, uint64_t count);
+
+// Merkle forest on device memory, launched on `stream`; returns false (with a
+// message in err) on invalid geometry or an unsupported hash.
+bool merkle_device(uint64_t *digests, uint64_t *caps, const uint64_t *leaves, uint64_t n_digests, uint64_t n_caps,
+                   uint64_t n_leaves, uint64_t leaf_size, uint64_t cap_height, uint64_t hash_type, cudaStream_t stream,
+                   std::string &err);
+
+bool merkle_geometry_ok(uint64_t n_digests, uint64_t n_caps, uint64_t n_leaves, uint64_t cap_height, std::string &err);
+
+}  // namespace zk

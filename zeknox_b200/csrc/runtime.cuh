@@ -1,0 +1,88 @@
+// runtime.cuh -- per-GPU state of the library.
+//
+// Replaces zeknox's native/utils/gpu_t.cuh + all_gpus.cu device registry and
+// the global twiddle/coset arrays of native/ntt/ntt.cu:25-27.  Differences:
+//   * tables are built by parallel kernels (the reference runs a serial
+//     <<<1,1>>> kernel per table) and lazily on first use, so a missing
+//     init_twiddle_factors() is not a null dereference;
+//   * every call takes the device's mutex, so concurrent calls from several
+//     host threads are serialised instead of racing on shared state;
+//   * temporaries come from the stream-ordered allocator on the device's
+//     stream and are returned on the same stream.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <map>
+#include <mutex>
+#include <stdexcept>
+#include <string>
+#include <tuple>
+#include <vector>
+
+namespace zk {
+
+// CUDA failure: code is the negated cudaError_t (native/utils/exception.cuh:21).
+struct cuda_failure : std::runtime_error {
+    int code;
+    cuda_failure(int c, const std::string &m) : std::runtime_error(m), code(c) {}
+};
+// Argument failure: code is +cudaErrorInvalidValue (native/ntt/ntt.cu:256,318,480).
+struct arg_failure : std::runtime_error {
+    int code;
+    explicit arg_failure(const std::string &m) : std::runtime_error(m), code((int)cudaErrorInvalidValue) {}
+};
+
+void cuda_check(cudaError_t e, const char *what, const char *file, int line);
+#define ZK_CUDA(x) ::zk::cuda_check((x), #x, __FILE__, __LINE__)
+
+struct DeviceCtx {
+    int id = 0;
+    cudaStream_t stream = nullptr;
+    std::recursive_mutex mu;
+    int sm_count = 0;
+
+    // twiddle tables: tw[inv][lg] = w_{2^lg}^t for t < 2^lg (w = OMEGA or OMEGA_INV)
+    uint64_t *tw[2][33] = {};
+    // coset powers g^i, i < 2^coset_lg (init_coset)
+    uint64_t *coset = nullptr;
+    uint32_t coset_lg = 0;
+    uint64_t coset_gen = 7;
+    bool coset_set = false;
+    // LDE coset tables: (lg_n, rate, g) -> (g * w_N^c)^j
+    std::map<std::tuple<uint32_t, uint32_t, uint64_t>, uint64_t *> lde_tabs;
+
+    const uint64_t *twiddles(uint32_t lg, bool inverse);
+    const uint64_t *coset_powers(uint32_t lg);  // builds g^i up to 2^lg if needed
+    const uint64_t *lde_table(uint32_t lg_n, uint32_t rate, uint64_t g);
+    void set_coset(uint32_t lg, uint64_t gen);
+
+    uint64_t *alloc(size_t bytes);
+    void free(void *p);
+    void sync();
+};
+
+int device_count();
+DeviceCtx &device(size_t id);  // throws arg_failure for a bad id; makes it current
+
+// RAII temporary on the device stream
+struct DevBuf {
+    DeviceCtx *ctx = nullptr;
+    uint64_t *p = nullptr;
+    DevBuf() = default;
+    DevBuf(DeviceCtx &c, size_t elems) : ctx(&c), p(elems ? c.alloc(elems * 8) : nullptr) {}
+    DevBuf(const DevBuf &) = delete;
+    DevBuf &operator=(const DevBuf &) = delete;
+    ~DevBuf()
+    {
+        if (p) ctx->free(p);
+    }
+};
+
+uint32_t ilog2_exact(uint64_t x);  // -1u if x is not a power of two
+
+// Count of kernels this library has launched (diagnostics: zeknox_launch_count).
+void note_launch(uint64_t n = 1);
+uint64_t launch_count();
+
+}  // namespace zk
