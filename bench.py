@@ -299,6 +299,27 @@ def run_ours(args, rank, world):
         print(json.dumps(line), flush=True)
 
 
+def run_stage(args):
+    """One stage of the workload at 2^lg_n coefficients per column, for ncu captures."""
+    import torch
+    import zeknox_b200 as zk
+    lg = args.lg_n
+    n, N = 1 << lg, 1 << (lg + RATE)
+    inp = torch.from_numpy(field_data(5, COLS * n).view(np.int64).copy()).cuda()
+    leaves = torch.empty(N * COLS, dtype=torch.int64, device="cuda")
+    n_dig, n_cap = zk.merkle_sizes(N, CAP)
+    dig = torch.empty(n_dig * 4, dtype=torch.int64, device="cuda")
+    caps = torch.empty(n_cap * 4, dtype=torch.int64, device="cuda")
+    zk.lde_rows(0, leaves, inp, lg, RATE, COLS)
+    for _ in range(args.warmup + args.steps):
+        if args.only == "lde":
+            zk.lde_rows(0, leaves, inp, lg, RATE, COLS)
+        else:
+            zk.fill_digests_buf_linear_gpu(dig, caps, leaves, N, COLS, CAP, HASH)
+    torch.cuda.synchronize()
+    print("stage %s lg_n %d done, %d launches" % (args.only, lg, zk.launch_count()))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -307,11 +328,16 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--cpu-lg", type=int, default=12, help="log2 coefficients per column of the CPU sample")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    ap.add_argument("--lg-n", type=int, default=LG_N, help="log2 coefficients per column (profiling cases)")
+    ap.add_argument("--only", default=None, choices=["lde", "merkle"],
+                    help="profiling: run only this stage for warmup+steps iterations and exit")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     if args.impl == "reference":
         return run_reference(args, rank, world)
+    if args.only:
+        return run_stage(args)
     if world > 1:
         import datetime
 

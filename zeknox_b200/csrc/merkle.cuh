@@ -56,19 +56,21 @@ __global__ void __launch_bounds__(T) merkle_leaf_kernel(const uint64_t *__restri
     const uint64_t i = i0 + t;
     uint64_t d[4];
     if (i < g.n_leaves) {
-        leaf_hash<H>(leaves + i * g.leaf_size, g.leaf_size, d);
-        if (g.sub_leaves == 1) {
-            // caps == leaves: the leaf hashes are the caps, digests untouched
+        // caps == leaves: the leaf hashes are the caps, digests untouched
+        uint64_t *dst = g.sub_leaves == 1 ? caps + 4 * i : digests + 4 * merkle_node_index(g, i, 0);
+        if (H == HASH_KECCAK && g.leaf_size < 4) {
+            // Keccak copies a < 4-word leaf and leaves the other digest words as
+            // they are in the output buffer (native/keccak/keccak.cu:118-121)
 #pragma unroll
-            for (int q = 0; q < 4; q++) caps[4 * i + q] = d[q];
-            return;
+            for (int q = 0; q < 4; q++) d[q] = dst[q];
         }
-        uint64_t di = merkle_node_index(g, i, 0);
+        leaf_hash<H>(leaves + i * g.leaf_size, g.leaf_size, d);
 #pragma unroll
         for (int q = 0; q < 4; q++) {
-            digests[4 * di + q] = d[q];
+            dst[q] = d[q];
             node[t][q] = d[q];
         }
+        if (g.sub_leaves == 1) return;
     }
     if (g.sub_leaves == 1) return;
     // Levels fully inside this CTA: height u has (L >> u) >= 2 nodes per subtree.
