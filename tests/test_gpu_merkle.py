@@ -18,7 +18,7 @@ def run_gpu(leaves_np, nl, ls, ch, h):
     cap = empty_dev(n_cap * 4)
     zk.fill_digests_buf_linear_gpu(dig, cap, leaves, nl, ls, ch, h)
     torch.cuda.synchronize()
-    return to_np(dig).reshape(-1, 4)[:n_dig], to_np(cap).reshape(-1, 4)
+    return to_np(dig)[:n_dig * 4].reshape(-1, 4), to_np(cap).reshape(-1, 4)
 
 
 @pytest.mark.parametrize("name", list(HASHES))

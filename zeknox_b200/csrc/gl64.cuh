@@ -69,18 +69,146 @@ ZK_HD uint64_t gl_reduce128(uint64_t lo, uint64_t hi)
     return gl_canon(t2);
 }
 
-// Reduce lo + 2^64*hi with hi < 2^32 (a "u96" value).
-ZK_HD uint64_t gl_reduce96(uint64_t lo, uint64_t hi)
+// Reduce lo + 2^64*hi with hi < 2^32 (a "u96" value) to a 64-bit
+// representative (_nc) or the canonical value.
+ZK_HD uint64_t gl_reduce96_nc(uint64_t lo, uint64_t hi)
 {
-    uint64_t t1 = (hi << 32) - hi;              // hi * EPS
+    uint64_t t1 = (hi << 32) - hi;              // hi * EPS < p
     uint64_t t2 = lo + t1;
-    if (t2 < t1) t2 += GL_EPS;
-    return gl_canon(t2);
+    if (t2 < t1) t2 += GL_EPS;                  // wrapped: lo + t1 - p < 2^64
+    return t2;
+}
+ZK_HD uint64_t gl_reduce96(uint64_t lo, uint64_t hi) { return gl_canon(gl_reduce96_nc(lo, hi)); }
+
+// ------------------------------------------------------------------------
+// Lazily reduced arithmetic ("nc" = any 64-bit representative, not
+// necessarily < p).  On the device these are 32-bit PTX carry chains: the
+// 64x64 product is 8 multiply-adds, the reduction of lo + 2^64*(h0 + 2^32*h1)
+// to lo - h1 + EPS*h0 is 13 integer ops with no compares or selects.
+
+#ifdef __CUDA_ARCH__
+__device__ __forceinline__ void mul_wide(uint64_t a, uint64_t b, uint32_t &r0, uint32_t &r1, uint32_t &r2, uint32_t &r3)
+{
+    const uint32_t a0 = (uint32_t)a, a1 = (uint32_t)(a >> 32), b0 = (uint32_t)b, b1 = (uint32_t)(b >> 32);
+    asm("{\n\t"
+        "mul.lo.u32      %0, %4, %6;\n\t"
+        "mul.hi.u32      %1, %4, %6;\n\t"
+        "mad.lo.cc.u32   %1, %5, %6, %1;\n\t"
+        "madc.hi.u32     %2, %5, %6, 0;\n\t"
+        "mad.lo.cc.u32   %1, %4, %7, %1;\n\t"
+        "madc.hi.cc.u32  %2, %4, %7, %2;\n\t"
+        "addc.u32        %3, 0, 0;\n\t"
+        "mad.lo.cc.u32   %2, %5, %7, %2;\n\t"
+        "madc.hi.u32     %3, %5, %7, %3;\n\t"
+        "}"
+        : "=&r"(r0), "=&r"(r1), "=&r"(r2), "=&r"(r3)
+        : "r"(a0), "r"(a1), "r"(b0), "r"(b1));
 }
 
-ZK_HD uint64_t gl_mul(uint64_t a, uint64_t b) { return gl_reduce128(a * b, mulhi64(a, b)); }
+__device__ __forceinline__ void sqr_wide(uint64_t a, uint32_t &r0, uint32_t &r1, uint32_t &r2, uint32_t &r3)
+{
+    // a^2 = a0^2 + 2^33 a0 a1 + 2^64 a1^2
+    const uint32_t a0 = (uint32_t)a, a1 = (uint32_t)(a >> 32);
+    uint32_t m0, m1;
+    asm("{\n\t"
+        "mul.lo.u32      %4, %6, %7;\n\t"
+        "mul.hi.u32      %5, %6, %7;\n\t"
+        "mul.lo.u32      %0, %6, %6;\n\t"
+        "mul.hi.u32      %1, %6, %6;\n\t"
+        "mul.lo.u32      %2, %7, %7;\n\t"
+        "mul.hi.u32      %3, %7, %7;\n\t"
+        "add.cc.u32      %1, %1, %4;\n\t"
+        "addc.cc.u32     %2, %2, %5;\n\t"
+        "addc.u32        %3, %3, 0;\n\t"
+        "add.cc.u32      %1, %1, %4;\n\t"
+        "addc.cc.u32     %2, %2, %5;\n\t"
+        "addc.u32        %3, %3, 0;\n\t"
+        "}"
+        : "=&r"(r0), "=&r"(r1), "=&r"(r2), "=&r"(r3), "=&r"(m0), "=&r"(m1)
+        : "r"(a0), "r"(a1));
+}
 
-ZK_HD uint64_t gl_sqr(uint64_t a) { return gl_mul(a, a); }
+// r1:r0 + 2^64 (r2 + 2^32 r3)  ->  64-bit representative
+__device__ __forceinline__ uint64_t reduce_nc(uint32_t r0, uint32_t r1, uint32_t r2, uint32_t r3)
+{
+    uint32_t t0, t1, b, e0, e1, c;
+    asm("{\n\t"
+        "sub.cc.u32      %0, %6, %9;\n\t"   // t = lo - h1
+        "subc.cc.u32     %1, %7, 0;\n\t"
+        "subc.u32        %2, 0, 0;\n\t"     // b = borrow ? 0xffffffff : 0
+        "sub.cc.u32      %0, %0, %2;\n\t"   // borrow: t -= EPS (t + 1 - 2^32)
+        "subc.u32        %1, %1, 0;\n\t"
+        "sub.cc.u32      %3, 0, %8;\n\t"    // e = h0 * EPS = 2^32 h0 - h0
+        "subc.u32        %4, %8, 0;\n\t"
+        "add.cc.u32      %0, %0, %3;\n\t"   // t += e
+        "addc.cc.u32     %1, %1, %4;\n\t"
+        "addc.u32        %5, 0, 0;\n\t"     // c = carry
+        "neg.s32         %5, %5;\n\t"       // carry: t += EPS
+        "add.cc.u32      %0, %0, %5;\n\t"
+        "addc.u32        %1, %1, 0;\n\t"
+        "}"
+        : "=&r"(t0), "=&r"(t1), "=&r"(b), "=&r"(e0), "=&r"(e1), "=&r"(c)
+        : "r"(r0), "r"(r1), "r"(r2), "r"(r3));
+    return ((uint64_t)t1 << 32) | t0;
+}
+#endif
+
+// a * b for any 64-bit representatives; result any 64-bit representative.
+ZK_HD uint64_t gl_mul_nc(uint64_t a, uint64_t b)
+{
+#ifdef __CUDA_ARCH__
+    uint32_t r0, r1, r2, r3;
+    mul_wide(a, b, r0, r1, r2, r3);
+    return reduce_nc(r0, r1, r2, r3);
+#else
+    unsigned __int128 x = (unsigned __int128)a * b;
+    return gl_reduce128((uint64_t)x, (uint64_t)(x >> 64));
+#endif
+}
+
+ZK_HD uint64_t gl_sqr_nc(uint64_t a)
+{
+#ifdef __CUDA_ARCH__
+    uint32_t r0, r1, r2, r3;
+    sqr_wide(a, r0, r1, r2, r3);
+    return reduce_nc(r0, r1, r2, r3);
+#else
+    return gl_mul_nc(a, a);
+#endif
+}
+
+// a * b + c (c any 64-bit value) reduced once.
+ZK_HD uint64_t gl_mul_add_nc(uint64_t a, uint64_t b, uint64_t c)
+{
+#ifdef __CUDA_ARCH__
+    uint32_t r0, r1, r2, r3;
+    mul_wide(a, b, r0, r1, r2, r3);
+    asm("{\n\t"
+        "add.cc.u32   %0, %0, %4;\n\t"
+        "addc.cc.u32  %1, %1, %5;\n\t"
+        "addc.cc.u32  %2, %2, 0;\n\t"
+        "addc.u32     %3, %3, 0;\n\t"
+        "}"
+        : "+r"(r0), "+r"(r1), "+r"(r2), "+r"(r3)
+        : "r"((uint32_t)c), "r"((uint32_t)(c >> 32)));
+    return reduce_nc(r0, r1, r2, r3);
+#else
+    unsigned __int128 x = (unsigned __int128)a * b + c;
+    return gl_reduce128((uint64_t)x, (uint64_t)(x >> 64));
+#endif
+}
+
+// a + b where at least one operand is < p: one wrap correction suffices
+// (a + b - 2^64 + EPS = a + b - p < 2^64).
+ZK_HD uint64_t gl_add_nc(uint64_t a, uint64_t b)
+{
+    uint64_t s = a + b;
+    return s + (s < a ? GL_EPS : 0);
+}
+
+ZK_HD uint64_t gl_mul(uint64_t a, uint64_t b) { return gl_canon(gl_mul_nc(a, b)); }
+
+ZK_HD uint64_t gl_sqr(uint64_t a) { return gl_canon(gl_sqr_nc(a)); }
 
 // a * 2^s for 0 <= s < 64: the 128-bit shift then the special reduction.
 ZK_HD uint64_t gl_mul_pow2_lt64(uint64_t a, unsigned s)
@@ -121,6 +249,15 @@ ZK_HD uint64_t gl_sbox7(uint64_t x)
     uint64_t x4 = gl_sqr(x2);
     uint64_t x3 = gl_mul(x2, x);
     return gl_mul(x3, x4);
+}
+
+// Same S-box on lazily reduced values.
+ZK_HD uint64_t gl_sbox7_nc(uint64_t x)
+{
+    uint64_t x2 = gl_sqr_nc(x);
+    uint64_t x4 = gl_sqr_nc(x2);
+    uint64_t x3 = gl_mul_nc(x2, x);
+    return gl_mul_nc(x3, x4);
 }
 
 ZK_HD uint32_t bitrev32(uint32_t x, unsigned bits)

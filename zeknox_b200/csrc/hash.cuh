@@ -82,8 +82,22 @@ struct Acc96 {
     {
         uint64_t l = lo + (hi << 32);
         uint64_t h = (hi >> 32) + (l < lo);
-        return gl_reduce96(l, h);
+        return gl_reduce96_nc(l, h);
     }
+};
+
+// Sum of 64-bit values with the carries counted: lo + 2^64 * c.
+struct Sum64 {
+    uint64_t lo;
+    uint32_t c;
+    ZK_HD void set(uint64_t x) { lo = x; c = 0; }
+    ZK_HD void add(uint64_t x)
+    {
+        lo += x;
+        c += lo < x;
+    }
+    // lo + c * EPS, one wrap correction (c * EPS < 2^36)
+    ZK_HD uint64_t reduce() const { return gl_add_nc(lo, ((uint64_t)c << 32) - c); }
 };
 
 // ----------------------------------------------------------------- Poseidon
@@ -109,27 +123,29 @@ ZK_HD void poseidon_mds(uint64_t s[12])
     for (int i = 0; i < 12; i++) s[i] = t[i];
 }
 
-ZK_HD void poseidon_permute(uint64_t s[12])
+// Lanes hold any 64-bit representative between rounds (round constants are
+// < p, so one wrap correction suffices when adding them); the caller
+// canonicalises the digest.
+ZK_HD void poseidon_full_round(uint64_t s[12], int r)
 {
 #pragma unroll
-    for (int r = 0; r < 4; r++) {
-#pragma unroll
-        for (int i = 0; i < 12; i++) s[i] = gl_sbox7(gl_add(s[i], ZKC(POSEIDON_RC)[12 * r + i]));
-        poseidon_mds(s);
-    }
-#pragma unroll 2
+    for (int i = 0; i < 12; i++) s[i] = gl_sbox7_nc(gl_add_nc(s[i], ZKC(POSEIDON_RC)[12 * r + i]));
+    poseidon_mds(s);
+}
+
+ZK_HD void poseidon_permute(uint64_t s[12])
+{
+#pragma unroll 1
+    for (int r = 0; r < 4; r++) poseidon_full_round(s, r);
+#pragma unroll 1
     for (int r = 4; r < 26; r++) {
-        s[0] = gl_sbox7(gl_add(s[0], ZKC(POSEIDON_RC)[12 * r]));
+        s[0] = gl_sbox7_nc(gl_add_nc(s[0], ZKC(POSEIDON_RC)[12 * r]));
 #pragma unroll
-        for (int i = 1; i < 12; i++) s[i] = gl_add(s[i], ZKC(POSEIDON_RC)[12 * r + i]);
+        for (int i = 1; i < 12; i++) s[i] = gl_add_nc(s[i], ZKC(POSEIDON_RC)[12 * r + i]);
         poseidon_mds(s);
     }
-#pragma unroll
-    for (int r = 26; r < 30; r++) {
-#pragma unroll
-        for (int i = 0; i < 12; i++) s[i] = gl_sbox7(gl_add(s[i], ZKC(POSEIDON_RC)[12 * r + i]));
-        poseidon_mds(s);
-    }
+#pragma unroll 1
+    for (int r = 26; r < 30; r++) poseidon_full_round(s, r);
 }
 
 // ----------------------------------------------------------------- Poseidon2
@@ -166,37 +182,34 @@ ZK_HD void p2_external(uint64_t s[12])
     for (int i = 0; i < 12; i++) s[i] = y[i];
 }
 
+ZK_HD void p2_full_round(uint64_t s[12], int r)
+{
+#pragma unroll
+    for (int i = 0; i < 12; i++) s[i] = gl_sbox7_nc(gl_add_nc(s[i], ZKC(POSEIDON2_RC)[12 * r + i]));
+    p2_external(s);
+}
+
+// Lanes hold any 64-bit representative between layers; digests are
+// canonicalised by the sponge.
 ZK_HD void poseidon2_permute(uint64_t s[12])
 {
     p2_external(s);
-#pragma unroll
-    for (int r = 0; r < 4; r++) {
-#pragma unroll
-        for (int i = 0; i < 12; i++) s[i] = gl_sbox7(gl_add(s[i], ZKC(POSEIDON2_RC)[12 * r + i]));
-        p2_external(s);
-    }
-#pragma unroll 2
+#pragma unroll 1
+    for (int r = 0; r < 4; r++) p2_full_round(s, r);
+#pragma unroll 1
     for (int r = 4; r < 26; r++) {
-        s[0] = gl_sbox7(gl_add(s[0], ZKC(POSEIDON2_RC)[12 * r]));
-        uint64_t sum = s[0];
+        s[0] = gl_sbox7_nc(gl_add_nc(s[0], ZKC(POSEIDON2_RC)[12 * r]));
+        Sum64 acc;
+        acc.set(s[0]);
 #pragma unroll
-        for (int i = 1; i < 12; i++) sum = gl_add(sum, s[i]);
+        for (int i = 1; i < 12; i++) acc.add(s[i]);
+        const uint64_t sum = acc.reduce();
         // s_i * d_i + sum as one 128-bit value, reduced once
 #pragma unroll
-        for (int i = 0; i < 12; i++) {
-            uint64_t d = ZKC(POSEIDON2_DIAG)[i];
-            uint64_t lo = s[i] * d, hi = mulhi64(s[i], d);
-            lo += sum;
-            hi += lo < sum;
-            s[i] = gl_reduce128(lo, hi);
-        }
+        for (int i = 0; i < 12; i++) s[i] = gl_mul_add_nc(s[i], ZKC(POSEIDON2_DIAG)[i], sum);
     }
-#pragma unroll
-    for (int r = 26; r < 30; r++) {
-#pragma unroll
-        for (int i = 0; i < 12; i++) s[i] = gl_sbox7(gl_add(s[i], ZKC(POSEIDON2_RC)[12 * r + i]));
-        p2_external(s);
-    }
+#pragma unroll 1
+    for (int r = 26; r < 30; r++) p2_full_round(s, r);
 }
 
 // ----------------------------------------------------------------- Monolith
@@ -236,7 +249,7 @@ ZK_HD void mono_concrete(uint64_t s[12], const uint32_t hi[12], int round)
         // value = lo + 2^32*hi + 2^64*top
         uint64_t l = a.lo + (a.hi << 32);
         uint64_t h = (a.hi >> 32) + (l < a.lo) + top;
-        t[r] = gl_reduce96(l, h);
+        t[r] = gl_reduce96_nc(l, h);
     }
 #pragma unroll
     for (int i = 0; i < 12; i++) s[i] = t[i];
@@ -250,11 +263,12 @@ ZK_HD void monolith_permute(uint64_t s[12])
     mono_concrete(s, hi, 0);
 #pragma unroll 1
     for (int r = 1; r <= 6; r++) {
+        // Bars act on the bits of the canonical value
 #pragma unroll
-        for (int i = 0; i < 4; i++) s[i] = mono_bar(s[i]);
+        for (int i = 0; i < 4; i++) s[i] = mono_bar(gl_canon(s[i]));
         uint64_t sq[11];
 #pragma unroll
-        for (int i = 0; i < 11; i++) sq[i] = gl_sqr(gl_canon(s[i]));
+        for (int i = 0; i < 11; i++) sq[i] = gl_sqr_nc(s[i]);
         hi[0] = 0;
 #pragma unroll
         for (int i = 1; i < 12; i++) {

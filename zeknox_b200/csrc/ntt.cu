@@ -31,6 +31,7 @@ static void launch_one(const NttPassArgs &a, uint64_t grid, uint32_t smem, cudaS
     static bool attr = false;
     if (!attr) {
         ZK_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, PASS_TILE * 8));
+        ZK_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared));
         attr = true;
     }
     k<<<(unsigned)grid, PASS_NT, smem, s>>>(a);

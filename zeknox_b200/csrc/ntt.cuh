@@ -98,10 +98,11 @@ __device__ __forceinline__ void dif_substep(uint64_t *sm, uint32_t tile_elems, u
     const uint32_t R_cur = 1u << log_rcur;
     const uint32_t Q = R_cur >> LOGE;
     const uint32_t tasks = tile_elems >> LOGE;
+    const uint32_t log_q = log_rcur - LOGE;
     for (uint32_t t = threadIdx.x; t < tasks; t += NT) {
         uint32_t m_lo = t & (Q - 1);
-        uint32_t blk = t >> (log_rcur - LOGE);  // block of R_cur (across groups)
-        uint32_t base = blk * R_cur + m_lo;
+        uint32_t blk = t >> log_q;  // block of R_cur (across groups)
+        uint32_t base = (blk << log_rcur) + m_lo;
         uint64_t x[E];
 #pragma unroll
         for (int e = 0; e < E; e++) x[e] = sm[swz(base + e * Q)];
@@ -130,60 +131,65 @@ __device__ __forceinline__ void dif_substep(uint64_t *sm, uint32_t tile_elems, u
 //     consecutive source columns x W positions, so every output leaf row gets
 //     16 consecutive 8-byte words.
 template <int LOGR, int INV, int NT, int TILE, int LOADM, int STOREM>
-__global__ void __launch_bounds__(NT) ntt_pass_kernel(NttPassArgs a)
+__global__ void __launch_bounds__(NT, 2) ntt_pass_kernel(NttPassArgs a)
 {
     extern __shared__ uint64_t sm[];
     constexpr uint32_t R = 1u << LOGR;
-    constexpr uint32_t CW = 16;
-    const uint32_t S = 1u << a.s_lo;
+    constexpr uint32_t LOG_CW = 4, CW = 1u << LOG_CW;
+    constexpr uint32_t LOG_TILE = __builtin_ctz(TILE);
+    // all sizes are powers of two: index math is shifts and masks
+    const uint32_t s_lo = a.s_lo;
+    const uint32_t S = 1u << s_lo;
     const uint64_t n = 1ULL << a.L;
-    const uint64_t M = (uint64_t)R << a.s_lo;
+    const uint32_t log_m = s_lo + LOGR;  // log2 M, M = R * S
     const uint32_t rmask = (1u << a.rate) - 1;
-    const uint32_t W = (STOREM == STORE_ROWS) ? (uint32_t)(n < TILE / CW ? n : TILE / CW) : 0;
-    const uint32_t tile = (STOREM == STORE_ROWS) ? CW * W : (uint32_t)(n < TILE ? n : TILE);
-    const uint32_t G = tile / R;    // groups per tile
-    const uint32_t GW = W / R;      // groups per virtual column (row tiles)
+    const uint32_t log_w = (STOREM == STORE_ROWS) ? (a.L < LOG_TILE - LOG_CW ? a.L : LOG_TILE - LOG_CW) : 0;
+    const uint32_t log_tile = (STOREM == STORE_ROWS) ? LOG_CW + log_w : (a.L < LOG_TILE ? a.L : LOG_TILE);
+    const uint32_t tile = 1u << log_tile;
+    const uint32_t log_g = log_tile - LOGR;       // groups per tile
+    const uint32_t log_gw = log_w - LOGR;         // groups per virtual column (row tiles)
 
     uint64_t v0, pos0;
     if (STOREM == STORE_ROWS) {
-        const uint64_t per_v = n / W;
+        const uint32_t log_per_v = a.L - log_w;
         const uint64_t t = blockIdx.x;
-        const uint64_t posblk = t % per_v, cg = t / per_v;
-        const uint64_t ncg = (a.cols + CW - 1) / CW;
-        const uint64_t coset = cg / ncg, colg = cg % ncg;
-        v0 = ((colg * CW) << a.rate) | coset;
-        pos0 = posblk * W;
+        const uint64_t posblk = t & ((1ULL << log_per_v) - 1), cg = t >> log_per_v;
+        const uint64_t ncg = (a.cols + CW - 1) >> LOG_CW;
+        const uint64_t coset = cg / ncg, colg = cg - coset * ncg;
+        v0 = ((colg << LOG_CW) << a.rate) | coset;
+        pos0 = posblk << log_w;
     } else {
-        const uint64_t tiles_per_v = n / tile;
-        v0 = blockIdx.x / tiles_per_v;
-        pos0 = (blockIdx.x % tiles_per_v) * tile;
+        const uint32_t log_tpv = a.L - log_tile;
+        v0 = (uint64_t)blockIdx.x >> log_tpv;
+        pos0 = ((uint64_t)blockIdx.x & ((1ULL << log_tpv) - 1)) << log_tile;
     }
+    const uint64_t gid0 = pos0 >> LOGR;
 
     // tile element (group g, member m) -> (virtual column, position)
     auto gpos = [&](uint32_t g, uint32_t m, uint64_t &vcol, uint64_t &pos) {
         if (STOREM == STORE_ROWS) {
-            const uint32_t c = g / GW, gg = g % GW;
+            const uint32_t c = g >> log_gw, gg = g & ((1u << log_gw) - 1);
             vcol = v0 + ((uint64_t)c << a.rate);
-            pos = pos0 + (uint64_t)gg * R + m;
+            pos = pos0 + ((uint64_t)gg << LOGR) + m;
         } else {
             vcol = v0;
-            const uint64_t gid = pos0 / R + g;
-            pos = (gid >> a.s_lo) * M + (uint64_t)m * S + (gid & (S - 1));
+            const uint64_t gid = gid0 + g;
+            pos = ((gid >> s_lo) << log_m) + ((uint64_t)m << s_lo) + (gid & (S - 1));
         }
     };
     // linear index e -> (g, m) so that consecutive e are consecutive addresses
     auto split_in = [&](uint32_t e, uint32_t &g, uint32_t &m) {
         if (STOREM == STORE_ROWS) {
-            const uint32_t c = e / W, w = e % W;
-            g = c * GW + w / R;
-            m = w % R;
-        } else if (S >= G) {
-            g = e % G;
-            m = e / G;
+            const uint32_t c = e >> log_w, w = e & ((1u << log_w) - 1);
+            g = (c << log_gw) + (w >> LOGR);
+            m = w & (R - 1);
+        } else if (s_lo >= log_g) {
+            g = e & ((1u << log_g) - 1);
+            m = e >> log_g;
         } else {
-            const uint32_t blk = e / (uint32_t)M, rem = e % (uint32_t)M;
-            m = rem >> a.s_lo;
-            g = blk * S + (rem & (S - 1));
+            const uint32_t blk = e >> log_m, rem = e & ((1u << log_m) - 1);
+            m = rem >> s_lo;
+            g = (blk << s_lo) + (rem & (S - 1));
         }
     };
 
@@ -201,12 +207,12 @@ __global__ void __launch_bounds__(NT) ntt_pass_kernel(NttPassArgs a)
             } else if (LOADM == LOAD_SCALE) {
                 val = gl_mul(a.src[vcol * a.src_stride + pos], __ldg(a.tab + pos));
             } else if (LOADM == LOAD_COSETS) {
-                val = gl_mul(a.src[(vcol >> a.rate) * a.src_stride + pos], __ldg(a.tab + (vcol & rmask) * n + pos));
+                val = gl_mul(a.src[(vcol >> a.rate) * a.src_stride + pos], __ldg(a.tab + ((vcol & rmask) << a.L) + pos));
             } else {  // LOAD_EXTEND
                 val = pos < a.n_src ? a.src[vcol * a.src_stride + pos] : 0;
             }
         }
-        sm[swz(g * R + m)] = val;
+        sm[swz((g << LOGR) + m)] = val;
     }
     __syncthreads();
 
@@ -226,15 +232,15 @@ __global__ void __launch_bounds__(NT) ntt_pass_kernel(NttPassArgs a)
     for (uint32_t e = threadIdx.x; e < tile; e += NT) {
         uint32_t g, m;
         if (STOREM == STORE_ROWS) {
-            const uint32_t w = e / CW, c = e % CW;  // consecutive e -> consecutive columns of one row
-            g = c * GW + w / R;
-            m = w % R;
+            const uint32_t w = e >> LOG_CW, c = e & (CW - 1);  // consecutive e -> consecutive columns of one row
+            g = (c << log_gw) + (w >> LOGR);
+            m = w & (R - 1);
         } else {
             split_in(e, g, m);
         }
         uint64_t vcol, pos;
         gpos(g, m, vcol, pos);
-        uint64_t val = sm[swz(g * R + m)];
+        uint64_t val = sm[swz((g << LOGR) + m)];
         if (S > 1) {
             const uint64_t o = pos & (S - 1);
             const uint64_t f = bitrev32(m, LOGR);
