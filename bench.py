@@ -320,6 +320,141 @@ def run_stage(args):
     print("stage %s lg_n %d done, %d launches" % (args.only, lg, zk.launch_count()))
 
 
+def dev_field(numel, seed):
+    """Seeded uniform field elements generated on the GPU (int64 bit patterns)."""
+    import torch
+    g = torch.Generator(device="cuda")
+    g.manual_seed(seed)
+    x = torch.randint(-(1 << 63), (1 << 63) - 1, (numel,), dtype=torch.int64, device="cuda", generator=g)
+    # u64 values >= p are the int64 values in [-(2^32 - 1), -1]: subtract p (= add 2^32 - 1)
+    big = (x < 0) & (x >= -((1 << 32) - 1))
+    return torch.where(big, x + ((1 << 32) - 1), x)
+
+
+def uneven_jobs(count=64, seed=3):
+    """The uneven-batch workload: log2 size U{10..20}, columns U{8..400},
+    rate_bits U{1,2,3}, Poseidon, cap_height min(4, log2 leaves)."""
+    rng = np.random.default_rng(seed)
+    jobs = []
+    for j in range(count):
+        lg = int(rng.integers(10, 21))
+        cols = int(rng.integers(8, 401))
+        rate = int(rng.integers(1, 4))
+        jobs.append({"lg_n": lg, "cols": cols, "rate": rate, "cap": min(4, lg + rate), "hash": 0, "seed": 3000 + j})
+    return jobs
+
+
+def run_batch(args):
+    """Uneven batch: one graph per memory wave (batched) vs one synchronous C-ABI
+    call per stage per job (plain: compute_batched_lde -> compute_transpose_rev ->
+    fill_digests_buf_linear_gpu_with_gpu_ptr)."""
+    import torch
+    import zeknox_b200 as zk
+    torch.cuda.set_device(0)
+    jobs = uneven_jobs()
+    budget = int(args.budget_gb * (1 << 30))
+    waves, cur, used = [], [], 0
+    for jb in jobs:
+        n, N = 1 << jb["lg_n"], 1 << (jb["lg_n"] + jb["rate"])
+        need = 8 * (n * jb["cols"] + N * jb["cols"] + 2 * N * 4)
+        if cur and used + need > budget:
+            waves.append(cur)
+            cur, used = [], 0
+        cur.append(jb)
+        used += need
+    waves.append(cur)
+    total_elems = sum((1 << (j["lg_n"] + j["rate"])) * j["cols"] for j in jobs)
+    t_batch, t_plain, max_job = 0.0, 0.0, 0
+    for wave in waves:
+        bufs, cjobs = [], []
+        for jb in wave:
+            n, N = 1 << jb["lg_n"], 1 << (jb["lg_n"] + jb["rate"])
+            inp = dev_field(n * jb["cols"], jb["seed"])
+            leaves = torch.empty(N * jb["cols"], dtype=torch.int64, device="cuda")
+            n_dig, n_cap = zk.merkle_sizes(N, jb["cap"])
+            dig = torch.empty(max(n_dig, 1) * 4, dtype=torch.int64, device="cuda")
+            caps = torch.empty(n_cap * 4, dtype=torch.int64, device="cuda")
+            bufs.append((inp, leaves, dig, caps, n_dig, n_cap))
+            cjobs.append(zk.commit_job(jb["lg_n"], jb["rate"], jb["cols"], jb["cap"], jb["hash"], inp, leaves, dig, caps))
+            max_job = max(max_job, N * jb["cols"])
+        zk.commit_batch(0, cjobs)  # capture
+        torch.cuda.synchronize()
+        caps_b = [b[3].clone() for b in bufs]
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        for _ in range(args.steps):
+            a.record()
+            zk.commit_batch(0, cjobs)
+            b.record()
+            torch.cuda.synchronize()
+            t_batch += a.elapsed_time(b) / args.steps
+        # plain path, same jobs and buffers
+        for _ in range(args.steps):
+            a.record()
+            for jb, (inp, leaves, dig, caps, n_dig, n_cap) in zip(wave, bufs):
+                N = 1 << (jb["lg_n"] + jb["rate"])
+                ev = torch.empty(N * jb["cols"], dtype=torch.int64, device="cuda")
+                zk.lde_batch(0, ev, inp, jb["lg_n"], jb["cols"], jb["rate"], with_coset=True)
+                zk.transpose_rev_batch(0, leaves, ev, jb["lg_n"] + jb["rate"], jb["cols"])
+                del ev
+                zk.fill_digests_buf_linear_gpu(dig, caps, leaves, N, jb["cols"], jb["cap"], jb["hash"])
+                torch.cuda.synchronize()
+            b.record()
+            torch.cuda.synchronize()
+            t_plain += a.elapsed_time(b) / args.steps
+        for cb, bb in zip(caps_b, bufs):
+            assert torch.equal(cb, bb[3]), "batched and plain commitments differ"
+        del bufs, cjobs, caps_b
+        torch.cuda.empty_cache()
+    line = {"metric": "uneven batch LDE+Merkle commit elems/s (batched graph vs plain per-call)",
+            "unit": "elems/s", "batched": total_elems / (t_batch * 1e-3), "plain": total_elems / (t_plain * 1e-3),
+            "batched_over_plain": t_plain / t_batch, "batched_ms": t_batch, "plain_ms": t_plain, "jobs": len(jobs),
+            "waves": len(waves), "elements": total_elems, "steps": args.steps, "dtype": "u64",
+            "config": {"workload": "64 jobs: lg_n U{10..20}, cols U{8..400}, rate_bits U{1,2,3}, Poseidon, "
+                                   "cap_height min(4, lg N), seed 3", "budget_gb": args.budget_gb}}
+    print(json.dumps(line), flush=True)
+
+
+def run_hashes(args):
+    """Alternative hashes at scale: 2^20 leaves x 135 elements, cap_height 4,
+    Poseidon2 + Monolith + Keccak forests built as one batch (one graph)."""
+    import torch
+    import zeknox_b200 as zk
+    torch.cuda.set_device(0)
+    nl, ls, ch = 1 << 20, 135, 4
+    trees = []
+    for k, h in enumerate((3, 4, 1)):
+        leaves = dev_field(nl * ls, 40 + k)
+        n_dig, n_cap = zk.merkle_sizes(nl, ch)
+        dig = torch.empty(n_dig * 4, dtype=torch.int64, device="cuda")
+        caps = torch.empty(n_cap * 4, dtype=torch.int64, device="cuda")
+        trees.append((h, leaves, dig, caps))
+    jobs = [zk.merkle_job(l, d, c, nl, ls, ch, h) for h, l, d, c in trees]
+    zk.merkle_batch(0, jobs)
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record()
+    for _ in range(args.steps):
+        zk.merkle_batch(0, jobs)
+    b.record()
+    torch.cuda.synchronize()
+    batch_ms = a.elapsed_time(b) / args.steps
+    per = {}
+    for h, l, d, c in trees:
+        a.record()
+        for _ in range(args.steps):
+            zk.fill_digests_buf_linear_gpu(d, c, l, nl, ls, ch, h)
+        b.record()
+        torch.cuda.synchronize()
+        ms = a.elapsed_time(b) / args.steps
+        name = {3: "poseidon2", 4: "monolith", 1: "keccak"}[h]
+        perms = nl * ((ls + 7) // 8) + (nl - (1 << ch)) if h != 1 else nl * ((ls * 8) // 136 + 1) + (nl - (1 << ch))
+        per[name] = {"ms": ms, "leaves_per_s": nl / (ms * 1e-3), "perms_per_s": perms / (ms * 1e-3)}
+    line = {"metric": "Merkle forests (2^20 leaves x 135, cap 4) leaves/s", "unit": "leaves/s",
+            "batched_value": 3 * nl / (batch_ms * 1e-3), "batched_ms": batch_ms, "per_hash": per, "steps": args.steps,
+            "dtype": "u64", "config": {"workload": "Poseidon2 + Monolith + Keccak forests, 2^20 leaves x 135, cap 4"}}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -331,6 +466,10 @@ def main():
     ap.add_argument("--lg-n", type=int, default=LG_N, help="log2 coefficients per column (profiling cases)")
     ap.add_argument("--only", default=None, choices=["lde", "merkle"],
                     help="profiling: run only this stage for warmup+steps iterations and exit")
+    ap.add_argument("--workload", default="commit", choices=["commit", "batch", "hashes"],
+                    help="commit: the headline line; batch: uneven 64-job batch vs plain calls; hashes: 2^20 x 135 "
+                         "forests with Poseidon2, Monolith and Keccak")
+    ap.add_argument("--budget-gb", type=float, default=48.0, help="batch workload: device memory per wave")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -338,6 +477,10 @@ def main():
         return run_reference(args, rank, world)
     if args.only:
         return run_stage(args)
+    if args.workload == "batch":
+        return run_batch(args)
+    if args.workload == "hashes":
+        return run_hashes(args)
     if world > 1:
         import datetime
 

@@ -53,6 +53,22 @@ RustError zeknox_commit_batch(size_t device_id, const zk_commit_job *jobs, uint3
  * allocates them from the stream-ordered pool when called). */
 uint64_t zeknox_commit_scratch_words(const zk_commit_job *job);
 
+/* One Merkle forest of fill_digests_buf_linear_gpu_with_gpu_ptr's layout. */
+typedef struct {
+    const uint64_t *leaves;   /* n_leaves x leaf_size, leaf-major */
+    uint64_t *digests;        /* 2 * (n_leaves - 2^cap_height) x 4 */
+    uint64_t *caps;           /* 2^cap_height x 4 */
+    uint64_t n_leaves;
+    uint64_t leaf_size;
+    uint32_t cap_height;
+    uint32_t hash_type;
+} zk_merkle_job;
+
+/* Build `njobs` forests (any mix of hashes and sizes) as one CUDA graph whose
+ * branches run concurrently; cached and replayed like zeknox_commit_batch.
+ * Synchronous. */
+RustError zeknox_merkle_batch(size_t device_id, const zk_merkle_job *jobs, uint32_t njobs);
+
 /* The LDE stage of a commit alone: rows[r * cols + b] = LDE_b(rev(r)), the
  * leaf-major bit-reversed matrix (compute_batched_lde + compute_transpose_rev
  * in one pass structure).  coeffs: cols x 2^lg_n column-major; rows:

@@ -116,3 +116,40 @@ def test_commit_argument_errors():
     job.hash_type = 2
     with pytest.raises(zk.ZeknoxError):
         zk.commit(0, job)
+
+
+def test_batch_graph_replay_reads_current_inputs():
+    """The cached graph is replayed on the second call with the same buffers:
+    new input data must produce the new commitment."""
+    shapes = [(11, 2, 24, 3, 3), (9, 3, 7, 2, 0), (12, 1, 16, 4, 4)]
+    jobs, bufs = [], []
+    for i, (lg, rate, cols, cap, h) in enumerate(shapes):
+        inp = to_dev(O.field_data(300 + i, cols << lg))
+        j, b = alloc_job(lg, rate, cols, cap, h, inp)
+        jobs.append(j)
+        bufs.append((inp,) + b)
+    zk.commit_batch(0, jobs)
+    for rnd in range(2):
+        for i, (lg, rate, cols, cap, h) in enumerate(shapes):
+            bufs[i][0].copy_(to_dev(O.field_data(400 + 10 * rnd + i, cols << lg)))
+        launches = zk.launch_count()
+        zk.commit_batch(0, jobs)  # replay: no new host launches
+        assert zk.launch_count() == launches
+        for i, (lg, rate, cols, cap, h) in enumerate(shapes):
+            rows, d, cp = expect(O.field_data(400 + 10 * rnd + i, cols << lg), lg, rate, cols, cap, h)
+            inp, leaves, dig, caps, n_dig = bufs[i]
+            assert np.array_equal(to_np(caps).reshape(-1, 4), cp)
+            assert np.array_equal(to_np(dig).reshape(-1, 4)[:n_dig], d)
+
+
+def test_commit_on_caller_stream():
+    lg, rate, cols, cap, h = 12, 2, 40, 4, 3
+    c = O.field_data(77, cols << lg)
+    s = torch.cuda.Stream()
+    with torch.cuda.stream(s):
+        inp = to_dev(c)
+        job, (leaves, dig, caps, n_dig) = alloc_job(lg, rate, cols, cap, h, inp)
+        zk.commit(0, job, stream=s.cuda_stream)
+    s.synchronize()
+    rows, d, cp = expect(c, lg, rate, cols, cap, h)
+    assert np.array_equal(to_np(caps).reshape(-1, 4), cp)

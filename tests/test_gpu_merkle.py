@@ -95,3 +95,20 @@ def test_multigpu_entry_matches_single():
     d2, c2 = O.merkle(leaves_np, ls, ch, 3)
     assert np.array_equal(to_np(cap).reshape(-1, 4), c2)
     assert np.array_equal(to_np(dig).reshape(-1, 4), d2)
+
+
+def test_merkle_batch_mixed_hashes():
+    cases = [(1 << 12, 135, 4, 3), (1 << 12, 135, 4, 4), (1 << 12, 135, 4, 1), (1 << 10, 9, 0, 0), (64, 5, 6, 3)]
+    jobs, bufs = [], []
+    for k, (nl, ls, ch, h) in enumerate(cases):
+        leaves_np = O.field_data(500 + k, nl * ls)
+        n_dig, n_cap = zk.merkle_sizes(nl, ch)
+        lv, dg, cp = to_dev(leaves_np), empty_dev(n_dig * 4), empty_dev(n_cap * 4)
+        jobs.append(zk.merkle_job(lv, dg, cp, nl, ls, ch, h))
+        bufs.append((leaves_np, lv, dg, cp, n_dig, ls, ch, h))
+    for _ in range(2):  # capture, then replay
+        zk.merkle_batch(0, jobs)
+        for leaves_np, lv, dg, cp, n_dig, ls, ch, h in bufs:
+            d2, c2 = O.merkle(leaves_np, ls, ch, h)
+            assert np.array_equal(to_np(cp).reshape(-1, 4), c2)
+            assert np.array_equal(to_np(dg)[:n_dig * 4].reshape(-1, 4), d2)

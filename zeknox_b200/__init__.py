@@ -32,7 +32,7 @@ ABI_SYMBOLS = [
     "fill_digests_buf_linear_cpu", "cuda_available",
 ]
 EXT_SYMBOLS = ["zeknox_last_error", "zeknox_commit", "zeknox_commit_batch", "zeknox_commit_scratch_words",
-               "zeknox_lde_rows", "zeknox_launch_count", "zeknox_measure_mul_rate"]
+               "zeknox_lde_rows", "zeknox_launch_count", "zeknox_measure_mul_rate", "zeknox_merkle_batch"]
 
 
 class RustError(ctypes.Structure):
@@ -78,6 +78,19 @@ class CommitJob(ctypes.Structure):
         ("leaves", ctypes.c_void_p),
         ("digests", ctypes.c_void_p),
         ("caps", ctypes.c_void_p),
+    ]
+
+
+class MerkleJob(ctypes.Structure):
+    """include/zeknox_b200.h zk_merkle_job."""
+    _fields_ = [
+        ("leaves", ctypes.c_void_p),
+        ("digests", ctypes.c_void_p),
+        ("caps", ctypes.c_void_p),
+        ("n_leaves", ctypes.c_uint64),
+        ("leaf_size", ctypes.c_uint64),
+        ("cap_height", ctypes.c_uint32),
+        ("hash_type", ctypes.c_uint32),
     ]
 
 
@@ -141,6 +154,8 @@ def load():
     L.zeknox_launch_count.restype = u64
     L.zeknox_measure_mul_rate.restype = ctypes.c_double
     L.zeknox_measure_mul_rate.argtypes = [sz]
+    L.zeknox_merkle_batch.restype = RustError
+    L.zeknox_merkle_batch.argtypes = [sz, ctypes.POINTER(MerkleJob), u32]
     _lib = L
     return L
 
@@ -332,3 +347,17 @@ def launch_count():
 
 def measure_mul_rate(device_id=0):
     return load().zeknox_measure_mul_rate(device_id)
+
+
+def merkle_job(leaves, digests, caps, n_leaves, leaf_size, cap_height, hash_type):
+    j = MerkleJob()
+    j.leaves, j.caps = leaves.data_ptr(), caps.data_ptr()
+    j.digests = digests.data_ptr() if digests is not None and digests.numel() else None
+    j.n_leaves, j.leaf_size, j.cap_height, j.hash_type = n_leaves, leaf_size, cap_height, hash_type
+    return j
+
+
+def merkle_batch(device_id, jobs):
+    """zeknox_merkle_batch: several forests as one cached CUDA graph."""
+    arr = (MerkleJob * len(jobs))(*jobs)
+    _check(load().zeknox_merkle_batch(device_id, arr, len(jobs)))

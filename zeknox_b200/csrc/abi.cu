@@ -13,6 +13,7 @@
 
 #include "../../include/lib.h"
 #include "../../include/zeknox_b200.h"
+#include "batch.cuh"
 #include "gl64.cuh"
 #include "ntt_api.cuh"
 #include "runtime.cuh"
@@ -386,65 +387,34 @@ extern "C" void fill_digests_buf_linear_cpu(void *digests_buf_ptr, void *cap_buf
 
 extern "C" const char *zeknox_last_error(void) { return g_last_error.empty() ? nullptr : g_last_error.c_str(); }
 
-static void check_job(const zk_commit_job &j)
-{
-    if (j.lg_n == 0 || j.rate_bits == 0 || j.cols == 0) throw zk::arg_failure("lg_n, rate_bits and cols must be >= 1");
-    if (j.lg_n + j.rate_bits > 32) throw zk::arg_failure("extended size above 2^32");
-    if (j.cap_height > j.lg_n + j.rate_bits) throw zk::arg_failure("cap_height above log2 of the leaf count");
-    if (!j.input || !j.leaves || !j.caps || (!j.digests && j.cap_height < j.lg_n + j.rate_bits))
-        throw zk::arg_failure("null buffer");
-    if (j.hash_type != 0 && j.hash_type != 1 && j.hash_type != 3 && j.hash_type != 4)
-        throw zk::arg_failure("unsupported hash_type");
-}
-
 extern "C" uint64_t zeknox_commit_scratch_words(const zk_commit_job *job)
 {
     if (!job) return 0;
-    uint64_t n = 1ULL << job->lg_n;
-    uint64_t w = zk::lde_rows_scratch_elems(job->lg_n, job->rate_bits, job->cols);
-    if (job->input_is_values) w += 2 * n * job->cols;
-    return w;
-}
-
-static void commit_on(zk::DeviceCtx &c, const zk_commit_job &j, cudaStream_t s)
-{
-    const uint64_t n = 1ULL << j.lg_n;
-    const uint64_t N = n << j.rate_bits;
-    const uint64_t gen = j.coset_gen ? j.coset_gen : ZK_GENERATOR;
-    cudaStream_t keep = c.stream;
-    c.stream = s;  // run the whole job on the caller's stream
-    try {
-        const uint64_t *coeffs = j.input;
-        zk::DevBuf cf;
-        if (j.input_is_values) {
-            cf.ctx = &c;
-            cf.p = c.alloc(n * j.cols * 8);
-            ZK_CUDA(cudaMemcpyAsync(cf.p, j.input, n * j.cols * 8, cudaMemcpyDeviceToDevice, s));
-            zk::ntt_batch_device(c, cf.p, j.lg_n, j.cols, true, false);
-            coeffs = cf.p;
-        }
-        zk::lde_rows_device(c, j.leaves, coeffs, j.lg_n, j.rate_bits, j.cols, gen, nullptr);
-        std::string err;
-        const uint64_t n_caps = 1ULL << j.cap_height;
-        if (!zk::merkle_device(j.digests, j.caps, j.leaves, 2 * (N - n_caps), n_caps, N, j.cols, j.cap_height,
-                               j.hash_type, s, err))
-            throw zk::arg_failure(err);
-    } catch (...) {
-        c.stream = keep;
-        throw;
-    }
-    c.stream = keep;
+    return zk::commit_scratch_words(job->lg_n, job->rate_bits, job->cols, job->input_is_values != 0);
 }
 
 extern "C" RustError zeknox_commit(size_t device_id, const zk_commit_job *job, void *stream)
 {
     return guarded([&] {
         if (!job) throw zk::arg_failure("null job");
-        check_job(*job);
+        zk::check_job(*job);
         zk::DeviceCtx &c = zk::device(device_id);
         std::lock_guard<std::recursive_mutex> lk(c.mu);
         cudaStream_t s = stream ? (cudaStream_t)stream : c.stream;
-        commit_on(c, *job, s);
+        const uint64_t words = zeknox_commit_scratch_words(job);
+        zk::DevBuf scratch;
+        if (words) {
+            scratch.ctx = &c;
+            cudaStream_t keep = c.stream;
+            c.stream = s;  // allocate and free on the stream that uses it
+            scratch.p = c.alloc(words * 8);
+            c.stream = keep;
+        }
+        zk::commit_enqueue(c, *job, s, scratch.p);
+        if (scratch.p) {
+            (void)cudaFreeAsync(scratch.p, s);
+            scratch.p = nullptr;
+        }
         if (!stream) c.sync();
     });
 }
@@ -453,10 +423,21 @@ extern "C" RustError zeknox_commit_batch(size_t device_id, const zk_commit_job *
 {
     return guarded([&] {
         if (njobs && !jobs) throw zk::arg_failure("null jobs");
-        for (uint32_t i = 0; i < njobs; i++) check_job(jobs[i]);
+        for (uint32_t i = 0; i < njobs; i++) zk::check_job(jobs[i]);
         zk::DeviceCtx &c = zk::device(device_id);
         std::lock_guard<std::recursive_mutex> lk(c.mu);
-        for (uint32_t i = 0; i < njobs; i++) commit_on(c, jobs[i], c.stream);
+        zk::commit_batch_graph(c, jobs, njobs);
+        c.sync();
+    });
+}
+
+extern "C" RustError zeknox_merkle_batch(size_t device_id, const zk_merkle_job *jobs, uint32_t njobs)
+{
+    return guarded([&] {
+        if (njobs && !jobs) throw zk::arg_failure("null jobs");
+        zk::DeviceCtx &c = zk::device(device_id);
+        std::lock_guard<std::recursive_mutex> lk(c.mu);
+        zk::merkle_batch_graph(c, jobs, njobs);
         c.sync();
     });
 }

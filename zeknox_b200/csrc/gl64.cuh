@@ -251,11 +251,15 @@ ZK_HD uint64_t gl_sbox7(uint64_t x)
     return gl_mul(x3, x4);
 }
 
-// Same S-box on lazily reduced values.
+// Same S-box on lazily reduced values.  ZK_SBOX_SQR selects the dedicated
+// squaring product (6 multiplies + 6 adds) over the general one (8 multiply-adds).
+#ifndef ZK_SBOX_SQR
+#define ZK_SBOX_SQR 0
+#endif
 ZK_HD uint64_t gl_sbox7_nc(uint64_t x)
 {
-    uint64_t x2 = gl_sqr_nc(x);
-    uint64_t x4 = gl_sqr_nc(x2);
+    uint64_t x2 = ZK_SBOX_SQR ? gl_sqr_nc(x) : gl_mul_nc(x, x);
+    uint64_t x4 = ZK_SBOX_SQR ? gl_sqr_nc(x2) : gl_mul_nc(x2, x2);
     uint64_t x3 = gl_mul_nc(x2, x);
     return gl_mul_nc(x3, x4);
 }

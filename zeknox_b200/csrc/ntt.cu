@@ -96,6 +96,7 @@ struct DifJob {
     uint32_t L;
     uint32_t rate;
     uint32_t cols;
+    uint64_t row_stride;
     bool rows;
     bool inverse;
     uint64_t *scratch;
@@ -125,6 +126,7 @@ static void run_dif(DeviceCtx &c, const DifJob &j)
         a.s_lo = ps.s_lo;
         a.rate = j.rate;
         a.cols = j.cols;
+        a.row_stride = j.row_stride;
         const bool store_rows = j.rows && last;
         if (store_rows) {
             a.dst = j.dst;
@@ -182,36 +184,44 @@ static void reorder(DeviceCtx &c, const uint64_t *src, uint64_t src_stride, uint
 
 // --------------------------------------------------------------- public ops
 
-void ntt_batch_device(DeviceCtx &c, uint64_t *inout, uint32_t lg, uint64_t batches, bool inverse, bool with_coset)
+void ntt_batch_device(DeviceCtx &c, uint64_t *inout, uint32_t lg, uint64_t batches, bool inverse, bool with_coset,
+                      uint64_t *scratch)
 {
     const uint64_t n = 1ULL << lg;
     if (batches == 0) return;
-    DevBuf tmp(c, n * batches);
+    DevBuf tmp;
+    if (scratch) {
+        tmp.p = nullptr;
+    } else {
+        tmp.ctx = &c;
+        tmp.p = c.alloc(n * batches * 8);
+    }
+    uint64_t *tp = scratch ? scratch : tmp.p;
     if (!inverse) {
         DifJob j{};
         j.src = inout;
         j.src_stride = n;
         j.load = with_coset ? LOAD_SCALE : LOAD_PLAIN;
         j.tab = with_coset ? c.coset_powers(lg) : nullptr;
-        j.dst = tmp.p;
+        j.dst = tp;
         j.dst_stride = n;
         j.vcols = batches;
         j.L = lg;
         run_dif(c, j);
-        reorder(c, tmp.p, n, inout, n, lg, 0, batches, 1, nullptr);
+        reorder(c, tp, n, inout, n, lg, 0, batches, 1, nullptr);
     } else {
         DifJob j{};
         j.src = inout;
         j.src_stride = n;
         j.load = LOAD_PLAIN;
-        j.dst = tmp.p;
+        j.dst = tp;
         j.dst_stride = n;
         j.vcols = batches;
         j.L = lg;
         j.inverse = true;
         run_dif(c, j);
         // reference order: coset multiply (forward powers) then n^-1 (ntt.cu:137-143)
-        reorder(c, tmp.p, n, inout, n, lg, 0, batches, H_SIZE_INV[lg], with_coset ? c.coset_powers(lg) : nullptr);
+        reorder(c, tp, n, inout, n, lg, 0, batches, H_SIZE_INV[lg], with_coset ? c.coset_powers(lg) : nullptr);
     }
 }
 
@@ -255,37 +265,71 @@ void lde_batch_device(DeviceCtx &c, uint64_t *out, const uint64_t *in, uint32_t 
     }
 }
 
+// Columns per chunk of the fused LDE: the intermediate of a chunk (2^(lg_n +
+// rate) words per column) is kept within ZK_L2_CHUNK_BYTES so the second pass
+// reads it back from L2 instead of HBM.  A multiple of the 16-column row tile.
+static constexpr uint64_t ZK_L2_CHUNK_BYTES = 40ULL << 20;
+
+uint32_t lde_rows_chunk_cols(uint32_t lg_n, uint32_t rate, uint64_t cols)
+{
+    const uint64_t per_col = 8ULL << (lg_n + rate);
+    uint64_t c = ZK_L2_CHUNK_BYTES / per_col;
+    c = c < 16 ? 16 : (c / 16) * 16;
+    return (uint32_t)(c < cols ? c : ((cols + 15) / 16) * 16);
+}
+
+uint64_t lde_rows_scratch_elems(uint32_t lg_n, uint32_t rate, uint64_t cols)
+{
+    if (plan_passes(lg_n, true).size() == 1) return 0;
+    return (1ULL << (lg_n + rate)) * lde_rows_chunk_cols(lg_n, rate, cols);
+}
+
 void lde_rows_device(DeviceCtx &c, uint64_t *rows, const uint64_t *coeffs, uint32_t lg_n, uint32_t rate, uint64_t cols,
                      uint64_t coset_gen, uint64_t *scratch)
 {
     const uint64_t n = 1ULL << lg_n;
     if (cols == 0) return;
-    DifJob j{};
-    j.src = coeffs;
-    j.src_stride = n;
-    j.load = LOAD_COSETS;
-    j.tab = c.lde_table(lg_n, rate, coset_gen % GL_P);
-    j.dst = rows;
-    j.vcols = cols << rate;
-    j.L = lg_n;
-    j.rate = rate;
-    j.cols = (uint32_t)cols;
-    j.rows = true;
+    const bool multi = plan_passes(lg_n, true).size() > 1;
+    const uint64_t chunk = multi ? lde_rows_chunk_cols(lg_n, rate, cols) : cols;
     DevBuf tmp;
-    if (plan_passes(lg_n, true).size() > 1) {
-        if (!scratch) {
-            tmp.ctx = &c;
-            tmp.p = c.alloc((n << rate) * cols * 8);
-            scratch = tmp.p;
-        }
-        j.scratch = scratch;
+    if (multi && !scratch) {
+        tmp.ctx = &c;
+        tmp.p = c.alloc(lde_rows_scratch_elems(lg_n, rate, cols) * 8);
+        scratch = tmp.p;
     }
-    run_dif(c, j);
+    const uint64_t *tab = c.lde_table(lg_n, rate, coset_gen % GL_P);
+    for (uint64_t c0 = 0; c0 < cols; c0 += chunk) {
+        const uint64_t cc = cols - c0 < chunk ? cols - c0 : chunk;
+        DifJob j{};
+        j.src = coeffs + c0 * n;
+        j.src_stride = n;
+        j.load = LOAD_COSETS;
+        j.tab = tab;
+        j.dst = rows + c0;
+        j.row_stride = cols;
+        j.vcols = cc << rate;
+        j.L = lg_n;
+        j.rate = rate;
+        j.cols = (uint32_t)cc;
+        j.rows = true;
+        j.scratch = scratch;
+        run_dif(c, j);
+    }
 }
 
-uint64_t lde_rows_scratch_elems(uint32_t lg_n, uint32_t rate, uint64_t cols)
+// Tables a commit of this shape reads, built now (the batched path captures
+// its launches in a CUDA graph, where nothing may allocate).
+void prepare_tables(DeviceCtx &c, uint32_t lg_n, uint32_t rate, uint64_t coset_gen, bool values)
 {
-    return plan_passes(lg_n, true).size() > 1 ? ((1ULL << (lg_n + rate)) * cols) : 0;
+    c.lde_table(lg_n, rate, coset_gen % GL_P);
+    c.twiddles(12, false);
+    for (const Pass &ps : plan_passes(lg_n, true))
+        if (ps.s_lo) c.twiddles(ps.s_lo + ps.logr, false);
+    if (values) {
+        c.twiddles(12, true);
+        for (const Pass &ps : plan_passes(lg_n, false))
+            if (ps.s_lo) c.twiddles(ps.s_lo + ps.logr, true);
+    }
 }
 
 void transpose_rev_device(DeviceCtx &c, uint64_t *out, const uint64_t *in, uint32_t lg, uint64_t cols)

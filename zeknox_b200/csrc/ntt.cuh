@@ -85,7 +85,8 @@ struct NttPassArgs {
     uint32_t L;               // log2 transform size
     uint32_t s_lo;            // lowest stage of this pass
     uint32_t rate;            // LOAD_COSETS / STORE_ROWS: log2 cosets per column
-    uint32_t cols;            // STORE_ROWS: real columns (row length of the output)
+    uint32_t cols;            // STORE_ROWS: real columns in this launch
+    uint64_t row_stride;      // STORE_ROWS: words per output row (>= cols; dst points at the first column)
 };
 
 // Sub-step of the in-CTA R-point DIF: every task owns E elements spaced Q apart
@@ -250,7 +251,7 @@ __global__ void __launch_bounds__(NT, 2) ntt_pass_kernel(NttPassArgs a)
             const uint64_t b = vcol >> a.rate;
             if (b < a.cols) {
                 const uint64_t row = ((uint64_t)bitrev32((uint32_t)(vcol & rmask), a.rate) << a.L) + pos;
-                a.dst[row * a.cols + b] = val;
+                a.dst[row * a.row_stride + b] = val;
             }
         } else if (vcol < a.vcols) {
             a.dst[vcol * a.dst_stride + pos] = val;

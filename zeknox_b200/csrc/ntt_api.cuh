@@ -7,7 +7,9 @@
 namespace zk {
 
 // compute_batched_ntt on device memory: natural order in and out, in place.
-void ntt_batch_device(DeviceCtx &c, uint64_t *inout, uint32_t lg, uint64_t batches, bool inverse, bool with_coset);
+// `scratch` (n * batches words) may be null: then it comes from the stream-ordered pool.
+void ntt_batch_device(DeviceCtx &c, uint64_t *inout, uint32_t lg, uint64_t batches, bool inverse, bool with_coset,
+                      uint64_t *scratch = nullptr);
 
 // compute_batched_lde on device memory: column-major natural-order evaluations.
 void lde_batch_device(DeviceCtx &c, uint64_t *out, const uint64_t *in, uint32_t lg_n, uint32_t rate, uint64_t batches,
@@ -19,6 +21,10 @@ void lde_batch_device(DeviceCtx &c, uint64_t *out, const uint64_t *in, uint32_t 
 void lde_rows_device(DeviceCtx &c, uint64_t *rows, const uint64_t *coeffs, uint32_t lg_n, uint32_t rate, uint64_t cols,
                      uint64_t coset_gen, uint64_t *scratch);
 uint64_t lde_rows_scratch_elems(uint32_t lg_n, uint32_t rate, uint64_t cols);
+uint32_t lde_rows_chunk_cols(uint32_t lg_n, uint32_t rate, uint64_t cols);
+
+// Build every table a commit of this shape uses (before graph capture).
+void prepare_tables(DeviceCtx &c, uint32_t lg_n, uint32_t rate, uint64_t coset_gen, bool values);
 
 void transpose_rev_device(DeviceCtx &c, uint64_t *out, const uint64_t *in, uint32_t lg, uint64_t cols);
 
