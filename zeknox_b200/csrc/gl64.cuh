@@ -86,7 +86,7 @@ ZK_HD uint64_t gl_reduce96(uint64_t lo, uint64_t hi) { return gl_canon(gl_reduce
 // 64x64 product is 8 multiply-adds, the reduction of lo + 2^64*(h0 + 2^32*h1)
 // to lo - h1 + EPS*h0 is 13 integer ops with no compares or selects.
 
-#ifdef __CUDA_ARCH__
+#ifdef __CUDACC__
 __device__ __forceinline__ void mul_wide(uint64_t a, uint64_t b, uint32_t &r0, uint32_t &r1, uint32_t &r2, uint32_t &r3)
 {
     const uint32_t a0 = (uint32_t)a, a1 = (uint32_t)(a >> 32), b0 = (uint32_t)b, b1 = (uint32_t)(b >> 32);

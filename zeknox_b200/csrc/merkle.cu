@@ -14,7 +14,8 @@
 
 namespace zk {
 
-static constexpr int LEAF_T = 128;     // leaves (threads) per CTA
+static constexpr int LEAF_T = 128;     // leaves (threads) per CTA of the leaf kernel
+static constexpr int FOLD_T = 256;     // leaf digests per CTA of the fold kernel
 static constexpr int TAIL_MAXM = 1024; // nodes a tail CTA can take
 
 bool merkle_geometry_ok(uint64_t n_digests, uint64_t n_caps, uint64_t n_leaves, uint64_t cap_height, std::string &err)
@@ -28,10 +29,14 @@ static void merkle_launch(uint64_t *digests, uint64_t *caps, const uint64_t *lea
     uint64_t blocks = (g.n_leaves + LEAF_T - 1) / LEAF_T;
     merkle_leaf_kernel<H, LEAF_T><<<(unsigned)blocks, LEAF_T, 0, s>>>(leaves, digests, caps, g);
     note_launch();
-    if (g.sub_leaves <= (uint64_t)LEAF_T) return;  // caps written by the leaf kernel
-    // heights folded by the leaf kernel
+    if (g.sub_leaves == 1) return;  // caps == leaves
+    blocks = (g.n_leaves + FOLD_T - 1) / FOLD_T;
+    merkle_fold_kernel<H, FOLD_T><<<(unsigned)blocks, FOLD_T, 0, s>>>(digests, caps, g);
+    note_launch();
+    if (g.sub_leaves <= (uint64_t)FOLD_T) return;  // caps written by the fold kernel
+    // heights folded by the fold kernel
     uint32_t u0 = 0;
-    while ((1u << (u0 + 1)) <= (uint32_t)LEAF_T && u0 + 1 <= g.log_sub - 1) u0++;
+    while ((1u << (u0 + 1)) <= (uint32_t)FOLD_T && u0 + 1 <= g.log_sub - 1) u0++;
     while ((g.sub_leaves >> u0) > (uint64_t)TAIL_MAXM) {
         u0++;
         uint64_t total = (g.sub_leaves >> u0) * g.n_caps;

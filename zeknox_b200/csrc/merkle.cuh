@@ -9,9 +9,9 @@
 //
 // Kernel structure (B200-first instead of one launch per level):
 //   * leaf kernel: one thread per leaf runs the sponge with the state in
-//     registers; the CTA then folds its own T leaves log2(T) levels up in
-//     shared memory, writing every node it produces, and when whole subtrees
-//     fit in the CTA it also writes their caps;
+//     registers (nothing else, so no warp idles on a barrier);
+//   * fold kernel: each CTA folds T consecutive leaf digests log2(T) levels up
+//     in shared memory, writing every node, and the caps of subtrees that fit;
 //   * tail kernel: one CTA per subtree folds the remaining levels in shared
 //     memory and writes the cap (only when L > T).
 #pragma once
@@ -45,53 +45,56 @@ __device__ __forceinline__ void leaf_hash(const uint64_t *__restrict__ row, uint
     hash_one<H>(row, len, out);
 }
 
-// T threads per CTA, T a power of two.  smem: T digests.
+// Leaf digests only: one thread per leaf, no shared memory, no barriers, so
+// every warp stays on the hash for the whole kernel.
 template <int H, int T>
 __global__ void __launch_bounds__(T) merkle_leaf_kernel(const uint64_t *__restrict__ leaves, uint64_t *__restrict__ digests,
                                                         uint64_t *__restrict__ caps, MerkleGeom g)
 {
+    const uint64_t i = (uint64_t)blockIdx.x * T + threadIdx.x;
+    if (i >= g.n_leaves) return;
+    // caps == leaves: the leaf hashes are the caps, digests untouched
+    uint64_t *dst = g.sub_leaves == 1 ? caps + 4 * i : digests + 4 * merkle_node_index(g, i, 0);
+    uint64_t d[4];
+    if (H == HASH_KECCAK && g.leaf_size < 4) {
+        // Keccak copies a < 4-word leaf and leaves the other digest words as
+        // they are in the output buffer (native/keccak/keccak.cu:118-121)
+#pragma unroll
+        for (int q = 0; q < 4; q++) d[q] = dst[q];
+    }
+    leaf_hash<H>(leaves + i * g.leaf_size, g.leaf_size, d);
+#pragma unroll
+    for (int q = 0; q < 4; q++) dst[q] = d[q];
+}
+
+// Folds the stored leaf digests upwards: each CTA takes T consecutive leaves'
+// digests and computes every node whose leaves all lie in it (log2 T levels,
+// or up to the subtree's two top nodes), writing each node; when whole
+// subtrees fit in the CTA it also writes their caps.
+template <int H, int T>
+__global__ void __launch_bounds__(T) merkle_fold_kernel(uint64_t *__restrict__ digests, uint64_t *__restrict__ caps,
+                                                        MerkleGeom g)
+{
     __shared__ uint64_t node[T][4];
     const uint64_t i0 = (uint64_t)blockIdx.x * T;
     const uint32_t t = threadIdx.x;
-    const uint64_t i = i0 + t;
-    uint64_t d[4];
-    if (i < g.n_leaves) {
-        // caps == leaves: the leaf hashes are the caps, digests untouched
-        uint64_t *dst = g.sub_leaves == 1 ? caps + 4 * i : digests + 4 * merkle_node_index(g, i, 0);
-        if (H == HASH_KECCAK && g.leaf_size < 4) {
-            // Keccak copies a < 4-word leaf and leaves the other digest words as
-            // they are in the output buffer (native/keccak/keccak.cu:118-121)
+    const uint64_t cta_leaves = g.n_leaves - i0 < (uint64_t)T ? g.n_leaves - i0 : (uint64_t)T;
+    if (t < cta_leaves) {
+        const uint64_t di = merkle_node_index(g, i0 + t, 0);
 #pragma unroll
-            for (int q = 0; q < 4; q++) d[q] = dst[q];
-        }
-        leaf_hash<H>(leaves + i * g.leaf_size, g.leaf_size, d);
-#pragma unroll
-        for (int q = 0; q < 4; q++) {
-            dst[q] = d[q];
-            node[t][q] = d[q];
-        }
-        if (g.sub_leaves == 1) return;
+        for (int q = 0; q < 4; q++) node[t][q] = digests[4 * di + q];
     }
-    if (g.sub_leaves == 1) return;
-    // Levels fully inside this CTA: height u has (L >> u) >= 2 nodes per subtree.
-    uint32_t top = g.log_sub - 1;  // highest stored height
+    const uint32_t top = g.log_sub - 1;  // highest stored height
     uint32_t U = 0;
     while ((1u << (U + 1)) <= T && U + 1 <= top) U++;
-    const uint64_t cta_leaves = g.n_leaves - i0 < (uint64_t)T ? g.n_leaves - i0 : (uint64_t)T;
     for (uint32_t u = 1; u <= U; u++) {
         __syncthreads();
-        uint32_t nodes = T >> u;
+        const uint32_t nodes = T >> u;
         uint64_t h[4];
-        bool act = t < nodes && ((uint64_t)t << u) < cta_leaves;
+        const bool act = t < nodes && ((uint64_t)t << u) < cta_leaves;
         if (act) {
-            uint64_t l[4], r[4];
-#pragma unroll
-            for (int q = 0; q < 4; q++) {
-                l[q] = node[2 * t][q];
-                r[q] = node[2 * t + 1][q];
-            }
-            hash_two<H>(l, r, h);
-            uint64_t di = merkle_node_index(g, i0 + ((uint64_t)t << u), u);
+            hash_two<H>(node[2 * t], node[2 * t + 1], h);
+            const uint64_t di = merkle_node_index(g, i0 + ((uint64_t)t << u), u);
 #pragma unroll
             for (int q = 0; q < 4; q++) digests[4 * di + q] = h[q];
         }
@@ -101,19 +104,13 @@ __global__ void __launch_bounds__(T) merkle_leaf_kernel(const uint64_t *__restri
             for (int q = 0; q < 4; q++) node[t][q] = h[q];
         }
     }
-    // Whole subtrees inside the CTA: their caps come from the two top nodes.
     if (U == top && g.sub_leaves <= (uint64_t)T) {
         __syncthreads();
-        uint32_t subs = (uint32_t)((cta_leaves + g.sub_leaves - 1) >> g.log_sub);
+        const uint32_t subs = (uint32_t)((cta_leaves + g.sub_leaves - 1) >> g.log_sub);
         if (t < subs) {
-            uint64_t l[4], r[4], h[4];
-#pragma unroll
-            for (int q = 0; q < 4; q++) {
-                l[q] = node[2 * t][q];
-                r[q] = node[2 * t + 1][q];
-            }
-            hash_two<H>(l, r, h);
-            uint64_t k = (i0 >> g.log_sub) + t;
+            uint64_t h[4];
+            hash_two<H>(node[2 * t], node[2 * t + 1], h);
+            const uint64_t k = (i0 >> g.log_sub) + t;
 #pragma unroll
             for (int q = 0; q < 4; q++) caps[4 * k + q] = h[q];
         }
