@@ -38,18 +38,48 @@ ZK_HD uint64_t mulhi64(uint64_t a, uint64_t b)
 // exactly when sum + EPS wraps.
 ZK_HD uint64_t gl_add(uint64_t a, uint64_t b)
 {
+#ifdef __CUDA_ARCH__
+    uint32_t r0, r1, t0, t1, c;
+    asm("{\n\t"
+        "add.cc.u32   %0, %5, %7;\n\t"
+        "addc.cc.u32  %1, %6, %8;\n\t"
+        "addc.u32     %4, 0, 0;\n\t"
+        "add.cc.u32   %2, %0, 0xffffffff;\n\t"
+        "addc.cc.u32  %3, %1, 0;\n\t"
+        "addc.u32     %4, %4, 0;\n\t"
+        "}"
+        : "=&r"(r0), "=&r"(r1), "=&r"(t0), "=&r"(t1), "=&r"(c)
+        : "r"((uint32_t)a), "r"((uint32_t)(a >> 32)), "r"((uint32_t)b), "r"((uint32_t)(b >> 32)));
+    return c ? (((uint64_t)t1 << 32) | t0) : (((uint64_t)r1 << 32) | r0);
+#else
     uint64_t s = a + b;
     uint64_t t = s + GL_EPS;
     bool c1 = s < a;
     bool c2 = t < s;
     return (c1 | c2) ? t : s;
+#endif
 }
 
-// a - b for canonical a, b: a borrow means a - b + 2^64, fix by subtracting EPS.
+// a - b for canonical a, b: a borrow means a - b + 2^64, fix by adding p.
 ZK_HD uint64_t gl_sub(uint64_t a, uint64_t b)
 {
+#ifdef __CUDA_ARCH__
+    uint32_t r0, r1, m, m1;
+    asm("{\n\t"
+        "sub.cc.u32   %0, %4, %6;\n\t"
+        "subc.cc.u32  %1, %5, %7;\n\t"
+        "subc.u32     %2, 0, 0;\n\t"
+        "and.b32      %3, %2, 1;\n\t"
+        "add.cc.u32   %0, %0, %3;\n\t"
+        "addc.u32     %1, %1, %2;\n\t"
+        "}"
+        : "=&r"(r0), "=&r"(r1), "=&r"(m), "=&r"(m1)
+        : "r"((uint32_t)a), "r"((uint32_t)(a >> 32)), "r"((uint32_t)b), "r"((uint32_t)(b >> 32)));
+    return ((uint64_t)r1 << 32) | r0;
+#else
     uint64_t d = a - b;
     return (a < b) ? d - GL_EPS : d;
+#endif
 }
 
 ZK_HD uint64_t gl_neg(uint64_t a) { return a ? GL_P - a : 0; }
@@ -214,7 +244,12 @@ ZK_HD uint64_t gl_sqr(uint64_t a) { return gl_canon(gl_sqr_nc(a)); }
 ZK_HD uint64_t gl_mul_pow2_lt64(uint64_t a, unsigned s)
 {
     if (s == 0) return a;
+#ifdef __CUDA_ARCH__
+    const uint64_t lo = a << s, hi = a >> (64 - s);
+    return gl_canon(reduce_nc((uint32_t)lo, (uint32_t)(lo >> 32), (uint32_t)hi, (uint32_t)(hi >> 32)));
+#else
     return gl_reduce128(a << s, a >> (64 - s));
+#endif
 }
 
 // a * 2^s for any s (taken mod 192, the order of 2).  2^96 = -1 turns
@@ -225,9 +260,13 @@ ZK_HD uint64_t gl_mul_pow2(uint64_t a, unsigned s)
     s %= 192;
     bool neg = s >= 96;
     if (neg) s -= 96;
-    uint64_t r = s < 64 ? gl_mul_pow2_lt64(a, s) : gl_sub(gl_mul_pow2_lt64(a, s - 32), gl_mul_pow2_lt64(a, s - 64));
+    // 64 <= s < 96: one multiply by the constant 2^s mod p (2^s = 2^(s-32) - 2^(s-64))
+    uint64_t r = s < 64 ? gl_mul_pow2_lt64(a, s)
+                        : gl_mul(a, ((1ULL << (s - 32)) - (1ULL << (s - 64))));
     return neg ? gl_neg(r) : r;
 }
+
+
 
 ZK_HD uint64_t gl_pow(uint64_t a, uint64_t e)
 {

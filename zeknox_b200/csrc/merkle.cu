@@ -14,7 +14,7 @@
 
 namespace zk {
 
-static constexpr int LEAF_T = 128;     // leaves (threads) per CTA of the leaf kernel
+static constexpr int LEAF_T = 256;     // leaves (threads) per CTA of the leaf kernel
 static constexpr int FOLD_T = 256;     // leaf digests per CTA of the fold kernel
 static constexpr int TAIL_MAXM = 1024; // nodes a tail CTA can take
 

@@ -268,7 +268,7 @@ void lde_batch_device(DeviceCtx &c, uint64_t *out, const uint64_t *in, uint32_t 
 // Columns per chunk of the fused LDE: the intermediate of a chunk (2^(lg_n +
 // rate) words per column) is kept within ZK_L2_CHUNK_BYTES so the second pass
 // reads it back from L2 instead of HBM.  A multiple of the 16-column row tile.
-static constexpr uint64_t ZK_L2_CHUNK_BYTES = 40ULL << 20;
+static constexpr uint64_t ZK_L2_CHUNK_BYTES = 64ULL << 20;
 
 uint32_t lde_rows_chunk_cols(uint32_t lg_n, uint32_t rate, uint64_t cols)
 {

@@ -36,24 +36,37 @@ __host__ __device__ constexpr unsigned root_exp(int h, int inv)
 }
 
 // In-register DIF on E = 2^LOGE values: natural input, bit-reversed output.
+// Stages and butterflies are expanded at compile time so every index and every
+// shift amount is a constant (the values stay in registers).
+template <int INV, int H, int SPAN, int BLK, int I>
+__device__ __forceinline__ void dif_bfly(uint64_t *x)
+{
+    const uint64_t u = x[BLK + I], v = x[BLK + I + SPAN];
+    x[BLK + I] = gl_add(u, v);
+    const uint64_t d = gl_sub(u, v);
+    x[BLK + I + SPAN] = I == 0 ? d : gl_mul_pow2(d, (root_exp(H, INV) * (unsigned)I) % 192u);
+    if constexpr (I + 1 < SPAN) dif_bfly<INV, H, SPAN, BLK, I + 1>(x);
+}
+
+template <int INV, int E, int H, int BLK>
+__device__ __forceinline__ void dif_stage(uint64_t *x)
+{
+    constexpr int SPAN = 1 << (H - 1);
+    dif_bfly<INV, H, SPAN, BLK, 0>(x);
+    if constexpr (BLK + 2 * SPAN < E) dif_stage<INV, E, H, BLK + 2 * SPAN>(x);
+}
+
+template <int INV, int E, int H>
+__device__ __forceinline__ void dif_stages(uint64_t *x)
+{
+    dif_stage<INV, E, H, 0>(x);
+    if constexpr (H > 1) dif_stages<INV, E, H - 1>(x);
+}
+
 template <int LOGE, int INV>
 __device__ __forceinline__ void dif_regs(uint64_t *x)
 {
-    constexpr int E = 1 << LOGE;
-#pragma unroll
-    for (int h = LOGE; h >= 1; h--) {
-        const int span = 1 << (h - 1);
-#pragma unroll
-        for (int blk = 0; blk < E; blk += 2 * span) {
-#pragma unroll
-            for (int i = 0; i < span; i++) {
-                uint64_t u = x[blk + i], v = x[blk + i + span];
-                x[blk + i] = gl_add(u, v);
-                uint64_t d = gl_sub(u, v);
-                x[blk + i + span] = i == 0 ? d : gl_mul_pow2(d, (root_exp(h, INV) * (unsigned)i) % 192u);
-            }
-        }
-    }
+    dif_stages<INV, 1 << LOGE, LOGE>(x);
 }
 
 // XOR-fold swizzle of a shared-memory word index (8-byte words): every
