@@ -77,6 +77,19 @@ RustError zeknox_merkle_batch(size_t device_id, const zk_merkle_job *jobs, uint3
 RustError zeknox_lde_rows(size_t device_id, uint64_t *rows, const uint64_t *coeffs, uint32_t lg_n, uint32_t rate_bits,
                           uint32_t cols, uint64_t coset_gen, void *stream);
 
+/* zeknox_lde_rows for callers that cannot allocate device memory (code being
+ * captured into a CUDA graph, code whose device memory is owned by another
+ * allocator or arena).  No counterpart in the reference.  It never allocates:
+ * its inter-pass scratch (32 MiB) and the tables it reads live in file-scope
+ * device arrays that every GPU loading the library holds until exit.  Limit:
+ * lg_n + rate_bits <= 18; larger sizes are rejected with
+ * cudaErrorInvalidValue.  The first call on a device looks up those arrays'
+ * addresses (make it before any stream capture).  All calls share the
+ * scratch, so calls that overlap on the GPU race; stream NULL means the legacy
+ * default stream and a synchronous call. */
+RustError zeknox_lde_rows_noalloc(size_t device_id, uint64_t *rows, const uint64_t *coeffs, uint32_t lg_n,
+                                  uint32_t rate_bits, uint32_t cols, uint64_t coset_gen, void *stream);
+
 /* Number of kernels this library has launched so far in the process. */
 uint64_t zeknox_launch_count(void);
 

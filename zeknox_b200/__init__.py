@@ -32,7 +32,8 @@ ABI_SYMBOLS = [
     "fill_digests_buf_linear_cpu", "cuda_available",
 ]
 EXT_SYMBOLS = ["zeknox_last_error", "zeknox_commit", "zeknox_commit_batch", "zeknox_commit_scratch_words",
-               "zeknox_lde_rows", "zeknox_launch_count", "zeknox_measure_mul_rate", "zeknox_merkle_batch"]
+               "zeknox_lde_rows", "zeknox_launch_count", "zeknox_measure_mul_rate", "zeknox_merkle_batch",
+               "zeknox_lde_rows_noalloc"]
 
 
 class RustError(ctypes.Structure):
@@ -154,6 +155,8 @@ def load():
     L.zeknox_launch_count.restype = u64
     L.zeknox_measure_mul_rate.restype = ctypes.c_double
     L.zeknox_measure_mul_rate.argtypes = [sz]
+    L.zeknox_lde_rows_noalloc.restype = RustError
+    L.zeknox_lde_rows_noalloc.argtypes = [sz, vp, vp, u32, u32, u32, u64, vp]
     L.zeknox_merkle_batch.restype = RustError
     L.zeknox_merkle_batch.argtypes = [sz, ctypes.POINTER(MerkleJob), u32]
     _lib = L
@@ -338,6 +341,14 @@ def lde_rows(device_id, rows, coeffs, lg_n, rate_bits, cols, coset_gen=7, stream
     """zeknox_lde_rows: coefficient columns -> bit-reversed leaf-major LDE matrix."""
     _check(load().zeknox_lde_rows(device_id, _ptr(rows), _ptr(coeffs), lg_n, rate_bits, cols, coset_gen,
                                   ctypes.c_void_p(stream) if stream else None))
+    return rows
+
+
+def lde_rows_noalloc(device_id, rows, coeffs, lg_n, rate_bits, cols, coset_gen=7, stream=None):
+    """zeknox_lde_rows_noalloc: the same result as lde_rows without allocating
+    device memory (static 32 MiB scratch; lg_n + rate_bits <= 18)."""
+    _check(load().zeknox_lde_rows_noalloc(device_id, _ptr(rows), _ptr(coeffs), lg_n, rate_bits, cols, coset_gen,
+                                          ctypes.c_void_p(stream) if stream else None))
     return rows
 
 

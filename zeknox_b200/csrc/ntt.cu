@@ -278,6 +278,64 @@ uint32_t lde_rows_chunk_cols(uint32_t lg_n, uint32_t rate, uint64_t cols)
     return (uint32_t)(c < cols ? c : ((cols + 15) / 16) * 16);
 }
 
+// ------------------------------------------------- explicit-table variant
+//
+// The same passes as run_dif / lde_rows_device for the fused LDE, with every
+// table and the scratch passed in by the caller and no DeviceCtx involved (no
+// lazy table builds, no pool allocations).  tw[lg] must hold w_{2^lg}^t,
+// t < 2^lg, for lg = 12 and every pass's lg M.
+void lde_rows_explicit(cudaStream_t stream, uint64_t *rows, const uint64_t *coeffs, uint32_t lg_n, uint32_t rate,
+                       uint64_t cols, const uint64_t *lde_tab, const uint64_t *const *tw, uint64_t *scratch,
+                       uint64_t chunk_cols)
+{
+    const uint64_t n = 1ULL << lg_n;
+    const auto passes = plan_passes(lg_n, true);
+    for (uint64_t c0 = 0; c0 < cols; c0 += chunk_cols) {
+        const uint64_t cc = cols - c0 < chunk_cols ? cols - c0 : chunk_cols;
+        for (size_t pi = 0; pi < passes.size(); pi++) {
+            const Pass &ps = passes[pi];
+            const bool first = pi == 0, last = pi + 1 == passes.size();
+            NttPassArgs a{};
+            a.src = first ? coeffs + c0 * n : scratch;
+            a.src_stride = n;
+            a.tab = lde_tab;
+            a.tw_small = tw[12];
+            a.tw_pass = ps.s_lo ? tw[ps.s_lo + ps.logr] : nullptr;
+            a.vcols = cc << rate;
+            a.L = lg_n;
+            a.s_lo = ps.s_lo;
+            a.rate = rate;
+            a.cols = (uint32_t)cc;
+            a.row_stride = cols;
+            a.dst = last ? rows + c0 : scratch;
+            a.dst_stride = n;
+            uint64_t grid;
+            uint32_t tile;
+            if (last) {
+                const uint32_t W = (uint32_t)std::min<uint64_t>(n, PASS_TILE / 16);
+                tile = 16 * W;
+                grid = (n / W) * ((cc + 15) / 16) * (1ULL << rate);
+                if (first) launch_pass<0, LOAD_COSETS, STORE_ROWS>(ps.logr, a, grid, tile * 8, stream);
+                else launch_pass<0, LOAD_PLAIN, STORE_ROWS>(ps.logr, a, grid, tile * 8, stream);
+            } else {
+                tile = (uint32_t)std::min<uint64_t>(n, PASS_TILE);
+                grid = a.vcols * (n / tile);
+                if (first) launch_pass<0, LOAD_COSETS, STORE_SAME>(ps.logr, a, grid, tile * 8, stream);
+                else launch_pass<0, LOAD_PLAIN, STORE_SAME>(ps.logr, a, grid, tile * 8, stream);
+            }
+            ZK_CUDA(cudaGetLastError());
+        }
+    }
+}
+
+// Passes of the fused LDE of 2^lg_n-point columns: (s_lo, log radix) pairs.
+std::vector<std::pair<uint32_t, uint32_t>> lde_rows_passes(uint32_t lg_n)
+{
+    std::vector<std::pair<uint32_t, uint32_t>> v;
+    for (const Pass &p : plan_passes(lg_n, true)) v.push_back({p.s_lo, p.logr});
+    return v;
+}
+
 uint64_t lde_rows_scratch_elems(uint32_t lg_n, uint32_t rate, uint64_t cols)
 {
     if (plan_passes(lg_n, true).size() == 1) return 0;

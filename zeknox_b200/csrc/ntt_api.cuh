@@ -2,6 +2,9 @@
 #pragma once
 #include <stdint.h>
 
+#include <utility>
+#include <vector>
+
 #include "runtime.cuh"
 
 namespace zk {
@@ -22,6 +25,15 @@ void lde_rows_device(DeviceCtx &c, uint64_t *rows, const uint64_t *coeffs, uint3
                      uint64_t coset_gen, uint64_t *scratch);
 uint64_t lde_rows_scratch_elems(uint32_t lg_n, uint32_t rate, uint64_t cols);
 uint32_t lde_rows_chunk_cols(uint32_t lg_n, uint32_t rate, uint64_t cols);
+
+// The fused LDE with caller-provided tables and scratch (no allocation, no
+// DeviceCtx): tw[lg] = w_{2^lg}^t tables for lg 12 and every pass's lg M,
+// lde_tab = (g * w_N^c)^j, scratch = 2^(lg_n+rate) * chunk_cols words when
+// the size needs more than one pass.  Launches on `stream`.
+void lde_rows_explicit(cudaStream_t stream, uint64_t *rows, const uint64_t *coeffs, uint32_t lg_n, uint32_t rate,
+                       uint64_t cols, const uint64_t *lde_tab, const uint64_t *const *tw, uint64_t *scratch,
+                       uint64_t chunk_cols);
+std::vector<std::pair<uint32_t, uint32_t>> lde_rows_passes(uint32_t lg_n);
 
 // Build every table a commit of this shape uses (before graph capture).
 void prepare_tables(DeviceCtx &c, uint32_t lg_n, uint32_t rate, uint64_t coset_gen, bool values);
