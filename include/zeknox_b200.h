@@ -90,6 +90,40 @@ RustError zeknox_lde_rows(size_t device_id, uint64_t *rows, const uint64_t *coef
 RustError zeknox_lde_rows_noalloc(size_t device_id, uint64_t *rows, const uint64_t *coeffs, uint32_t lg_n,
                                   uint32_t rate_bits, uint32_t cols, uint64_t coset_gen, void *stream);
 
+/* ---- Serving: continuous batching of commit requests on one GPU ----
+ *
+ * A server owns a device-memory budget and `slots` streams.  Requests
+ * (zk_serve_request) are queued by any host thread; a server thread admits
+ * them in arrival order whenever a slot is free and the job's memory (its
+ * leaves, digests, caps and scratch) fits the budget, runs the commit on the
+ * slot's stream -- so admitted jobs overlap on the device -- copies the caps to
+ * the request's host buffer, and records the latency (submit -> caps on host).
+ * Results stay in server-owned device memory until released. */
+typedef struct {
+    uint32_t lg_n, rate_bits, cols, cap_height, hash_type, input_is_values;
+    uint64_t coset_gen;       /* 0 means 7 */
+    const uint64_t *input;    /* device: cols x 2^lg_n, column-major; must stay valid until done */
+    uint64_t *caps_host;      /* host buffer of 2^cap_height x 4 words, filled on completion (may be NULL) */
+} zk_serve_request;
+
+typedef struct {
+    int status;               /* 0 queued, 1 running, 2 done, < 0 failed (negated cudaError or -1) */
+    double latency_ms;        /* submit -> caps on host (done only) */
+    double queue_ms;          /* submit -> admitted */
+    const uint64_t *leaves, *digests, *caps;  /* device results (done, until released) */
+} zk_serve_result;
+
+RustError zeknox_server_create(size_t device_id, uint64_t budget_bytes, uint32_t slots, void **server);
+RustError zeknox_server_submit(void *server, const zk_serve_request *req, uint64_t *ticket);
+/* Wait up to timeout_ms (< 0: forever) for the ticket; fills *result. */
+RustError zeknox_server_wait(void *server, uint64_t ticket, double timeout_ms, zk_serve_result *result);
+/* Free the ticket's device results (returns their bytes to the budget). */
+RustError zeknox_server_release(void *server, uint64_t ticket);
+/* Bytes currently admitted against the budget, and the peak so far. */
+RustError zeknox_server_stats(void *server, uint64_t *in_use_bytes, uint64_t *peak_bytes, uint64_t *completed);
+/* Waits for all admitted work, frees everything. */
+RustError zeknox_server_destroy(void *server);
+
 /* Number of kernels this library has launched so far in the process. */
 uint64_t zeknox_launch_count(void);
 

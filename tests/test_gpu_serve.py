@@ -1,0 +1,59 @@
+"""Continuous-batching server: every result in the mix equals the same job
+committed alone, the device-memory budget is never exceeded, and jobs that do
+not fit wait for memory instead of failing."""
+import numpy as np
+import pytest
+import torch
+
+import zeknox_b200 as zk
+from oracle import oracle as O
+from tests.helpers import to_dev, to_np
+
+pytestmark = pytest.mark.gpu
+
+SHAPES = [(12, 3, 64, 4, 0), (10, 2, 200, 3, 3), (14, 1, 33, 4, 4), (9, 3, 256, 2, 0), (13, 2, 17, 4, 1),
+          (11, 3, 100, 4, 3), (15, 1, 8, 0, 0), (12, 2, 129, 4, 3)]
+
+
+def alone(lg, rate, cols, cap, h, inp):
+    N = 1 << (lg + rate)
+    leaves = torch.zeros(N * cols, dtype=torch.int64, device="cuda")
+    n_dig, n_cap = zk.merkle_sizes(N, cap)
+    dig = torch.zeros(max(n_dig, 1) * 4, dtype=torch.int64, device="cuda")
+    caps = torch.zeros(n_cap * 4, dtype=torch.int64, device="cuda")
+    zk.commit(0, zk.commit_job(lg, rate, cols, cap, h, inp, leaves, dig, caps))
+    return to_np(caps), to_np(leaves)
+
+
+@pytest.mark.parametrize("budget_mb,slots", [(4096, 8), (96, 2)])
+def test_results_same_alone_and_in_the_mix(budget_mb, slots):
+    inputs = [to_dev(O.field_data(700 + i, s[2] << s[0])) for i, s in enumerate(SHAPES)]
+    solo = [alone(*s, inp) for s, inp in zip(SHAPES, inputs)]
+    caps_host = [torch.zeros((1 << s[3]) * 4, dtype=torch.int64).pin_memory() for s in SHAPES]
+    with zk.Server(0, budget_mb << 20, slots) as srv:
+        tickets = [srv.submit(*s, inp, caps_host=ch) for s, inp, ch in zip(SHAPES, inputs, caps_host)]
+        for t, (caps, leaves), ch, s in zip(tickets, solo, caps_host, SHAPES):
+            r = srv.wait(t)
+            assert r.status == 2, r.status
+            assert r.latency_ms >= r.queue_ms >= 0
+            assert np.array_equal(ch.numpy().view(np.uint64), caps)
+            N = 1 << (s[0] + s[1])
+            got = torch.empty(N * s[2], dtype=torch.int64, device="cuda")
+            torch.cuda.synchronize()
+            zk.load()  # results are device pointers owned by the server
+            import ctypes
+            ctypes.memmove  # noqa: B018
+            cudart = torch.cuda.cudart()
+            assert cudart.cudaMemcpy(got.data_ptr(), r.leaves, N * s[2] * 8, 3) == 0  # device to device
+            assert np.array_equal(to_np(got), leaves)
+            srv.release(t)
+        st = srv.stats()
+        assert st["peak"] <= budget_mb << 20
+        assert st["in_use"] == 0 and st["completed"] == len(SHAPES)
+
+
+def test_rejects_request_larger_than_budget():
+    inp = to_dev(O.field_data(1, 64 << 12))
+    with zk.Server(0, 1 << 20, 2) as srv:
+        with pytest.raises(zk.ZeknoxError):
+            srv.submit(12, 3, 64, 4, 0, inp)

@@ -33,7 +33,8 @@ ABI_SYMBOLS = [
 ]
 EXT_SYMBOLS = ["zeknox_last_error", "zeknox_commit", "zeknox_commit_batch", "zeknox_commit_scratch_words",
                "zeknox_lde_rows", "zeknox_launch_count", "zeknox_measure_mul_rate", "zeknox_merkle_batch",
-               "zeknox_lde_rows_noalloc"]
+               "zeknox_lde_rows_noalloc", "zeknox_server_create", "zeknox_server_submit", "zeknox_server_wait",
+               "zeknox_server_release", "zeknox_server_stats", "zeknox_server_destroy"]
 
 
 class RustError(ctypes.Structure):
@@ -93,6 +94,19 @@ class MerkleJob(ctypes.Structure):
         ("cap_height", ctypes.c_uint32),
         ("hash_type", ctypes.c_uint32),
     ]
+
+
+class ServeRequest(ctypes.Structure):
+    """include/zeknox_b200.h zk_serve_request."""
+    _fields_ = [("lg_n", ctypes.c_uint32), ("rate_bits", ctypes.c_uint32), ("cols", ctypes.c_uint32),
+                ("cap_height", ctypes.c_uint32), ("hash_type", ctypes.c_uint32), ("input_is_values", ctypes.c_uint32),
+                ("coset_gen", ctypes.c_uint64), ("input", ctypes.c_void_p), ("caps_host", ctypes.c_void_p)]
+
+
+class ServeResult(ctypes.Structure):
+    """include/zeknox_b200.h zk_serve_result."""
+    _fields_ = [("status", ctypes.c_int), ("latency_ms", ctypes.c_double), ("queue_ms", ctypes.c_double),
+                ("leaves", ctypes.c_void_p), ("digests", ctypes.c_void_p), ("caps", ctypes.c_void_p)]
 
 
 class ZeknoxError(RuntimeError):
@@ -157,6 +171,18 @@ def load():
     L.zeknox_measure_mul_rate.argtypes = [sz]
     L.zeknox_lde_rows_noalloc.restype = RustError
     L.zeknox_lde_rows_noalloc.argtypes = [sz, vp, vp, u32, u32, u32, u64, vp]
+    L.zeknox_server_create.restype = RustError
+    L.zeknox_server_create.argtypes = [sz, u64, u32, ctypes.POINTER(ctypes.c_void_p)]
+    L.zeknox_server_submit.restype = RustError
+    L.zeknox_server_submit.argtypes = [vp, ctypes.POINTER(ServeRequest), ctypes.POINTER(u64)]
+    L.zeknox_server_wait.restype = RustError
+    L.zeknox_server_wait.argtypes = [vp, u64, ctypes.c_double, ctypes.POINTER(ServeResult)]
+    L.zeknox_server_release.restype = RustError
+    L.zeknox_server_release.argtypes = [vp, u64]
+    L.zeknox_server_stats.restype = RustError
+    L.zeknox_server_stats.argtypes = [vp, ctypes.POINTER(u64), ctypes.POINTER(u64), ctypes.POINTER(u64)]
+    L.zeknox_server_destroy.restype = RustError
+    L.zeknox_server_destroy.argtypes = [vp]
     L.zeknox_merkle_batch.restype = RustError
     L.zeknox_merkle_batch.argtypes = [sz, ctypes.POINTER(MerkleJob), u32]
     _lib = L
@@ -372,3 +398,46 @@ def merkle_batch(device_id, jobs):
     """zeknox_merkle_batch: several forests as one cached CUDA graph."""
     arr = (MerkleJob * len(jobs))(*jobs)
     _check(load().zeknox_merkle_batch(device_id, arr, len(jobs)))
+
+
+class Server:
+    """Continuous-batching commit server (zeknox_server_*): requests are admitted
+    in arrival order as slots and the device-memory budget allow, and overlap on
+    the GPU."""
+
+    def __init__(self, device_id=0, budget_bytes=120 << 30, slots=8):
+        h = ctypes.c_void_p()
+        _check(load().zeknox_server_create(device_id, budget_bytes, slots, ctypes.byref(h)))
+        self._h = h
+
+    def submit(self, lg_n, rate_bits, cols, cap_height, hash_type, inp, caps_host=None, input_is_values=False,
+               coset_gen=7):
+        r = ServeRequest(lg_n, rate_bits, cols, cap_height, hash_type, int(bool(input_is_values)), coset_gen,
+                         inp.data_ptr(), caps_host.data_ptr() if caps_host is not None else None)
+        t = ctypes.c_uint64()
+        _check(load().zeknox_server_submit(self._h, ctypes.byref(r), ctypes.byref(t)))
+        return t.value
+
+    def wait(self, ticket, timeout_ms=-1.0):
+        res = ServeResult()
+        _check(load().zeknox_server_wait(self._h, ticket, timeout_ms, ctypes.byref(res)))
+        return res
+
+    def release(self, ticket):
+        _check(load().zeknox_server_release(self._h, ticket))
+
+    def stats(self):
+        a, b, c = ctypes.c_uint64(), ctypes.c_uint64(), ctypes.c_uint64()
+        _check(load().zeknox_server_stats(self._h, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c)))
+        return {"in_use": a.value, "peak": b.value, "completed": c.value}
+
+    def close(self):
+        if self._h:
+            _check(load().zeknox_server_destroy(self._h))
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()

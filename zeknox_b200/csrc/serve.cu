@@ -1,0 +1,336 @@
+// serve.cu -- continuous-batching commit server (include/zeknox_b200.h).
+//
+// Host side: any thread submits requests into a FIFO; one server thread per
+// server admits the head of the queue whenever a slot stream is idle and the
+// job's device memory fits the budget, enqueues the whole commit (allocation,
+// LDE, Merkle, caps copy-out) on that slot's stream, and polls the slot
+// events to retire finished jobs.  Device side: jobs on different slots
+// overlap; twiddle, coset and round-constant tables stay resident in the
+// device context across requests.
+#include <cuda_runtime.h>
+#include <string.h>
+
+#include <chrono>
+#include <condition_variable>
+#include <deque>
+#include <map>
+#include <mutex>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "../../include/zeknox_b200.h"
+#include "batch.cuh"
+#include "runtime.cuh"
+
+namespace zk {
+namespace {
+
+using Clock = std::chrono::steady_clock;
+
+struct Ticket {
+    zk_serve_request req;
+    Clock::time_point t_submit, t_admit, t_done;
+    int status = 0;  // 0 queued, 1 running, 2 done, < 0 failed
+    int slot = -1;
+    uint64_t bytes = 0;
+    uint64_t *leaves = nullptr, *digests = nullptr, *caps = nullptr, *scratch = nullptr;
+    cudaEvent_t done_ev = nullptr;
+};
+
+struct Server {
+    DeviceCtx *ctx = nullptr;
+    uint64_t budget = 0, in_use = 0, peak = 0, completed = 0;
+    std::vector<cudaStream_t> slot_stream;
+    std::vector<uint64_t> slot_ticket;  // 0 = idle
+    std::mutex mu;
+    std::condition_variable cv;  // signalled on submit, completion, release, stop
+    std::deque<uint64_t> queue;
+    std::map<uint64_t, Ticket> tickets;
+    uint64_t next_id = 1;
+    bool stop = false;
+    std::thread worker;
+
+    static uint64_t job_bytes(const zk_serve_request &r)
+    {
+        const uint64_t N = 1ULL << (r.lg_n + r.rate_bits);
+        const uint64_t caps = 1ULL << r.cap_height;
+        return 8 * (N * r.cols + 8 * (N - caps) + 4 * caps +
+                    commit_scratch_words(r.lg_n, r.rate_bits, r.cols, r.input_is_values != 0));
+    }
+
+    void run_one(uint64_t id, int slot)
+    {
+        Ticket &t = tickets[id];
+        const zk_serve_request &r = t.req;
+        cudaStream_t s = slot_stream[slot];
+        const uint64_t N = 1ULL << (r.lg_n + r.rate_bits);
+        const uint64_t n_caps = 1ULL << r.cap_height;
+        try {
+            std::lock_guard<std::recursive_mutex> lk(ctx->mu);
+            ZK_CUDA(cudaSetDevice(ctx->id));
+            ZK_CUDA(cudaMallocAsync((void **)&t.leaves, N * r.cols * 8, s));
+            if (N > n_caps) ZK_CUDA(cudaMallocAsync((void **)&t.digests, (N - n_caps) * 64, s));
+            ZK_CUDA(cudaMallocAsync((void **)&t.caps, n_caps * 32, s));
+            const uint64_t sw = commit_scratch_words(r.lg_n, r.rate_bits, r.cols, r.input_is_values != 0);
+            if (sw) ZK_CUDA(cudaMallocAsync((void **)&t.scratch, sw * 8, s));
+            zk_commit_job j{};
+            j.lg_n = r.lg_n;
+            j.rate_bits = r.rate_bits;
+            j.cols = r.cols;
+            j.cap_height = r.cap_height;
+            j.hash_type = r.hash_type;
+            j.input_is_values = r.input_is_values;
+            j.coset_gen = r.coset_gen;
+            j.input = r.input;
+            j.leaves = t.leaves;
+            j.digests = t.digests;
+            j.caps = t.caps;
+            prepare_job(*ctx, j);
+            ZK_CUDA(cudaStreamSynchronize(ctx->stream));  // tables built on the context stream
+            commit_enqueue(*ctx, j, s, t.scratch);
+            if (t.scratch) {
+                ZK_CUDA(cudaFreeAsync(t.scratch, s));
+                t.scratch = nullptr;
+            }
+            if (r.caps_host) ZK_CUDA(cudaMemcpyAsync(r.caps_host, t.caps, n_caps * 32, cudaMemcpyDeviceToHost, s));
+            ZK_CUDA(cudaEventCreateWithFlags(&t.done_ev, cudaEventDisableTiming));
+            ZK_CUDA(cudaEventRecord(t.done_ev, s));
+            t.status = 1;
+        } catch (const cuda_failure &e) {
+            t.status = e.code < 0 ? e.code : -1;
+        } catch (const std::exception &) {
+            t.status = -1;
+        }
+    }
+
+    void loop()
+    {
+        std::unique_lock<std::mutex> lk(mu);
+        while (true) {
+            // retire finished jobs
+            bool progressed = false;
+            for (size_t k = 0; k < slot_ticket.size(); k++) {
+                uint64_t id = slot_ticket[k];
+                if (!id) continue;
+                Ticket &t = tickets[id];
+                if (t.status < 0) {
+                    slot_ticket[k] = 0;
+                    progressed = true;
+                    continue;
+                }
+                cudaError_t q = cudaEventQuery(t.done_ev);
+                if (q == cudaErrorNotReady) continue;
+                t.t_done = Clock::now();
+                t.status = q == cudaSuccess ? 2 : -(int)q;
+                if (q != cudaSuccess) (void)cudaGetLastError();
+                cudaEventDestroy(t.done_ev);
+                t.done_ev = nullptr;
+                slot_ticket[k] = 0;
+                completed++;
+                progressed = true;
+            }
+            if (progressed) cv.notify_all();
+            // admit in arrival order
+            while (!queue.empty()) {
+                const uint64_t id = queue.front();
+                Ticket &t = tickets[id];
+                int slot = -1;
+                for (size_t k = 0; k < slot_ticket.size(); k++)
+                    if (!slot_ticket[k]) {
+                        slot = (int)k;
+                        break;
+                    }
+                if (slot < 0 || in_use + t.bytes > budget) break;
+                queue.pop_front();
+                in_use += t.bytes;
+                peak = in_use > peak ? in_use : peak;
+                t.slot = slot;
+                t.t_admit = Clock::now();
+                slot_ticket[slot] = id;
+                run_one(id, slot);
+                if (t.status < 0) {
+                    // could not start: give the memory back now
+                    in_use -= t.bytes;
+                    t.bytes = 0;
+                }
+                cv.notify_all();
+            }
+            bool busy = false;
+            for (uint64_t id : slot_ticket) busy |= id != 0;
+            if (stop && !busy && queue.empty()) break;
+            if (busy) {
+                lk.unlock();
+                std::this_thread::sleep_for(std::chrono::microseconds(50));
+                lk.lock();
+            } else {
+                cv.wait_for(lk, std::chrono::milliseconds(5));
+            }
+        }
+    }
+};
+
+Server *as_server(void *p)
+{
+    if (!p) throw arg_failure("null server");
+    return (Server *)p;
+}
+
+RustError to_error(int code, const std::string &msg)
+{
+    RustError e;
+    e.code = code;
+    e.message = msg.empty() ? nullptr : strdup(msg.c_str());
+    return e;
+}
+
+template <class F>
+RustError guard(F &&f)
+{
+    try {
+        f();
+        return RustError{0, nullptr};
+    } catch (const arg_failure &e) {
+        return to_error(e.code, e.what());
+    } catch (const cuda_failure &e) {
+        return to_error(e.code, e.what());
+    } catch (const std::exception &e) {
+        return to_error(-(int)cudaErrorUnknown, e.what());
+    }
+}
+
+}  // namespace
+}  // namespace zk
+
+using zk::Server;
+
+extern "C" RustError zeknox_server_create(size_t device_id, uint64_t budget_bytes, uint32_t slots, void **server)
+{
+    return zk::guard([&] {
+        if (!server) throw zk::arg_failure("null out pointer");
+        if (slots == 0 || slots > 64) throw zk::arg_failure("slots must be 1..64");
+        zk::DeviceCtx &c = zk::device(device_id);
+        Server *s = new Server();
+        s->ctx = &c;
+        s->budget = budget_bytes;
+        s->slot_stream.resize(slots);
+        s->slot_ticket.assign(slots, 0);
+        for (auto &st : s->slot_stream) ZK_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+        s->worker = std::thread([s] {
+            cudaSetDevice(s->ctx->id);
+            s->loop();
+        });
+        *server = s;
+    });
+}
+
+extern "C" RustError zeknox_server_submit(void *server, const zk_serve_request *req, uint64_t *ticket)
+{
+    return zk::guard([&] {
+        Server *s = zk::as_server(server);
+        if (!req || !ticket) throw zk::arg_failure("null pointer");
+        zk_commit_job j{};
+        j.lg_n = req->lg_n;
+        j.rate_bits = req->rate_bits;
+        j.cols = req->cols;
+        j.cap_height = req->cap_height;
+        j.hash_type = req->hash_type;
+        j.input = req->input;
+        j.leaves = (uint64_t *)1;  // buffers are the server's: check shape only
+        j.digests = (uint64_t *)1;
+        j.caps = (uint64_t *)1;
+        zk::check_job(j);
+        const uint64_t bytes = Server::job_bytes(*req);
+        std::lock_guard<std::mutex> lk(s->mu);
+        if (bytes > s->budget) throw zk::arg_failure("request needs more device memory than the server's budget");
+        const uint64_t id = s->next_id++;
+        zk::Ticket &t = s->tickets[id];
+        t.req = *req;
+        t.bytes = bytes;
+        t.t_submit = zk::Clock::now();
+        s->queue.push_back(id);
+        *ticket = id;
+        s->cv.notify_all();
+    });
+}
+
+extern "C" RustError zeknox_server_wait(void *server, uint64_t ticket, double timeout_ms, zk_serve_result *result)
+{
+    return zk::guard([&] {
+        Server *s = zk::as_server(server);
+        std::unique_lock<std::mutex> lk(s->mu);
+        auto it = s->tickets.find(ticket);
+        if (it == s->tickets.end()) throw zk::arg_failure("unknown ticket");
+        auto done = [&] { return it->second.status == 2 || it->second.status < 0; };
+        if (timeout_ms < 0) s->cv.wait(lk, done);
+        else s->cv.wait_for(lk, std::chrono::duration<double, std::milli>(timeout_ms), done);
+        const zk::Ticket &t = it->second;
+        if (result) {
+            result->status = t.status;
+            result->latency_ms = t.status == 2 ? std::chrono::duration<double, std::milli>(t.t_done - t.t_submit).count() : 0;
+            result->queue_ms = t.status >= 1 || t.status < 0
+                                   ? std::chrono::duration<double, std::milli>(t.t_admit - t.t_submit).count()
+                                   : 0;
+            result->leaves = t.status == 2 ? t.leaves : nullptr;
+            result->digests = t.status == 2 ? t.digests : nullptr;
+            result->caps = t.status == 2 ? t.caps : nullptr;
+        }
+    });
+}
+
+extern "C" RustError zeknox_server_release(void *server, uint64_t ticket)
+{
+    return zk::guard([&] {
+        Server *s = zk::as_server(server);
+        std::lock_guard<std::mutex> lk(s->mu);
+        auto it = s->tickets.find(ticket);
+        if (it == s->tickets.end()) throw zk::arg_failure("unknown ticket");
+        zk::Ticket &t = it->second;
+        if (t.status == 0 || t.status == 1) throw zk::arg_failure("ticket still queued or running");
+        {
+            std::lock_guard<std::recursive_mutex> dl(s->ctx->mu);
+            ZK_CUDA(cudaSetDevice(s->ctx->id));
+            cudaStream_t st = t.slot >= 0 ? s->slot_stream[t.slot] : s->ctx->stream;
+            for (uint64_t *p : {t.leaves, t.digests, t.caps, t.scratch})
+                if (p) (void)cudaFreeAsync(p, st);
+        }
+        s->in_use -= t.bytes;
+        s->tickets.erase(it);
+        s->cv.notify_all();
+    });
+}
+
+extern "C" RustError zeknox_server_stats(void *server, uint64_t *in_use_bytes, uint64_t *peak_bytes,
+                                         uint64_t *completed)
+{
+    return zk::guard([&] {
+        Server *s = zk::as_server(server);
+        std::lock_guard<std::mutex> lk(s->mu);
+        if (in_use_bytes) *in_use_bytes = s->in_use;
+        if (peak_bytes) *peak_bytes = s->peak;
+        if (completed) *completed = s->completed;
+    });
+}
+
+extern "C" RustError zeknox_server_destroy(void *server)
+{
+    return zk::guard([&] {
+        Server *s = zk::as_server(server);
+        {
+            std::lock_guard<std::mutex> lk(s->mu);
+            s->stop = true;
+            s->cv.notify_all();
+        }
+        s->worker.join();
+        std::lock_guard<std::recursive_mutex> dl(s->ctx->mu);
+        ZK_CUDA(cudaSetDevice(s->ctx->id));
+        for (auto &kv : s->tickets)
+            for (uint64_t *p : {kv.second.leaves, kv.second.digests, kv.second.caps, kv.second.scratch})
+                if (p) (void)cudaFreeAsync(p, s->slot_stream[kv.second.slot >= 0 ? kv.second.slot : 0]);
+        for (auto &st : s->slot_stream) {
+            cudaStreamSynchronize(st);
+            cudaStreamDestroy(st);
+        }
+        delete s;
+    });
+}
