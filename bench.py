@@ -67,7 +67,7 @@ class ClockSampler:
     def start(self):
         try:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.Q,
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", "50"],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
@@ -455,6 +455,84 @@ def run_hashes(args):
     print(json.dumps(line), flush=True)
 
 
+def run_serve(args):
+    """Serving: a Poisson stream of LDE + Poseidon commit requests (log2 size
+    U{12..22}, columns U{16..256}, rate_bits 3, cap height 4) admitted by
+    zeknox_server against a 120 GB budget; arrival rate 0.7x the capacity
+    measured with serial plain calls.  Reports p50/p99 latency (submit -> caps
+    on host) and throughput vs the serial plain calls."""
+    import threading as th
+
+    import torch
+    import zeknox_b200 as zk
+    torch.cuda.set_device(0)
+    rng = np.random.default_rng(5)
+    reqs = []
+    for k in range(args.requests):
+        lg, cols = int(rng.integers(12, 23)), int(rng.integers(16, 257))
+        reqs.append((lg, 3, cols, 4, 0, dev_field(cols << lg, 5000 + k)))
+    elems = [(1 << (lg + r)) * c for lg, r, c, _, _, _ in reqs]
+    # serial plain calls: one synchronous zeknox_commit per request
+    serial = []
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    for lg, r, c, cap, h, inp in reqs:
+        N = 1 << (lg + r)
+        leaves = torch.empty(N * c, dtype=torch.int64, device="cuda")
+        n_dig, n_cap = zk.merkle_sizes(N, cap)
+        dig = torch.empty(n_dig * 4, dtype=torch.int64, device="cuda")
+        caps = torch.empty(n_cap * 4, dtype=torch.int64, device="cuda")
+        job = zk.commit_job(lg, r, c, cap, h, inp, leaves, dig, caps)
+        zk.commit(0, job)  # tables, pool
+        a.record()
+        zk.commit(0, job)
+        b.record()
+        torch.cuda.synchronize()
+        serial.append(a.elapsed_time(b))
+        del leaves, dig, caps
+        torch.cuda.empty_cache()
+    capacity = sum(elems) / (sum(serial) * 1e-3)
+    rate = 0.7 / (np.mean(serial) * 1e-3)  # requests per second
+    gaps = rng.exponential(1.0 / rate, size=len(reqs))
+    caps_host = [torch.zeros((1 << cap) * 4, dtype=torch.int64).pin_memory() for _, _, _, cap, _, _ in reqs]
+    lat, queue = [None] * len(reqs), [None] * len(reqs)
+    done_t = [None] * len(reqs)
+    with zk.Server(0, 120 << 30, 8) as srv:
+        tickets = [None] * len(reqs)
+        ready = th.Semaphore(0)
+
+        def reaper():
+            for i in range(len(reqs)):
+                ready.acquire()
+                r = srv.wait(tickets[i])
+                assert r.status == 2, r.status
+                lat[i], queue[i], done_t[i] = r.latency_ms, r.queue_ms, time.perf_counter()
+                srv.release(tickets[i])
+
+        rt = th.Thread(target=reaper)
+        rt.start()
+        t0 = time.perf_counter()
+        when = t0
+        for i, (lg, r, c, cap, h, inp) in enumerate(reqs):
+            when += gaps[i]
+            delay = when - time.perf_counter()
+            if delay > 0:
+                time.sleep(delay)
+            tickets[i] = srv.submit(lg, r, c, cap, h, inp, caps_host=caps_host[i])
+            ready.release()
+        rt.join()
+        st = srv.stats()
+    span = max(done_t) - t0
+    line = {"metric": "serving LDE+Poseidon commit: p50/p99 latency and throughput", "unit": "ms",
+            "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+            "mean_queue_ms": float(np.mean(queue)), "throughput_elems_per_s": sum(elems) / span,
+            "serial_plain_elems_per_s": capacity, "offered_load": 0.7, "requests": len(reqs),
+            "arrival_rate_per_s": rate, "peak_budget_bytes": st["peak"], "budget_bytes": 120 << 30,
+            "slots": 8, "dtype": "u64",
+            "config": {"workload": "Poisson stream: lg_n U{12..22}, cols U{16..256}, rate_bits 3, Poseidon, cap 4, "
+                                   "120 GB budget, 8 slots, seed 5"}}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -466,7 +544,8 @@ def main():
     ap.add_argument("--lg-n", type=int, default=LG_N, help="log2 coefficients per column (profiling cases)")
     ap.add_argument("--only", default=None, choices=["lde", "merkle"],
                     help="profiling: run only this stage for warmup+steps iterations and exit")
-    ap.add_argument("--workload", default="commit", choices=["commit", "batch", "hashes"],
+    ap.add_argument("--requests", type=int, default=16, help="serve workload: number of requests")
+    ap.add_argument("--workload", default="commit", choices=["commit", "batch", "hashes", "serve"],
                     help="commit: the headline line; batch: uneven 64-job batch vs plain calls; hashes: 2^20 x 135 "
                          "forests with Poseidon2, Monolith and Keccak")
     ap.add_argument("--budget-gb", type=float, default=48.0, help="batch workload: device memory per wave")
@@ -481,6 +560,8 @@ def main():
         return run_batch(args)
     if args.workload == "hashes":
         return run_hashes(args)
+    if args.workload == "serve":
+        return run_serve(args)
     if world > 1:
         import datetime
 

@@ -39,12 +39,10 @@ def test_results_same_alone_and_in_the_mix(budget_mb, slots):
             assert np.array_equal(ch.numpy().view(np.uint64), caps)
             N = 1 << (s[0] + s[1])
             got = torch.empty(N * s[2], dtype=torch.int64, device="cuda")
-            torch.cuda.synchronize()
-            zk.load()  # results are device pointers owned by the server
-            import ctypes
-            ctypes.memmove  # noqa: B018
-            cudart = torch.cuda.cudart()
-            assert cudart.cudaMemcpy(got.data_ptr(), r.leaves, N * s[2] * 8, 3) == 0  # device to device
+            # results are device pointers owned by the server: copy the leaves out
+            from cuda.bindings import runtime as rt
+            err, = rt.cudaMemcpy(got.data_ptr(), r.leaves, N * s[2] * 8, rt.cudaMemcpyKind.cudaMemcpyDeviceToDevice)
+            assert err == rt.cudaError_t.cudaSuccess
             assert np.array_equal(to_np(got), leaves)
             srv.release(t)
         st = srv.stats()
