@@ -33,7 +33,8 @@ typedef struct {
     uint32_t hash_type;       /* HashType: 0 Poseidon, 1 Keccak, 3 Poseidon2, 4 Monolith */
     uint32_t input_is_values; /* 0: columns are coefficients; 1: evaluations on H (inverse NTT first) */
     uint64_t coset_gen;       /* coset shift; 0 means 7 */
-    const uint64_t *input;    /* cols x 2^lg_n, column-major */
+    const uint64_t *input;    /* cols x 2^lg_n, column-major; device memory, or (zeknox_commit only)
+                                 host memory, copied in column chunks that overlap the transform */
     uint64_t *leaves;         /* out: 2^(lg_n+rate_bits) rows x cols; row r = evaluation rev(r) */
     uint64_t *digests;        /* out: 2 * (2^(lg_n+rate_bits) - 2^cap_height) x 4 */
     uint64_t *caps;           /* out: 2^cap_height x 4 */

@@ -153,3 +153,20 @@ def test_commit_on_caller_stream():
     s.synchronize()
     rows, d, cp = expect(c, lg, rate, cols, cap, h)
     assert np.array_equal(to_np(caps).reshape(-1, 4), cp)
+
+
+@pytest.mark.parametrize("pinned", [True, False])
+def test_commit_from_host_memory(pinned):
+    """zeknox_commit with a host input pointer stages the coefficients itself
+    (chunked copies overlapping the LDE); same commitment as a device input."""
+    lg, rate, cols, cap, h = 13, 3, 72, 4, 3
+    c = O.field_data(88, cols << lg)
+    host = torch.from_numpy(c.view(np.int64).copy())
+    if pinned:
+        host = host.pin_memory()
+    job, (leaves, dig, caps, n_dig) = alloc_job(lg, rate, cols, cap, h, host)
+    zk.commit(0, job)
+    rows, d, cp = expect(c, lg, rate, cols, cap, h)
+    assert np.array_equal(to_np(leaves), rows)
+    assert np.array_equal(to_np(caps).reshape(-1, 4), cp)
+    assert np.array_equal(to_np(dig).reshape(-1, 4)[:n_dig], d)

@@ -401,7 +401,9 @@ extern "C" RustError zeknox_commit(size_t device_id, const zk_commit_job *job, v
         zk::DeviceCtx &c = zk::device(device_id);
         std::lock_guard<std::recursive_mutex> lk(c.mu);
         cudaStream_t s = stream ? (cudaStream_t)stream : c.stream;
-        const uint64_t words = zeknox_commit_scratch_words(job);
+        const bool host_input = zk::is_host_pointer(job->input);
+        const uint64_t words = zk::commit_scratch_words(job->lg_n, job->rate_bits, job->cols, job->input_is_values != 0,
+                                                        host_input);
         zk::DevBuf scratch;
         if (words) {
             scratch.ctx = &c;
@@ -410,7 +412,7 @@ extern "C" RustError zeknox_commit(size_t device_id, const zk_commit_job *job, v
             scratch.p = c.alloc(words * 8);
             c.stream = keep;
         }
-        zk::commit_enqueue(c, *job, s, scratch.p);
+        zk::commit_enqueue(c, *job, s, scratch.p, host_input);
         if (scratch.p) {
             (void)cudaFreeAsync(scratch.p, s);
             scratch.p = nullptr;

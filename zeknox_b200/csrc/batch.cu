@@ -23,11 +23,22 @@ void check_job(const zk_commit_job &j)
         throw arg_failure("unsupported hash_type");
 }
 
-uint64_t commit_scratch_words(uint32_t lg_n, uint32_t rate_bits, uint32_t cols, bool values)
+uint64_t commit_scratch_words(uint32_t lg_n, uint32_t rate_bits, uint32_t cols, bool values, bool host_input)
 {
     uint64_t w = lde_rows_scratch_elems(lg_n, rate_bits, cols);
     if (values) w += 2 * ((uint64_t)cols << lg_n);  // coefficients + inverse-transform temporary
+    else if (host_input) w += (uint64_t)cols << lg_n;  // device staging of the coefficients
     return w;
+}
+
+bool is_host_pointer(const void *p)
+{
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        (void)cudaGetLastError();
+        return true;  // not known to CUDA: pageable host memory
+    }
+    return a.type == cudaMemoryTypeHost || a.type == cudaMemoryTypeUnregistered;
 }
 
 static uint64_t gen_of(const zk_commit_job &j) { return j.coset_gen ? j.coset_gen : ZK_GENERATOR; }
@@ -37,7 +48,7 @@ void prepare_job(DeviceCtx &c, const zk_commit_job &j)
     prepare_tables(c, j.lg_n, j.rate_bits, gen_of(j), j.input_is_values != 0);
 }
 
-void commit_enqueue(DeviceCtx &c, const zk_commit_job &j, cudaStream_t s, uint64_t *scratch)
+void commit_enqueue(DeviceCtx &c, const zk_commit_job &j, cudaStream_t s, uint64_t *scratch, bool host_input)
 {
     const uint64_t n = 1ULL << j.lg_n;
     const uint64_t N = n << j.rate_bits;
@@ -45,15 +56,20 @@ void commit_enqueue(DeviceCtx &c, const zk_commit_job &j, cudaStream_t s, uint64
     c.stream = s;
     try {
         const uint64_t *coeffs = j.input;
+        const uint64_t *host_coeffs = nullptr;
         uint64_t *lde_scratch = scratch;
+        uint64_t *extra = scratch + lde_rows_scratch_elems(j.lg_n, j.rate_bits, j.cols);
         if (j.input_is_values) {
             // evaluations on H -> coefficients (inverse NTT), then the LDE
-            uint64_t *cf = scratch + lde_rows_scratch_elems(j.lg_n, j.rate_bits, j.cols);
-            ZK_CUDA(cudaMemcpyAsync(cf, j.input, n * j.cols * 8, cudaMemcpyDeviceToDevice, s));
+            uint64_t *cf = extra;
+            ZK_CUDA(cudaMemcpyAsync(cf, j.input, n * j.cols * 8, cudaMemcpyDefault, s));
             ntt_batch_device(c, cf, j.lg_n, j.cols, true, false, cf + n * j.cols);
             coeffs = cf;
+        } else if (host_input) {
+            host_coeffs = j.input;
+            coeffs = extra;  // staging, filled chunk by chunk
         }
-        lde_rows_device(c, j.leaves, coeffs, j.lg_n, j.rate_bits, j.cols, gen_of(j), lde_scratch);
+        lde_rows_device(c, j.leaves, coeffs, j.lg_n, j.rate_bits, j.cols, gen_of(j), lde_scratch, host_coeffs);
         std::string err;
         const uint64_t n_caps = 1ULL << j.cap_height;
         if (!merkle_device(j.digests, j.caps, j.leaves, 2 * (N - n_caps), n_caps, N, j.cols, j.cap_height,
@@ -204,7 +220,8 @@ void commit_batch_graph(DeviceCtx &c, const zk_commit_job *jobs, uint32_t njobs)
     for (uint32_t i = 0; i < njobs; i++) {
         const zk_commit_job &j = jobs[i];
         cost[i] = (double)(1ULL << (j.lg_n + j.rate_bits)) * ((j.cols + 7) / 8 + 1);
-        words[i] = commit_scratch_words(j.lg_n, j.rate_bits, j.cols, j.input_is_values != 0);
+        if (is_host_pointer(j.input)) throw arg_failure("batched commits take device inputs");
+        words[i] = commit_scratch_words(j.lg_n, j.rate_bits, j.cols, j.input_is_values != 0, false);
         prepare_job(c, j);
     }
     ZK_CUDA(cudaStreamSynchronize(c.stream));

@@ -12,12 +12,16 @@ namespace zk {
 void check_job(const zk_commit_job &j);
 
 // Words of scratch commit_enqueue needs for a job of this shape.
-uint64_t commit_scratch_words(uint32_t lg_n, uint32_t rate_bits, uint32_t cols, bool values);
+uint64_t commit_scratch_words(uint32_t lg_n, uint32_t rate_bits, uint32_t cols, bool values, bool host_input = false);
+
+// True when p is host memory (pinned or pageable).
+bool is_host_pointer(const void *p);
 
 // Queue one commit on `s` using `scratch` (commit_scratch_words words, may be
 // null when that is 0).  Allocates nothing and never synchronises, so it can be
 // recorded into a CUDA graph once prepare_job() has built the tables it reads.
-void commit_enqueue(DeviceCtx &c, const zk_commit_job &j, cudaStream_t s, uint64_t *scratch);
+// host_input: j.input is host memory, staged through the scratch chunk by chunk.
+void commit_enqueue(DeviceCtx &c, const zk_commit_job &j, cudaStream_t s, uint64_t *scratch, bool host_input = false);
 void prepare_job(DeviceCtx &c, const zk_commit_job &j);
 
 // Run a batch of commits: the launches of every job are recorded once into a

@@ -343,7 +343,7 @@ uint64_t lde_rows_scratch_elems(uint32_t lg_n, uint32_t rate, uint64_t cols)
 }
 
 void lde_rows_device(DeviceCtx &c, uint64_t *rows, const uint64_t *coeffs, uint32_t lg_n, uint32_t rate, uint64_t cols,
-                     uint64_t coset_gen, uint64_t *scratch)
+                     uint64_t coset_gen, uint64_t *scratch, const uint64_t *host_coeffs)
 {
     const uint64_t n = 1ULL << lg_n;
     if (cols == 0) return;
@@ -356,8 +356,25 @@ void lde_rows_device(DeviceCtx &c, uint64_t *rows, const uint64_t *coeffs, uint3
         scratch = tmp.p;
     }
     const uint64_t *tab = c.lde_table(lg_n, rate, coset_gen % GL_P);
-    for (uint64_t c0 = 0; c0 < cols; c0 += chunk) {
+    if (host_coeffs) {
+        // coefficients are in host memory: copy chunk by chunk on the copy
+        // stream into `coeffs` (device staging) so chunk k+1 crosses PCIe while
+        // chunk k is transformed
+        cudaStream_t cs = c.copy_stream_get();
+        cudaEvent_t ready = c.chunk_event(0);
+        ZK_CUDA(cudaEventRecord(ready, c.stream));
+        ZK_CUDA(cudaStreamWaitEvent(cs, ready, 0));  // staging is free once earlier work on the stream is done
+        size_t k = 1;
+        for (uint64_t c0 = 0; c0 < cols; c0 += chunk, k++) {
+            const uint64_t cc = cols - c0 < chunk ? cols - c0 : chunk;
+            ZK_CUDA(cudaMemcpyAsync((void *)(coeffs + c0 * n), host_coeffs + c0 * n, cc * n * 8, cudaMemcpyHostToDevice, cs));
+            ZK_CUDA(cudaEventRecord(c.chunk_event(k), cs));
+        }
+    }
+    size_t k = 1;
+    for (uint64_t c0 = 0; c0 < cols; c0 += chunk, k++) {
         const uint64_t cc = cols - c0 < chunk ? cols - c0 : chunk;
+        if (host_coeffs) ZK_CUDA(cudaStreamWaitEvent(c.stream, c.chunk_event(k), 0));
         DifJob j{};
         j.src = coeffs + c0 * n;
         j.src_stride = n;

@@ -21,8 +21,12 @@ void lde_batch_device(DeviceCtx &c, uint64_t *out, const uint64_t *in, uint32_t 
 // Fused LDE + bit-reverse + transpose: rows[r * cols + b] = LDE_b[rev_{lg_n+rate}(r)]
 // (the leaf-major matrix compute_transpose_rev would produce).  `scratch` may
 // be null (allocated on the stream) or hold lde_rows_scratch_elems() words.
+// When host_coeffs is non-null the coefficients are read from that host
+// memory, staged chunk by chunk into `coeffs` (a device buffer of cols * 2^lg_n
+// words) on the context's copy stream, overlapping the transfer with the
+// transform of the previous chunk.
 void lde_rows_device(DeviceCtx &c, uint64_t *rows, const uint64_t *coeffs, uint32_t lg_n, uint32_t rate, uint64_t cols,
-                     uint64_t coset_gen, uint64_t *scratch);
+                     uint64_t coset_gen, uint64_t *scratch, const uint64_t *host_coeffs = nullptr);
 uint64_t lde_rows_scratch_elems(uint32_t lg_n, uint32_t rate, uint64_t cols);
 uint32_t lde_rows_chunk_cols(uint32_t lg_n, uint32_t rate, uint64_t cols);
 

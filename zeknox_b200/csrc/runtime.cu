@@ -79,6 +79,22 @@ DeviceCtx &device(size_t id)
     return *g_devs[id];
 }
 
+cudaStream_t DeviceCtx::copy_stream_get()
+{
+    if (!copy_stream) ZK_CUDA(cudaStreamCreateWithFlags(&copy_stream, cudaStreamNonBlocking));
+    return copy_stream;
+}
+
+cudaEvent_t DeviceCtx::chunk_event(size_t i)
+{
+    while (chunk_events.size() <= i) {
+        cudaEvent_t e;
+        ZK_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        chunk_events.push_back(e);
+    }
+    return chunk_events[i];
+}
+
 uint64_t *DeviceCtx::alloc(size_t bytes)
 {
     void *p = nullptr;

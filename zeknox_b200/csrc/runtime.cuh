@@ -57,6 +57,12 @@ struct DeviceCtx {
     const uint64_t *lde_table(uint32_t lg_n, uint32_t rate, uint64_t g);
     void set_coset(uint32_t lg, uint64_t gen);
 
+    // host->device staging of commit inputs: a copy stream and per-chunk events
+    cudaStream_t copy_stream = nullptr;
+    std::vector<cudaEvent_t> chunk_events;
+    cudaStream_t copy_stream_get();
+    cudaEvent_t chunk_event(size_t i);
+
     uint64_t *alloc(size_t bytes);
     void free(void *p);
     void sync();
