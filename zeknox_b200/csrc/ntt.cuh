@@ -103,36 +103,48 @@ struct NttPassArgs {
 };
 
 // Sub-step of the in-CTA R-point DIF: every task owns E elements spaced Q apart
-// inside a block of size R_cur = E * Q.
-template <int LOGE, int INV, int NT>
-__device__ __forceinline__ void dif_substep(uint64_t *sm, uint32_t tile_elems, uint32_t log_rcur,
-                                            const uint64_t *__restrict__ tw_small)
+// inside a block of size R_cur = E * Q.  The task base (block * R_cur + m_lo,
+// m_lo < Q) and the element offsets e * Q occupy disjoint bits, and swz() is
+// linear over XOR, so swz(base + e * Q) = swz(base) ^ swz(e * Q) with the
+// second term a compile-time constant.
+__host__ __device__ constexpr uint32_t swz_c(uint32_t w) { return w ^ (((w >> 4) ^ (w >> 8) ^ (w >> 12)) & 15u); }
+
+template <int LOGE, int INV, int NT, int LOG_RCUR>
+__device__ __forceinline__ void dif_substep(uint64_t *sm, uint32_t tile_elems, const uint64_t *__restrict__ tw_small)
 {
     constexpr int E = 1 << LOGE;
-    const uint32_t R_cur = 1u << log_rcur;
-    const uint32_t Q = R_cur >> LOGE;
+    constexpr uint32_t Q = 1u << (LOG_RCUR - LOGE);
     const uint32_t tasks = tile_elems >> LOGE;
-    const uint32_t log_q = log_rcur - LOGE;
     for (uint32_t t = threadIdx.x; t < tasks; t += NT) {
-        uint32_t m_lo = t & (Q - 1);
-        uint32_t blk = t >> log_q;  // block of R_cur (across groups)
-        uint32_t base = (blk << log_rcur) + m_lo;
+        const uint32_t m_lo = t & (Q - 1);
+        const uint32_t blk = t >> (LOG_RCUR - LOGE);  // block of R_cur (across groups)
+        const uint32_t sb = swz((blk << LOG_RCUR) + m_lo);
         uint64_t x[E];
 #pragma unroll
-        for (int e = 0; e < E; e++) x[e] = sm[swz(base + e * Q)];
+        for (int e = 0; e < E; e++) x[e] = sm[sb ^ swz_c(e * Q)];
         dif_regs<LOGE, INV>(x);
         if (Q > 1) {
             // position p gets w_{R_cur}^(m_lo * rev_e(p)); w_{R_cur} = w_4096^(4096 / R_cur)
-            uint32_t step = (uint32_t)m_lo << (12 - log_rcur);
+            const uint32_t step = m_lo << (12 - LOG_RCUR);
 #pragma unroll
             for (int p = 1; p < E; p++) {
-                uint32_t f = bitrev32((uint32_t)p, LOGE);
+                const uint32_t f = bitrev32((uint32_t)p, LOGE);
                 x[p] = gl_mul(x[p], __ldg(tw_small + ((step * f) & 4095u)));
             }
         }
 #pragma unroll
-        for (int e = 0; e < E; e++) sm[swz(base + e * Q)] = x[e];
+        for (int e = 0; e < E; e++) sm[sb ^ swz_c(e * Q)] = x[e];
     }
+}
+
+// All sub-steps of an R = 2^LOGR point DIF: 16-point steps, then the remainder.
+template <int LOGR, int INV, int NT, int LOG_RCUR>
+__device__ __forceinline__ void dif_substeps(uint64_t *sm, uint32_t tile, const uint64_t *__restrict__ tw_small)
+{
+    if constexpr (LOG_RCUR >= 4) dif_substep<4, INV, NT, LOG_RCUR>(sm, tile, tw_small);
+    else dif_substep<LOG_RCUR, INV, NT, LOG_RCUR>(sm, tile, tw_small);
+    __syncthreads();
+    if constexpr (LOG_RCUR > 4) dif_substeps<LOGR, INV, NT, LOG_RCUR - 4>(sm, tile, tw_small);
 }
 
 // One pass: LOGR stages on groups of R = 2^LOGR elements; at most TILE
@@ -231,16 +243,7 @@ __global__ void __launch_bounds__(NT, 2) ntt_pass_kernel(NttPassArgs a)
     __syncthreads();
 
     // ---- R-point DIF in sub-steps of up to 16 points
-    constexpr int NSTEP = (LOGR + 3) / 4;
-#pragma unroll
-    for (int st = 0; st < NSTEP; st++) {
-        const uint32_t log_rcur = LOGR - 4 * st;
-        if (log_rcur >= 4) dif_substep<4, INV, NT>(sm, tile, log_rcur, a.tw_small);
-        else if (log_rcur == 3) dif_substep<3, INV, NT>(sm, tile, 3, a.tw_small);
-        else if (log_rcur == 2) dif_substep<2, INV, NT>(sm, tile, 2, a.tw_small);
-        else dif_substep<1, INV, NT>(sm, tile, 1, a.tw_small);
-        __syncthreads();
-    }
+    dif_substeps<LOGR, INV, NT, LOGR>(sm, tile, a.tw_small);
 
     // ---- pass twiddle + store
     for (uint32_t e = threadIdx.x; e < tile; e += NT) {
