@@ -17,6 +17,7 @@ namespace zk {
 static constexpr int LEAF_T = 256;     // leaves (threads) per CTA of the leaf kernel
 static constexpr int FOLD_T = 256;     // leaf digests per CTA of the fold kernel
 static constexpr int TAIL_MAXM = 1024; // nodes a tail CTA can take
+static constexpr uint64_t WIDE_LEVEL_NODES = 1ULL << 15;  // levels at least this wide run node-parallel
 
 bool merkle_geometry_ok(uint64_t n_digests, uint64_t n_caps, uint64_t n_leaves, uint64_t cap_height, std::string &err)
 {
@@ -30,13 +31,26 @@ static void merkle_launch(uint64_t *digests, uint64_t *caps, const uint64_t *lea
     merkle_leaf_kernel<H, LEAF_T><<<(unsigned)blocks, LEAF_T, 0, s>>>(leaves, digests, caps, g);
     note_launch();
     if (g.sub_leaves == 1) return;  // caps == leaves
-    blocks = (g.n_leaves + FOLD_T - 1) / FOLD_T;
-    merkle_fold_kernel<H, FOLD_T><<<(unsigned)blocks, FOLD_T, 0, s>>>(digests, caps, g);
-    note_launch();
-    if (g.sub_leaves <= (uint64_t)FOLD_T) return;  // caps written by the fold kernel
-    // heights folded by the fold kernel
+    // Wide levels: one node per thread while a level still fills the GPU.
     uint32_t u0 = 0;
-    while ((1u << (u0 + 1)) <= (uint32_t)FOLD_T && u0 + 1 <= g.log_sub - 1) u0++;
+    const uint32_t top = g.log_sub - 1;
+    while (u0 + 1 <= top && (g.n_leaves >> (u0 + 1)) >= WIDE_LEVEL_NODES) {
+        u0++;
+        const uint64_t total = g.n_leaves >> u0;
+        merkle_level_kernel<H><<<(unsigned)((total + 255) / 256), 256, 0, s>>>(digests, g, u0);
+        note_launch();
+    }
+    // Narrow levels: folded inside CTAs of FOLD_T nodes.
+    const uint64_t count = g.n_leaves >> u0;
+    blocks = (count + FOLD_T - 1) / FOLD_T;
+    merkle_fold_kernel<H, FOLD_T><<<(unsigned)blocks, FOLD_T, 0, s>>>(digests, caps, g, u0);
+    note_launch();
+    const uint64_t sub_nodes = g.sub_leaves >> u0;
+    if (sub_nodes <= (uint64_t)FOLD_T) return;  // caps written by the fold kernel
+    // heights folded by the fold kernel
+    uint32_t U = 0;
+    while ((1u << (U + 1)) <= (uint32_t)FOLD_T && u0 + U + 1 <= top) U++;
+    u0 += U;
     while ((g.sub_leaves >> u0) > (uint64_t)TAIL_MAXM) {
         u0++;
         uint64_t total = (g.sub_leaves >> u0) * g.n_caps;

@@ -67,34 +67,36 @@ __global__ void __launch_bounds__(T) merkle_leaf_kernel(const uint64_t *__restri
     for (int q = 0; q < 4; q++) dst[q] = d[q];
 }
 
-// Folds the stored leaf digests upwards: each CTA takes T consecutive leaves'
-// digests and computes every node whose leaves all lie in it (log2 T levels,
-// or up to the subtree's two top nodes), writing each node; when whole
-// subtrees fit in the CTA it also writes their caps.
+// Folds stored digests upwards from height u0 (0 = leaf digests): each CTA
+// takes T consecutive nodes of that height and computes every node above them
+// whose subtree lies in the CTA (up to log2 T levels, or up to the subtree's
+// two top nodes), writing each node; when whole subtrees fit in the CTA it
+// also writes their caps.
 template <int H, int T>
 __global__ void __launch_bounds__(T) merkle_fold_kernel(uint64_t *__restrict__ digests, uint64_t *__restrict__ caps,
-                                                        MerkleGeom g)
+                                                        MerkleGeom g, uint32_t u0)
 {
     __shared__ uint64_t node[T][4];
-    const uint64_t i0 = (uint64_t)blockIdx.x * T;
+    const uint64_t count = g.n_leaves >> u0;     // nodes at height u0
+    const uint64_t i0 = (uint64_t)blockIdx.x * T;  // first node of this CTA (height u0)
     const uint32_t t = threadIdx.x;
-    const uint64_t cta_leaves = g.n_leaves - i0 < (uint64_t)T ? g.n_leaves - i0 : (uint64_t)T;
-    if (t < cta_leaves) {
-        const uint64_t di = merkle_node_index(g, i0 + t, 0);
+    const uint64_t cta_nodes = count - i0 < (uint64_t)T ? count - i0 : (uint64_t)T;
+    if (t < cta_nodes) {
+        const uint64_t di = merkle_node_index(g, (i0 + t) << u0, u0);
 #pragma unroll
         for (int q = 0; q < 4; q++) node[t][q] = digests[4 * di + q];
     }
     const uint32_t top = g.log_sub - 1;  // highest stored height
     uint32_t U = 0;
-    while ((1u << (U + 1)) <= T && U + 1 <= top) U++;
-    for (uint32_t u = 1; u <= U; u++) {
+    while ((1u << (U + 1)) <= T && u0 + U + 1 <= top) U++;
+    for (uint32_t v = 1; v <= U; v++) {
         __syncthreads();
-        const uint32_t nodes = T >> u;
+        const uint32_t nodes = T >> v;
         uint64_t h[4];
-        const bool act = t < nodes && ((uint64_t)t << u) < cta_leaves;
+        const bool act = t < nodes && ((uint64_t)t << v) < cta_nodes;
         if (act) {
             hash_two<H>(node[2 * t], node[2 * t + 1], h);
-            const uint64_t di = merkle_node_index(g, i0 + ((uint64_t)t << u), u);
+            const uint64_t di = merkle_node_index(g, (i0 + ((uint64_t)t << v)) << u0, u0 + v);
 #pragma unroll
             for (int q = 0; q < 4; q++) digests[4 * di + q] = h[q];
         }
@@ -104,13 +106,14 @@ __global__ void __launch_bounds__(T) merkle_fold_kernel(uint64_t *__restrict__ d
             for (int q = 0; q < 4; q++) node[t][q] = h[q];
         }
     }
-    if (U == top && g.sub_leaves <= (uint64_t)T) {
+    const uint64_t sub_nodes = g.sub_leaves >> u0;  // height-u0 nodes per subtree
+    if (u0 + U == top && sub_nodes <= (uint64_t)T) {
         __syncthreads();
-        const uint32_t subs = (uint32_t)((cta_leaves + g.sub_leaves - 1) >> g.log_sub);
+        const uint32_t subs = (uint32_t)(cta_nodes / sub_nodes);
         if (t < subs) {
             uint64_t h[4];
             hash_two<H>(node[2 * t], node[2 * t + 1], h);
-            const uint64_t k = (i0 >> g.log_sub) + t;
+            const uint64_t k = ((i0 << u0) >> g.log_sub) + t;
 #pragma unroll
             for (int q = 0; q < 4; q++) caps[4 * k + q] = h[q];
         }
