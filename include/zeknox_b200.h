@@ -125,6 +125,20 @@ RustError zeknox_server_stats(void *server, uint64_t *in_use_bytes, uint64_t *pe
 /* Waits for all admitted work, frees everything. */
 RustError zeknox_server_destroy(void *server);
 
+/* ---- Tuning (written by zeknox_b200/autotune.py; no reference counterpart)
+ * Knobs, each optionally per log2 size (lg = 0xFFFFFFFF: any size):
+ *   "leaf_threads.<hash_type>"  Merkle leaf kernel CTA size, 64/128/256 (lg = log2 leaves)
+ *   "lde_chunk_mib"             fused-LDE column chunk budget in MiB (lg = log2 N)
+ *   "lde_last_logr"             radix exponent of the fused LDE's row-output pass, 1..9 (lg = log2 n)
+ *   "wide_level_nodes.<hash_type>"  Merkle levels at least this wide run node-parallel (lg = log2 leaves)
+ * Unset knobs keep the built-in defaults.  Results never depend on the knobs. */
+RustError zeknox_tune_set(const char *name, uint32_t lg, uint64_t value);
+RustError zeknox_tune_clear(void);
+/* Value a knob has for log2 size lg (the size-free entry, else dflt). */
+uint64_t zeknox_tune_get(const char *name, uint32_t lg, uint64_t dflt);
+/* Load a table: one knob per line, "<name> <lg or *> <value>". */
+RustError zeknox_tune_load(const char *path);
+
 /* Number of kernels this library has launched so far in the process. */
 uint64_t zeknox_launch_count(void);
 

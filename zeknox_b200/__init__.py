@@ -34,7 +34,12 @@ ABI_SYMBOLS = [
 EXT_SYMBOLS = ["zeknox_last_error", "zeknox_commit", "zeknox_commit_batch", "zeknox_commit_scratch_words",
                "zeknox_lde_rows", "zeknox_launch_count", "zeknox_measure_mul_rate", "zeknox_merkle_batch",
                "zeknox_lde_rows_noalloc", "zeknox_server_create", "zeknox_server_submit", "zeknox_server_wait",
-               "zeknox_server_release", "zeknox_server_stats", "zeknox_server_destroy"]
+               "zeknox_server_release", "zeknox_server_stats", "zeknox_server_destroy", "zeknox_tune_set",
+               "zeknox_tune_get", "zeknox_tune_clear", "zeknox_tune_load"]
+
+# Tuning table measured on B200 by ``python -m zeknox_b200.autotune``; loaded
+# by load() unless ZEKNOX_TUNE_FILE names another table ("" or "none": no table).
+TUNE_TABLE = os.path.join(HERE, "tuning_b200.txt")
 
 
 class RustError(ctypes.Structure):
@@ -185,7 +190,18 @@ def load():
     L.zeknox_server_destroy.argtypes = [vp]
     L.zeknox_merkle_batch.restype = RustError
     L.zeknox_merkle_batch.argtypes = [sz, ctypes.POINTER(MerkleJob), u32]
+    L.zeknox_tune_set.restype = RustError
+    L.zeknox_tune_set.argtypes = [ctypes.c_char_p, u32, u64]
+    L.zeknox_tune_get.restype = u64
+    L.zeknox_tune_get.argtypes = [ctypes.c_char_p, u32, u64]
+    L.zeknox_tune_clear.restype = RustError
+    L.zeknox_tune_clear.argtypes = []
+    L.zeknox_tune_load.restype = RustError
+    L.zeknox_tune_load.argtypes = [ctypes.c_char_p]
     _lib = L
+    table = os.environ.get("ZEKNOX_TUNE_FILE", TUNE_TABLE)
+    if table and table != "none" and os.path.exists(table):
+        _check(L.zeknox_tune_load(table.encode()))
     return L
 
 
@@ -384,6 +400,33 @@ def launch_count():
 
 def measure_mul_rate(device_id=0):
     return load().zeknox_measure_mul_rate(device_id)
+
+
+# ------------------------------------------------------------------ tuning
+
+TUNE_ANY = 0xFFFFFFFF
+
+
+def tune_set(name, value, lg=None):
+    """Set a knob ("leaf_threads.<hash>", "lde_chunk_mib", "lde_last_logr",
+    "wide_level_nodes.<hash>"), for log2 size `lg` or for every size (lg None)."""
+    _check(load().zeknox_tune_set(name.encode(), TUNE_ANY if lg is None else lg, value))
+
+
+def tune_get(name, lg=None, default=0):
+    """Value of a knob for log2 size `lg` (falls back to the size-free entry,
+    then to `default`)."""
+    return load().zeknox_tune_get(name.encode(), TUNE_ANY if lg is None else lg, default)
+
+
+def tune_clear():
+    """Forget every knob (built-in defaults again)."""
+    _check(load().zeknox_tune_clear())
+
+
+def tune_load(path):
+    """Load a table of "<name> <lg|*> <value>" lines."""
+    _check(load().zeknox_tune_load(os.fspath(path).encode()))
 
 
 def merkle_job(leaves, digests, caps, n_leaves, leaf_size, cap_height, hash_type):

@@ -1,0 +1,204 @@
+"""Autotuner: times the library's launch-shape knobs on the GPU and writes the
+tuning table that ``zeknox_b200.load()`` reads.
+
+    python -m zeknox_b200.autotune [--device 0] [--out zeknox_b200/tuning_b200.txt] [--quick]
+
+Knobs (all shape choices only; results are bit-identical for every value, and
+the tuner checks that for each candidate against the default's output):
+
+* ``lde_last_logr`` (per log2 n): radix exponent 7..9 of the fused LDE's last
+  pass, the one that writes bit-reversed leaf rows;
+* ``lde_chunk_mib`` (per log2 N = log2 n + rate_bits): column-chunk budget of
+  the fused LDE, i.e. how much of the inter-pass intermediate is meant to stay
+  in the 126 MB L2 between the two passes;
+* ``leaf_threads.<hash>`` (per log2 leaves): CTA size of the Merkle leaf kernel
+  (one thread per leaf, a CTA of 64 / 128 / 256 leaves);
+* ``wide_level_nodes.<hash>`` (per log2 leaves): Merkle levels with at least this
+  many nodes run one launch per level (one thread per node) before the
+  in-CTA fold takes over.
+
+Each candidate is timed with CUDA events on the launching stream, median of
+several repetitions after warm-up, with the L2 flushed (a 256 MiB write)
+before every repetition.  Knobs are searched one at a time (coordinate
+descent) in the order above; a value replaces the built-in default only when
+it is faster by more than ``--margin`` (default 2 %).  The table lists every
+measured shape with its times as comments.
+
+The reference library has no tuner (its launch shapes are fixed constants in
+native/ntt/kernels.cu and native/merkle/merkle.cu); this is the B200 side's
+own.
+"""
+import argparse
+import os
+import statistics
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.dirname(HERE))
+
+DEFAULTS = {"lde_last_logr": 9, "lde_chunk_mib": 64, "leaf_threads": 256, "wide_level_nodes": 1 << 15}
+CANDIDATES = {
+    "lde_last_logr": [9, 8, 7],
+    "lde_chunk_mib": [64, 16, 32, 96],
+    "leaf_threads": [256, 128, 64],
+    "wide_level_nodes": [1 << 15, 1 << 13, 1 << 17, 1 << 40],
+}
+HASH_NAMES = {0: "poseidon", 1: "keccak", 3: "poseidon2", 4: "monolith"}
+RATE = 3
+
+
+def lde_shapes(quick):
+    """(lg_n, cols) of the fused-LDE shapes: rows at most 2^27 words (1 GiB)."""
+    lgs = [15, 16] if quick else [12, 13, 14, 15, 16, 17, 18, 19, 20]
+    return [(lg, min(256, 1 << (27 - lg - RATE))) for lg in lgs]
+
+
+def merkle_shapes(quick):
+    """(hash, lg leaves, leaf size): the commit's Poseidon2 forest and the
+    alternative-hash forests of 2^20 leaves x 135."""
+    out = [(3, 18, 256)]
+    if not quick:
+        out += [(3, 20, 135), (0, 20, 135), (4, 20, 135), (1, 20, 135), (0, 13, 84), (3, 16, 256)]
+    return out
+
+
+class Timer:
+    """CUDA-event timing on one stream, L2 flushed before every repetition."""
+
+    def __init__(self, torch, stream, warmup, reps):
+        self.torch, self.stream, self.warmup, self.reps = torch, stream, warmup, reps
+        self.flush = torch.empty(32 << 20, dtype=torch.int64, device="cuda")  # 256 MiB > L2
+
+    def __call__(self, fn):
+        t = self.torch
+        with t.cuda.stream(self.stream):
+            for _ in range(self.warmup):
+                fn()
+            times = []
+            for _ in range(self.reps):
+                self.flush.fill_(len(times))
+                e0, e1 = t.cuda.Event(enable_timing=True), t.cuda.Event(enable_timing=True)
+                e0.record(self.stream)
+                fn()
+                e1.record(self.stream)
+                e1.synchronize()
+                times.append(e0.elapsed_time(e1))
+        return statistics.median(times)
+
+
+def search(zk, timer, knob, lg, candidates, default, run, check, margin, log):
+    """Time `run` under each candidate value of `knob` at log2 size `lg`;
+    `check` compares the output with the default's (raises on a mismatch).
+    Leaves the chosen value set and returns (value, {value: ms})."""
+    times = {}
+    for v in candidates:
+        zk.tune_set(knob, v, lg=lg)
+        run()
+        check(knob, v)
+        times[v] = timer(run)
+    best = min(times, key=times.get)
+    if times[best] >= times[default] * (1.0 - margin):
+        best = default  # not clearly faster: keep the built-in value
+    zk.tune_set(knob, best, lg=lg)
+    log.append((knob, lg, best, times))
+    print("  %-22s lg %2d -> %-8d %s" % (knob, lg, best, " ".join("%d=%.3f" % kv for kv in times.items())),
+          flush=True)
+    return best, times
+
+
+def tune_lde(zk, torch, timer, dev, stream, lg, cols, margin, log):
+    n, N = 1 << lg, 1 << (lg + RATE)
+    coeffs = torch.randint(0, 1 << 62, (cols * n,), dtype=torch.int64, device="cuda")
+    rows = torch.empty(cols * N, dtype=torch.int64, device="cuda")
+
+    def run():
+        zk.lde_rows(dev, rows, coeffs, lg, RATE, cols, stream=stream.cuda_stream)
+
+    run()
+    stream.synchronize()
+    ref = rows.clone()
+
+    def check(knob, v):
+        stream.synchronize()
+        if not torch.equal(rows, ref):
+            raise RuntimeError("LDE 2^%d x %d differs from the default with %s = %d" % (lg, cols, knob, v))
+
+    print("LDE lg_n %d rate %d cols %d" % (lg, RATE, cols), flush=True)
+    search(zk, timer, "lde_last_logr", lg, CANDIDATES["lde_last_logr"], DEFAULTS["lde_last_logr"], run, check,
+           margin, log)
+    search(zk, timer, "lde_chunk_mib", lg + RATE, CANDIDATES["lde_chunk_mib"], DEFAULTS["lde_chunk_mib"], run,
+           check, margin, log)
+    del coeffs, rows, ref
+
+
+def tune_merkle(zk, torch, timer, h, lg, leaf_size, margin, log):
+    n = 1 << lg
+    cap = 4
+    leaves = torch.randint(0, 1 << 62, (n * leaf_size,), dtype=torch.int64, device="cuda")
+    n_dig, n_cap = zk.merkle_sizes(n, cap)
+    dig = torch.empty(max(n_dig, 1) * 4, dtype=torch.int64, device="cuda")
+    caps = torch.empty(n_cap * 4, dtype=torch.int64, device="cuda")
+
+    def run():
+        zk.fill_digests_buf_linear_gpu(dig, caps, leaves, n, leaf_size, cap, h)
+
+    run()
+    torch.cuda.synchronize()
+    ref_d, ref_c = dig.clone(), caps.clone()
+
+    def check(knob, v):
+        torch.cuda.synchronize()
+        if not (torch.equal(dig, ref_d) and torch.equal(caps, ref_c)):
+            raise RuntimeError("%s forest 2^%d x %d differs with %s = %d" % (HASH_NAMES[h], lg, leaf_size, knob, v))
+
+    print("Merkle %s 2^%d leaves x %d" % (HASH_NAMES[h], lg, leaf_size), flush=True)
+    search(zk, timer, "leaf_threads.%d" % h, lg, CANDIDATES["leaf_threads"], DEFAULTS["leaf_threads"], run, check,
+           margin, log)
+    search(zk, timer, "wide_level_nodes.%d" % h, lg, CANDIDATES["wide_level_nodes"], DEFAULTS["wide_level_nodes"],
+           run, check, margin, log)
+    del leaves, dig, caps, ref_d, ref_c
+
+
+def write_table(path, log, device_name):
+    lines = ["# zeknox_b200 tuning table: <knob> <log2 size | *> <value>",
+             "# measured on %s by python -m zeknox_b200.autotune (CUDA events, median, L2 flushed)" % device_name,
+             "# comment after each line: milliseconds per call for every candidate"]
+    for knob, lg, best, times in log:
+        lines.append("%-22s %2d %-14d # %s" % (knob, lg, best, " ".join("%d=%.3f" % kv for kv in times.items())))
+    with open(path, "w") as f:
+        f.write("\n".join(lines) + "\n")
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser(description=__doc__.split("\n\n")[0])
+    ap.add_argument("--device", type=int, default=0)
+    ap.add_argument("--out", default=os.path.join(HERE, "tuning_b200.txt"))
+    ap.add_argument("--quick", action="store_true", help="the headline shapes only")
+    ap.add_argument("--warmup", type=int, default=2)
+    ap.add_argument("--reps", type=int, default=7)
+    ap.add_argument("--margin", type=float, default=0.02)
+    args = ap.parse_args(argv)
+    os.environ["ZEKNOX_TUNE_FILE"] = "none"  # start from the built-in defaults
+    import torch
+    import zeknox_b200 as zk
+    if not torch.cuda.is_available():
+        raise SystemExit("autotune needs a GPU")
+    torch.cuda.set_device(args.device)
+    zk.load()
+    zk.tune_clear()
+    stream = torch.cuda.Stream()
+    timer = Timer(torch, stream, args.warmup, args.reps)
+    log = []
+    for lg, cols in lde_shapes(args.quick):
+        tune_lde(zk, torch, timer, args.device, stream, lg, cols, args.margin, log)
+        torch.cuda.empty_cache()
+    for h, lg, leaf_size in merkle_shapes(args.quick):
+        tune_merkle(zk, torch, timer, h, lg, leaf_size, args.margin, log)
+        torch.cuda.empty_cache()
+    write_table(args.out, log, torch.cuda.get_device_name(args.device))
+    changed = sum(1 for knob, _, best, _ in log if best != DEFAULTS[knob.split(".")[0]])
+    print("wrote %s: %d entries, %d differ from the built-in defaults" % (args.out, len(log), changed))
+
+
+if __name__ == "__main__":
+    main()

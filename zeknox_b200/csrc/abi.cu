@@ -444,6 +444,40 @@ extern "C" RustError zeknox_merkle_batch(size_t device_id, const zk_merkle_job *
     });
 }
 
+// ------------------------------------------------------------------ tuning
+
+extern "C" RustError zeknox_tune_set(const char *name, uint32_t lg, uint64_t value)
+{
+    return guarded([&] {
+        if (!name) throw zk::arg_failure("null knob name");
+        zk::tune_set(name, lg, value);
+    });
+}
+
+extern "C" uint64_t zeknox_tune_get(const char *name, uint32_t lg, uint64_t dflt)
+{
+    if (!name) return dflt;
+    try {
+        return zk::tune_get(name, lg, dflt);
+    } catch (...) {
+        return dflt;
+    }
+}
+
+extern "C" RustError zeknox_tune_clear(void)
+{
+    return guarded([&] { zk::tune_clear(); });
+}
+
+// Table file: one knob per line, "<name> <lg or *> <value>"; '#' starts a comment.
+extern "C" RustError zeknox_tune_load(const char *path)
+{
+    return guarded([&] {
+        if (!path) throw zk::arg_failure("null path");
+        zk::tune_load_file(path);
+    });
+}
+
 // ------------------------------------------------------------- diagnostics
 
 extern "C" uint64_t zeknox_launch_count(void) { return zk::launch_count(); }

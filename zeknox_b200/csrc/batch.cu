@@ -130,7 +130,9 @@ DevBatchState &state_for(DeviceCtx &c)
 std::vector<uint64_t> batch_key(const zk_commit_job *jobs, uint32_t njobs)
 {
     std::vector<uint64_t> k;
-    k.reserve(njobs * 11);
+    k.reserve(njobs * 7 + 2);
+    k.push_back(0xC0FFULL);  // distinct from Merkle batch keys
+    k.push_back(tune_generation());
     for (uint32_t i = 0; i < njobs; i++) {
         const zk_commit_job &j = jobs[i];
         k.push_back(((uint64_t)j.lg_n << 48) | ((uint64_t)j.rate_bits << 40) | ((uint64_t)j.cap_height << 32) | j.cols);
@@ -236,6 +238,7 @@ void merkle_batch_graph(DeviceCtx &c, const zk_merkle_job *jobs, uint32_t njobs)
     std::vector<uint64_t> words(njobs, 0);
     std::vector<uint64_t> key;
     key.push_back(0xFEEDULL);  // distinct from commit keys
+    key.push_back(tune_generation());
     for (uint32_t i = 0; i < njobs; i++) {
         const zk_merkle_job &j = jobs[i];
         std::string err;

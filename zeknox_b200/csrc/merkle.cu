@@ -14,10 +14,11 @@
 
 namespace zk {
 
-static constexpr int LEAF_T = 256;     // leaves (threads) per CTA of the leaf kernel
+static constexpr int LEAF_T = 256;     // default leaves (threads) per CTA of the leaf kernel ("leaf_threads.<hash>")
 static constexpr int FOLD_T = 256;     // leaf digests per CTA of the fold kernel
 static constexpr int TAIL_MAXM = 1024; // nodes a tail CTA can take
-static constexpr uint64_t WIDE_LEVEL_NODES = 1ULL << 15;  // levels at least this wide run node-parallel
+static constexpr uint64_t WIDE_LEVEL_NODES = 1ULL << 15;  // default: levels at least this wide run node-parallel
+                                                          // ("wide_level_nodes.<hash>")
 
 bool merkle_geometry_ok(uint64_t n_digests, uint64_t n_caps, uint64_t n_leaves, uint64_t cap_height, std::string &err)
 {
@@ -27,14 +28,26 @@ bool merkle_geometry_ok(uint64_t n_digests, uint64_t n_caps, uint64_t n_leaves, 
 template <int H>
 static void merkle_launch(uint64_t *digests, uint64_t *caps, const uint64_t *leaves, const MerkleGeom &g, cudaStream_t s)
 {
-    uint64_t blocks = (g.n_leaves + LEAF_T - 1) / LEAF_T;
-    merkle_leaf_kernel<H, LEAF_T><<<(unsigned)blocks, LEAF_T, 0, s>>>(leaves, digests, caps, g);
+    const uint32_t lg_leaves = ilog2_exact(g.n_leaves);
+    const uint64_t lt = tune_get("leaf_threads." + std::to_string(H), lg_leaves, LEAF_T);
+    uint64_t blocks;
+    if (lt == 64) {
+        blocks = (g.n_leaves + 63) / 64;
+        merkle_leaf_kernel<H, 64><<<(unsigned)blocks, 64, 0, s>>>(leaves, digests, caps, g);
+    } else if (lt == 128) {
+        blocks = (g.n_leaves + 127) / 128;
+        merkle_leaf_kernel<H, 128><<<(unsigned)blocks, 128, 0, s>>>(leaves, digests, caps, g);
+    } else {
+        blocks = (g.n_leaves + LEAF_T - 1) / LEAF_T;
+        merkle_leaf_kernel<H, LEAF_T><<<(unsigned)blocks, LEAF_T, 0, s>>>(leaves, digests, caps, g);
+    }
     note_launch();
+    const uint64_t wide = tune_get("wide_level_nodes." + std::to_string(H), lg_leaves, WIDE_LEVEL_NODES);
     if (g.sub_leaves == 1) return;  // caps == leaves
     // Wide levels: one node per thread while a level still fills the GPU.
     uint32_t u0 = 0;
     const uint32_t top = g.log_sub - 1;
-    while (u0 + 1 <= top && (g.n_leaves >> (u0 + 1)) >= WIDE_LEVEL_NODES) {
+    while (u0 + 1 <= top && (g.n_leaves >> (u0 + 1)) >= wide) {
         u0++;
         const uint64_t total = g.n_leaves >> u0;
         merkle_level_kernel<H><<<(unsigned)((total + 255) / 256), 256, 0, s>>>(digests, g, u0);

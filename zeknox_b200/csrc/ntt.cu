@@ -59,17 +59,20 @@ struct Pass {
 static std::vector<Pass> plan_passes(uint32_t L, bool rows)
 {
     std::vector<uint32_t> sizes;
-    const uint32_t last_max = rows ? 9 : 12;
+    // last pass of a row-output transform: radix 2^lde_last_logr (tuned, <= 9)
+    uint32_t last_rows = (uint32_t)tune_get("lde_last_logr", L, 9);
+    last_rows = last_rows < 1 ? 1 : (last_rows > 9 ? 9 : last_rows);
+    const uint32_t last_max = rows ? last_rows : 12;
     if (L <= last_max) {
         sizes.push_back(L);
     } else if (!rows) {
         uint32_t np = (L + 11) / 12;
         for (uint32_t i = 0; i < np; i++) sizes.push_back(L / np + (i < L % np ? 1 : 0));
     } else {
-        uint32_t rem = L - 9;
+        uint32_t rem = L - last_rows;
         uint32_t np = (rem + 11) / 12;
         for (uint32_t i = 0; i < np; i++) sizes.push_back(rem / np + (i < rem % np ? 1 : 0));
-        sizes.push_back(9);
+        sizes.push_back(last_rows);
     }
     std::vector<Pass> p;
     uint32_t hi = L;
@@ -266,14 +269,14 @@ void lde_batch_device(DeviceCtx &c, uint64_t *out, const uint64_t *in, uint32_t 
 }
 
 // Columns per chunk of the fused LDE: the intermediate of a chunk (2^(lg_n +
-// rate) words per column) is kept within ZK_L2_CHUNK_BYTES so the second pass
+// rate) words per column) is kept within lde_chunk_mib MiB so the second pass
 // reads it back from L2 instead of HBM.  A multiple of the 16-column row tile.
-static constexpr uint64_t ZK_L2_CHUNK_BYTES = 64ULL << 20;
+static constexpr uint64_t ZK_L2_CHUNK_MIB = 64;  // default; the autotuner may set "lde_chunk_mib"
 
 uint32_t lde_rows_chunk_cols(uint32_t lg_n, uint32_t rate, uint64_t cols)
 {
     const uint64_t per_col = 8ULL << (lg_n + rate);
-    uint64_t c = ZK_L2_CHUNK_BYTES / per_col;
+    uint64_t c = (tune_get("lde_chunk_mib", lg_n + rate, ZK_L2_CHUNK_MIB) << 20) / per_col;
     c = c < 16 ? 16 : (c / 16) * 16;
     return (uint32_t)(c < cols ? c : ((cols + 15) / 16) * 16);
 }

@@ -1,6 +1,7 @@
 // runtime.cu -- device registry, tables and temporaries.
 #include <cstdio>
 #include <cstdlib>
+#include <cstring>
 #include <atomic>
 #include <memory>
 
@@ -34,6 +35,80 @@ uint32_t ilog2_exact(uint64_t x)
 static std::atomic<uint64_t> g_launches{0};
 void note_launch(uint64_t n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
 uint64_t launch_count() { return g_launches.load(std::memory_order_relaxed); }
+
+static std::mutex g_tune_mu;
+static std::map<std::pair<std::string, uint32_t>, uint64_t> g_tune;
+static std::atomic<uint64_t> g_tune_gen{0};
+
+uint64_t tune_generation() { return g_tune_gen.load(std::memory_order_relaxed); }
+
+// A table named by ZEKNOX_TUNE_FILE ("none": no table) is read at the first
+// knob lookup, so consumers of the C ABI get tuned knobs without calling
+// zeknox_tune_load.
+static std::once_flag g_tune_env_once;
+static void tune_env_load()
+{
+    const char *path = getenv("ZEKNOX_TUNE_FILE");
+    if (!path || !*path || strcmp(path, "none") == 0) return;
+    try {
+        tune_load_file(path);
+    } catch (const std::exception &e) {
+        fprintf(stderr, "zeknox: ZEKNOX_TUNE_FILE ignored: %s\n", e.what());
+    }
+}
+
+uint64_t tune_get(const std::string &name, uint32_t lg, uint64_t dflt)
+{
+    std::call_once(g_tune_env_once, tune_env_load);
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    auto it = g_tune.find({name, lg});
+    if (it != g_tune.end()) return it->second;
+    it = g_tune.find({name, TUNE_ANY});
+    return it != g_tune.end() ? it->second : dflt;
+}
+
+void tune_set(const std::string &name, uint32_t lg, uint64_t value)
+{
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    g_tune[{name, lg}] = value;
+    g_tune_gen.fetch_add(1, std::memory_order_relaxed);
+}
+
+void tune_clear()
+{
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    g_tune.clear();
+    g_tune_gen.fetch_add(1, std::memory_order_relaxed);
+}
+
+void tune_load_file(const char *path)
+{
+    FILE *f = fopen(path, "r");
+    if (!f) throw arg_failure(std::string("cannot open tuning table ") + path);
+    std::vector<std::tuple<std::string, uint32_t, uint64_t>> entries;
+    char line[256];
+    int ln = 0;
+    while (fgets(line, sizeof line, f)) {
+        ln++;
+        char *hash = strchr(line, '#');
+        if (hash) *hash = 0;
+        char name[128], lgs[32], extra[8];
+        unsigned long long value;
+        const int got = sscanf(line, "%127s %31s %llu %7s", name, lgs, &value, extra);
+        if (got == EOF || got == 0) continue;  // blank or comment-only line
+        char *end = nullptr;
+        const unsigned long lg = strtoul(lgs, &end, 10);
+        const bool any = strcmp(lgs, "*") == 0;
+        if (got != 3 || (!any && (*end || lg > 64))) {
+            fclose(f);
+            throw arg_failure(std::string(path) + ":" + std::to_string(ln) + ": expected '<name> <lg|*> <value>'");
+        }
+        entries.emplace_back(name, any ? TUNE_ANY : (uint32_t)lg, (uint64_t)value);
+    }
+    fclose(f);
+    // all or nothing: a malformed table changes no knob
+    for (auto &e : entries) tune_set(std::get<0>(e), std::get<1>(e), std::get<2>(e));
+}
 
 static std::mutex g_reg_mu;
 static std::vector<std::unique_ptr<DeviceCtx>> g_devs;

@@ -87,6 +87,21 @@ struct DevBuf {
 
 uint32_t ilog2_exact(uint64_t x);  // -1u if x is not a power of two
 
+// Tuning table: named knobs, optionally per log2 size, set by the autotuner
+// (zeknox_tune_set / zeknox_tune_load); tune_get falls back to the size-free
+// entry and then to `dflt`.  Knobs: "leaf_threads.<hash>" (64/128/256),
+// "lde_chunk_mib", "lde_last_logr" (1..9), "wide_level_nodes.<hash>".
+uint64_t tune_get(const std::string &name, uint32_t lg, uint64_t dflt);
+void tune_set(const std::string &name, uint32_t lg, uint64_t value);
+void tune_clear();
+// Reads "<name> <lg|*> <value>" lines ('#' comments); throws arg_failure on a
+// malformed line, in which case no knob is changed.
+void tune_load_file(const char *path);
+// Bumped by every tune_set / tune_clear: cached CUDA graphs record it in their
+// key, so a graph captured under other knob values is not replayed.
+uint64_t tune_generation();
+constexpr uint32_t TUNE_ANY = 0xFFFFFFFFu;
+
 // Count of kernels this library has launched (diagnostics: zeknox_launch_count).
 void note_launch(uint64_t n = 1);
 uint64_t launch_count();
