@@ -69,6 +69,14 @@ class Timer:
         self.torch, self.stream, self.warmup, self.reps = torch, stream, warmup, reps
         self.flush = torch.empty(32 << 20, dtype=torch.int64, device="cuda")  # 256 MiB > L2
 
+    def on(self, stream):
+        """The same timer on another stream (the Merkle calls run on the
+        legacy default stream, which torch's own streams do not wait for)."""
+        other = Timer.__new__(Timer)
+        other.__dict__.update(self.__dict__)
+        other.stream = stream
+        return other
+
     def __call__(self, fn):
         t = self.torch
         with t.cuda.stream(self.stream):
@@ -193,7 +201,7 @@ def main(argv=None):
         tune_lde(zk, torch, timer, args.device, stream, lg, cols, args.margin, log)
         torch.cuda.empty_cache()
     for h, lg, leaf_size in merkle_shapes(args.quick):
-        tune_merkle(zk, torch, timer, h, lg, leaf_size, args.margin, log)
+        tune_merkle(zk, torch, timer.on(torch.cuda.default_stream()), h, lg, leaf_size, args.margin, log)
         torch.cuda.empty_cache()
     write_table(args.out, log, torch.cuda.get_device_name(args.device))
     changed = sum(1 for knob, _, best, _ in log if best != DEFAULTS[knob.split(".")[0]])
