@@ -13,6 +13,10 @@ way they are produced are this project's own:
 * Keccak-f[1600] round constants, rotation offsets and the pi lane walk are
   *derived* from the Keccak specification (LFSR rc(t), offsets (t+1)(t+2)/2) and
   cross-checked against native/keccak/keccak.cu:16-37.
+* Poseidon's sparse partial-round tables (first-round constants, per-round
+  scalars, the dense initial matrix and the per-round row/column vectors) are
+  *derived* from the MDS matrix and round constants (derive_poseidon_fast) and
+  cross-checked against native/poseidon/poseidon.hpp:38-801.
 * Poseidon round constants (native/poseidon/poseidon.hpp:803-1164, 360 values,
   MDS circulant row and diagonal :35-36), Poseidon2 round constants and internal
   diagonal (native/poseidon2/poseidon2.cu:8-59) and Monolith round constants and
@@ -110,6 +114,11 @@ def read_reference(ref):
     out["poseidon_rc"] = _numbers(_block(pos, r"ALL_ROUND_CONSTANTS\[[^\]]*\]\s*=\s*{"))
     out["poseidon_circ"] = _numbers(_block(pos, r"MDS_MATRIX_CIRC\[12\]\s*=\s*{"))
     out["poseidon_diag"] = _numbers(_block(pos, r"MDS_MATRIX_DIAG\[12\]\s*=\s*{"))
+    out["fast_first"] = _numbers(_block(pos, r"FAST_PARTIAL_FIRST_ROUND_CONSTANT\[12\]\s*=\s*{"))
+    out["fast_k"] = _numbers(_block(pos, r"FAST_PARTIAL_ROUND_CONSTANTS\[N_PARTIAL_ROUNDS\]\s*=\s*{"))
+    out["fast_v"] = _numbers(_block(pos, r"FAST_PARTIAL_ROUND_VS\[N_PARTIAL_ROUNDS\]\[11\]\s*=\s*{"))
+    out["fast_w"] = _numbers(_block(pos, r"FAST_PARTIAL_ROUND_W_HATS\[N_PARTIAL_ROUNDS\]\[11\]\s*=\s*{"))
+    out["fast_init"] = _numbers(_block(pos, r"FAST_PARTIAL_ROUND_INITIAL_MATRIX\[11\]\[11\]\s*=\s*{"))
     # the #ifdef'd declarations share one initializer: take the first brace after the CPU name
     diag_start = p2.index("const u64 MATRIX_DIAG_12_GOLDILOCKS[12] = {")
     out["p2_diag"] = _numbers(_block(p2[diag_start:], r"\[12\]\s*=\s*{"))
@@ -127,6 +136,109 @@ def read_reference(ref):
     out["k_rotc"] = _numbers(_block(kec, r"keccakf_rotc\)\[24\]\s*=\s*{"))
     out["k_piln"] = _numbers(_block(kec, r"keccakf_piln\)\[24\]\s*=\s*{"))
     return out
+
+
+def _mat_mul(a, b):
+    return [[sum(a[i][k] * b[k][j] for k in range(len(b))) % P for j in range(len(b[0]))] for i in range(len(a))]
+
+
+def _mat_vec(a, v):
+    return [sum(a[i][k] * v[k] for k in range(len(v))) % P for i in range(len(a))]
+
+
+def _mat_inv(a):
+    n = len(a)
+    m = [list(row) + [int(i == j) for j in range(n)] for i, row in enumerate(a)]
+    for c in range(n):
+        piv = next(r for r in range(c, n) if m[r][c])
+        m[c], m[piv] = m[piv], m[c]
+        inv = pow(m[c][c], P - 2, P)
+        m[c] = [x * inv % P for x in m[c]]
+        for r in range(n):
+            if r != c and m[r][c]:
+                f = m[r][c]
+                m[r] = [(x - f * y) % P for x, y in zip(m[r], m[c])]
+    return [row[n:] for row in m]
+
+
+def poseidon_mds_matrix(circ, diag):
+    return [[(circ[(j - r) % 12] + (diag[r] if r == j else 0)) % P for j in range(12)] for r in range(12)]
+
+
+def derive_poseidon_fast(rc, circ, diag, n_full_half=4, n_partial=22):
+    """Partial rounds of Poseidon in the sparse-matrix form of the Poseidon
+    paper (Grassi et al., eprint 2019/458, appendix B), derived here from the
+    MDS matrix and round constants.
+
+    The 22 partial rounds  x <- M * S0(x + c_r)  (S0: S-box on lane 0 only)
+    equal, exactly:
+        x <- x + first                       (12 constants)
+        x[1..11] <- init * x[1..11]          (11 x 11)
+        for r in 0..21:
+            x[0] <- S(x[0]) + k[r]            (k[21] = 0)
+            x[0], x[i] <- m00 * x[0] + sum_i w[r][i] * x[i],  x[i] + v[r][i] * x[0]
+    Derivation: constants are carried backwards through each M (M^-1 c), lane
+    0 of the carry stays in its round as k, lanes 1..11 pass through S0; each
+    M is factored M = B * D with D = diag(1, N^) acting on lanes 1..11 only
+    (commutes with S0 and with k) and B sparse (first row [m00, N^-T w],
+    first column v), D merged into the previous round's matrix."""
+    M = poseidon_mds_matrix(circ, diag)
+    Minv = _mat_inv(M)
+    m00 = M[0][0]
+    w = M[0][1:]
+    v = [M[i][0] for i in range(1, 12)]
+    Mh = [row[1:] for row in M[1:]]
+    # constants
+    base = 12 * n_full_half
+    cr = [rc[base + 12 * r: base + 12 * r + 12] for r in range(n_partial)]
+    k = [0] * n_partial
+    carry = [0] * 12
+    for r in range(n_partial - 1, 0, -1):
+        d = [(a + b) % P for a, b in zip(cr[r], carry)]
+        u = _mat_vec(Minv, d)
+        k[r - 1] = u[0]
+        carry = [0] + u[1:]
+    first = [(a + b) % P for a, b in zip(cr[0], carry)]
+    # matrices, last round first: N^_r = Mh^(R - r), v_r = Mh^(R-1-r) v, w_r = N^_r^-T w
+    ws, vs = [None] * n_partial, [None] * n_partial
+    Nh = Mh
+    vr = v
+    for r in range(n_partial - 1, -1, -1):
+        NhT_inv = _mat_inv([list(col) for col in zip(*Nh)])
+        ws[r] = _mat_vec(NhT_inv, w)
+        vs[r] = vr
+        if r:
+            vr = _mat_vec(Nh, v)
+            Nh = _mat_mul(Nh, Mh)
+    init = Nh
+
+    def sbox(x):
+        return pow(x, 7, P)
+
+    def naive(x):
+        for r in range(n_partial):
+            x = [(a + b) % P for a, b in zip(x, cr[r])]
+            x[0] = sbox(x[0])
+            x = _mat_vec(M, x)
+        return x
+
+    def fast(x):
+        x = [(a + b) % P for a, b in zip(x, first)]
+        x = [x[0]] + _mat_vec(init, x[1:])
+        for r in range(n_partial):
+            x[0] = (sbox(x[0]) + k[r]) % P
+            x0 = (m00 * x[0] + sum(a * b for a, b in zip(ws[r], x[1:]))) % P
+            x = [x0] + [(xi + vi * x[0]) % P for xi, vi in zip(x[1:], vs[r])]
+        return x
+
+    import random
+    rnd = random.Random(1)
+    for _ in range(8):
+        x = [rnd.randrange(P) for _ in range(12)]
+        assert naive(list(x)) == fast(list(x)), "fast partial rounds disagree with the round-by-round form"
+    assert k[-1] == 0
+    return {"m00": m00, "first": first, "init": [x for row in init for x in row], "k": k,
+            "w": [x for row in ws for x in row], "v": [x for row in vs for x in row]}
 
 
 def fmt_list(name, vals, per_line=4, hexw=16):
@@ -186,6 +298,21 @@ def main():
     hdr.append(fmt_list("ZK_POSEIDON_RC_LIST", ref["poseidon_rc"]))
     hdr.append(fmt_list("ZK_POSEIDON_CIRC_LIST", ref["poseidon_circ"], 12, 0))
     hdr.append("#define ZK_POSEIDON_DIAG0 %d\n" % ref["poseidon_diag"][0])
+    fast = derive_poseidon_fast(ref["poseidon_rc"], ref["poseidon_circ"], ref["poseidon_diag"])
+    # the derived sparse form agrees with the reference's own tables
+    # (native/poseidon/poseidon.hpp:38-801; its initial matrix is stored transposed)
+    assert ref["fast_first"] == fast["first"] and ref["fast_k"] == fast["k"], "fast partial constants mismatch"
+    assert ref["fast_v"] == fast["v"] and ref["fast_w"] == fast["w"], "fast partial v / w mismatch"
+    assert [ref["fast_init"][11 * j + i] for i in range(11) for j in range(11)] == fast["init"], "initial matrix mismatch"
+    hdr.append("/* Partial rounds in sparse form (derived by gen_constants.py, checked against\n"
+               " * the round-by-round form): x += FIRST; x[1..11] = INIT x[1..11]; per round r:\n"
+               " * x0 = S(x0) + K[r]; x0' = M00 x0 + sum W[r][i] x[i+1]; x[i+1] += V[r][i] x0. */\n")
+    hdr.append("#define ZK_POSEIDON_FAST_M00 %d\n" % fast["m00"])
+    hdr.append(fmt_list("ZK_POSEIDON_FAST_FIRST_LIST", fast["first"]))
+    hdr.append(fmt_list("ZK_POSEIDON_FAST_INIT_LIST", fast["init"]))
+    hdr.append(fmt_list("ZK_POSEIDON_FAST_K_LIST", fast["k"]))
+    hdr.append(fmt_list("ZK_POSEIDON_FAST_W_LIST", fast["w"]))
+    hdr.append(fmt_list("ZK_POSEIDON_FAST_V_LIST", fast["v"]))
     hdr.append("\n/* Poseidon2 (width 12, 4+4 external rounds, 22 internal rounds). */\n")
     hdr.append(fmt_list("ZK_POSEIDON2_RC_LIST", ref["p2_rc"]))
     hdr.append(fmt_list("ZK_POSEIDON2_DIAG_LIST", ref["p2_diag"]))

@@ -228,6 +228,63 @@ ZK_HD uint64_t gl_mul_add_nc(uint64_t a, uint64_t b, uint64_t c)
 #endif
 }
 
+// Sum of fewer than 2^32 - 1 full 128-bit products, reduced once: value =
+// limbs + 2^128 * top, and 2^128 = 2^96 * 2^32 = -2^32 (mod p).
+struct WideAcc {
+#ifdef __CUDA_ARCH__
+    uint32_t r0, r1, r2, r3, top;
+#else
+    uint64_t lo, hi;
+    uint32_t top;
+#endif
+    ZK_HD void zero()
+    {
+#ifdef __CUDA_ARCH__
+        r0 = r1 = r2 = r3 = top = 0;
+#else
+        lo = hi = 0;
+        top = 0;
+#endif
+    }
+    // += a * b (any 64-bit representatives)
+    ZK_HD void mac(uint64_t a, uint64_t b)
+    {
+#ifdef __CUDA_ARCH__
+        uint32_t p0, p1, p2, p3;
+        mul_wide(a, b, p0, p1, p2, p3);
+        asm("{\n\t"
+            "add.cc.u32   %0, %0, %5;\n\t"
+            "addc.cc.u32  %1, %1, %6;\n\t"
+            "addc.cc.u32  %2, %2, %7;\n\t"
+            "addc.cc.u32  %3, %3, %8;\n\t"
+            "addc.u32     %4, %4, 0;\n\t"
+            "}"
+            : "+r"(r0), "+r"(r1), "+r"(r2), "+r"(r3), "+r"(top)
+            : "r"(p0), "r"(p1), "r"(p2), "r"(p3));
+#else
+        const unsigned __int128 x = (unsigned __int128)a * b;
+        const unsigned __int128 s = (((unsigned __int128)hi << 64) | lo) + x;
+        top += s < x;
+        lo = (uint64_t)s;
+        hi = (uint64_t)(s >> 64);
+#endif
+    }
+    // any 64-bit representative of the sum
+    ZK_HD uint64_t reduce() const
+    {
+#ifdef __CUDA_ARCH__
+        const uint64_t t = reduce_nc(r0, r1, r2, r3);
+#else
+        const uint64_t t = gl_reduce128(lo, hi);
+#endif
+        // t - top * 2^32; when it borrows, t - x + p is in [0, 2^64) because
+        // x = top * 2^32 <= p
+        const uint64_t x = (uint64_t)top << 32;
+        const uint64_t d = t - x;
+        return t < x ? d - GL_EPS : d;
+    }
+};
+
 // a + b where at least one operand is < p: one wrap correction suffices
 // (a + b - 2^64 + EPS = a + b - p < 2^64).
 ZK_HD uint64_t gl_add_nc(uint64_t a, uint64_t b)

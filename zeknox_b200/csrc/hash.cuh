@@ -31,6 +31,11 @@ enum HashKind : int { HASH_POSEIDON = 0, HASH_KECCAK = 1, HASH_POSEIDON_BN128 = 
 #endif
 
 ZK_CONST_TABLE(uint64_t, POSEIDON_RC, 360, ZK_POSEIDON_RC_LIST)
+ZK_CONST_TABLE(uint64_t, POSEIDON_FAST_FIRST, 12, ZK_POSEIDON_FAST_FIRST_LIST)
+ZK_CONST_TABLE(uint64_t, POSEIDON_FAST_INIT, 121, ZK_POSEIDON_FAST_INIT_LIST)
+ZK_CONST_TABLE(uint64_t, POSEIDON_FAST_K, 22, ZK_POSEIDON_FAST_K_LIST)
+ZK_CONST_TABLE(uint64_t, POSEIDON_FAST_W, 242, ZK_POSEIDON_FAST_W_LIST)
+ZK_CONST_TABLE(uint64_t, POSEIDON_FAST_V, 242, ZK_POSEIDON_FAST_V_LIST)
 ZK_CONST_TABLE(uint64_t, POSEIDON2_RC, 360, ZK_POSEIDON2_RC_LIST)
 ZK_CONST_TABLE(uint64_t, POSEIDON2_DIAG, 12, ZK_POSEIDON2_DIAG_LIST)
 ZK_CONST_TABLE(uint64_t, MONOLITH_RC, 84, ZK_MONOLITH_RC_LIST)
@@ -123,22 +128,55 @@ ZK_HD void poseidon_mds(uint64_t s[12])
     for (int i = 0; i < 12; i++) s[i] = t[i];
 }
 
+// The 22 partial rounds in sparse-matrix form (Poseidon paper, eprint
+// 2019/458 appendix B; the same rewriting as native/poseidon/poseidon.cpp's
+// partial_rounds with its FAST_PARTIAL_* tables, whose values
+// gen_constants.py derives from the MDS matrix and round constants and checks
+// against the round-by-round form): one dense 11 x 11 layer, then per round
+// the S-box on lane 0 and a matrix with one dense row and one dense column --
+// 22 full multiplies per round instead of a 144-term MDS product.
+ZK_HD void poseidon_partial_rounds(uint64_t s[12])
+{
+#pragma unroll
+    for (int i = 0; i < 12; i++) s[i] = gl_add_nc(s[i], ZKC(POSEIDON_FAST_FIRST)[i]);
+    uint64_t t[11];
+#pragma unroll
+    for (int i = 0; i < 11; i++) {
+        WideAcc a;
+        a.zero();
+#pragma unroll
+        for (int j = 0; j < 11; j++) a.mac(s[1 + j], ZKC(POSEIDON_FAST_INIT)[11 * i + j]);
+        t[i] = a.reduce();
+    }
+#pragma unroll
+    for (int i = 0; i < 11; i++) s[1 + i] = t[i];
+#pragma unroll 1
+    for (int r = 0; r < 22; r++) {
+        const uint64_t x0 = gl_add_nc(gl_sbox7_nc(s[0]), ZKC(POSEIDON_FAST_K)[r]);
+        WideAcc a;
+        a.zero();
+        a.mac(x0, ZK_POSEIDON_FAST_M00);
+#pragma unroll
+        for (int i = 0; i < 11; i++) a.mac(s[1 + i], ZKC(POSEIDON_FAST_W)[11 * r + i]);
+        s[0] = a.reduce();
+#pragma unroll
+        for (int i = 0; i < 11; i++) s[1 + i] = gl_mul_add_nc(x0, ZKC(POSEIDON_FAST_V)[11 * r + i], s[1 + i]);
+    }
+}
+
 // Lanes hold any 64-bit representative between rounds (round constants are
 // < p, so one wrap correction suffices when adding them); the caller
-// canonicalises the digest.
+// canonicalises the digest.  One rolled loop over the 8 full rounds, the
+// partial rounds after the fourth, so the full-round code exists once.
 ZK_HD void poseidon_permute(uint64_t s[12])
 {
 #pragma unroll 1
-    for (int r = 0; r < 30; r++) {
-        if (r < 4 || r >= 26) {
+    for (int f = 0; f < 8; f++) {
+        const int r = f < 4 ? f : f + 22;
 #pragma unroll
-            for (int i = 0; i < 12; i++) s[i] = gl_sbox7_nc(gl_add_nc(s[i], ZKC(POSEIDON_RC)[12 * r + i]));
-        } else {
-            s[0] = gl_sbox7_nc(gl_add_nc(s[0], ZKC(POSEIDON_RC)[12 * r]));
-#pragma unroll
-            for (int i = 1; i < 12; i++) s[i] = gl_add_nc(s[i], ZKC(POSEIDON_RC)[12 * r + i]);
-        }
+        for (int i = 0; i < 12; i++) s[i] = gl_sbox7_nc(gl_add_nc(s[i], ZKC(POSEIDON_RC)[12 * r + i]));
         poseidon_mds(s);
+        if (f == 3) poseidon_partial_rounds(s);
     }
 }
 
