@@ -187,31 +187,51 @@ ZK_HD void poseidon_permute(uint64_t s[12])
 // groups, then every lane adds the sum of its column across the groups -- so
 // lane 4g+k ends as  sum_j (1 + [g'==g]) * (M4 x_g')_k.  Internal layer:
 // s_i <- s_i * diag_i + sum(s).
+//
+// The external layer runs on 22-bit pieces of each lane with the M4 addition chain
+// of the Poseidon2 paper (eprint 2023/323, appendix B): t0 = x0+x1, t1 = x2+x3,
+// t2 = 2x1+t1, t3 = 2x3+t0, t4 = 4t1+t3, t5 = 4t0+t2, M4 x = (t3+t5, t5, t2+t4,
+// t4).  Every coefficient of a lane (own block doubled plus the other two)
+// sums to 64, so a piece stays below 64 x 2^22 = 2^28.
+ZK_HD void p2_m4_pieces(uint32_t *x)
+{
+    const uint32_t t0 = x[0] + x[1], t1 = x[2] + x[3];
+    const uint32_t t2 = 2 * x[1] + t1, t3 = 2 * x[3] + t0;
+    const uint32_t t4 = 4 * t1 + t3, t5 = 4 * t0 + t2;
+    x[0] = t3 + t5;
+    x[1] = t5;
+    x[2] = t2 + t4;
+    x[3] = t4;
+}
+
 ZK_HD void p2_external(uint64_t s[12])
 {
-    // M4 rows expanded; each output is a small-coefficient combination, so
-    // accumulate the whole layer exactly and reduce once per lane.
-    uint64_t y[12];
+    uint32_t p[3][12];
 #pragma unroll
-    for (int k = 0; k < 4; k++) {
-        // coefficient of x_{4g'+j} in lane 4g+k: M4[k][j] * (1 + [g'==g])
-        constexpr uint32_t M4[4][4] = {{5, 7, 1, 3}, {4, 6, 1, 1}, {1, 3, 5, 7}, {1, 1, 4, 6}};
-        Acc96 col;
-        col.zero();
+    for (int j = 0; j < 12; j++) {
+        p[0][j] = (uint32_t)s[j] & 0x3FFFFFu;
+        p[1][j] = (uint32_t)(s[j] >> 22) & 0x3FFFFFu;
+        p[2][j] = (uint32_t)(s[j] >> 44);
+    }
 #pragma unroll
-        for (int g = 0; g < 3; g++)
+    for (int q = 0; q < 3; q++) {
 #pragma unroll
-            for (int j = 0; j < 4; j++) col.mac(s[4 * g + j], M4[k][j]);
+        for (int g = 0; g < 3; g++) p2_m4_pieces(&p[q][4 * g]);
 #pragma unroll
-        for (int g = 0; g < 3; g++) {
-            Acc96 a = col;
+        for (int k = 0; k < 4; k++) {
+            const uint32_t col = p[q][k] + p[q][4 + k] + p[q][8 + k];
 #pragma unroll
-            for (int j = 0; j < 4; j++) a.mac(s[4 * g + j], M4[k][j]);
-            y[4 * g + k] = a.reduce();
+            for (int g = 0; g < 3; g++) p[q][4 * g + k] += col;
         }
     }
 #pragma unroll
-    for (int i = 0; i < 12; i++) s[i] = y[i];
+    for (int j = 0; j < 12; j++) {
+        const uint64_t l1 = (uint64_t)p[0][j] + ((uint64_t)p[1][j] << 22);
+        const uint64_t l2 = (uint64_t)p[2][j] << 44;
+        const uint64_t lo = l1 + l2;
+        const uint64_t hi = (p[2][j] >> 20) + (lo < l2);
+        s[j] = gl_reduce96_nc(lo, hi);
+    }
 }
 
 // Lanes hold any 64-bit representative between layers; digests are
@@ -238,52 +258,6 @@ ZK_HD void poseidon2_permute(uint64_t s[12])
             // s_i * d_i + sum as one 128-bit value, reduced once
 #pragma unroll
             for (int i = 0; i < 12; i++) s[i] = gl_mul_add_nc(s[i], ZKC(POSEIDON2_DIAG)[i], sum);
-        }
-    }
-}
-
-// K independent Poseidon2 states advanced in lockstep: one instruction
-// stream serves K permutations (more ILP, fewer instruction fetches per
-// permutation).  Same arithmetic as poseidon2_permute.
-template <int K>
-ZK_HD void p2_external_k(uint64_t (&s)[K][12])
-{
-#pragma unroll
-    for (int k = 0; k < K; k++) p2_external(s[k]);
-}
-
-template <int K>
-ZK_HD void poseidon2_permute_k(uint64_t (&s)[K][12])
-{
-    p2_external_k<K>(s);
-#pragma unroll 1
-    for (int r = 0; r < 30; r++) {
-        if (r < 4 || r >= 26) {
-#pragma unroll
-            for (int i = 0; i < 12; i++) {
-                const uint64_t rc = ZKC(POSEIDON2_RC)[12 * r + i];
-#pragma unroll
-                for (int k = 0; k < K; k++) s[k][i] = gl_sbox7_nc(gl_add_nc(s[k][i], rc));
-            }
-            p2_external_k<K>(s);
-        } else {
-            const uint64_t rc = ZKC(POSEIDON2_RC)[12 * r];
-            uint64_t sum[K];
-#pragma unroll
-            for (int k = 0; k < K; k++) {
-                s[k][0] = gl_sbox7_nc(gl_add_nc(s[k][0], rc));
-                Sum64 acc;
-                acc.set(s[k][0]);
-#pragma unroll
-                for (int i = 1; i < 12; i++) acc.add(s[k][i]);
-                sum[k] = acc.reduce();
-            }
-#pragma unroll
-            for (int i = 0; i < 12; i++) {
-                const uint64_t d = ZKC(POSEIDON2_DIAG)[i];
-#pragma unroll
-                for (int k = 0; k < K; k++) s[k][i] = gl_mul_add_nc(s[k][i], d, sum[k]);
-            }
         }
     }
 }
