@@ -10,12 +10,14 @@
 #include "poseidon2/poseidon2.hpp"
 #include "keccak/keccak.hpp"
 #include "monolith/monolith.hpp"
+#include "poseidon/poseidon_bn128.hpp"
 
 extern "C" int zkref_hash_one(int type, u64 *in, u64 n, u64 *out)
 {
     switch (type) {
     case 0: PoseidonHasher::cpu_hash_one(in, n, out); return 0;
     case 1: KeccakHasher::cpu_hash_one(in, n, out); return 0;
+    case 2: PoseidonBN128Hasher::cpu_hash_one(in, n, out); return 0;
     case 3: Poseidon2Hasher::cpu_hash_one(in, n, out); return 0;
     case 4: MonolithHasher::cpu_hash_one(in, n, out); return 0;
     default: return -1;
@@ -27,6 +29,7 @@ extern "C" int zkref_hash_two(int type, u64 *l, u64 *r, u64 *out)
     switch (type) {
     case 0: PoseidonHasher::cpu_hash_two(l, r, out); return 0;
     case 1: KeccakHasher::cpu_hash_two(l, r, out); return 0;
+    case 2: PoseidonBN128Hasher::cpu_hash_two(l, r, out); return 0;
     case 3: Poseidon2Hasher::cpu_hash_two(l, r, out); return 0;
     case 4: MonolithHasher::cpu_hash_two(l, r, out); return 0;
     default: return -1;

@@ -380,6 +380,157 @@ static void keccak256(const uint8_t *in, u64 len, uint8_t out[32])
     memcpy(out, st, 32);
 }
 
+/* --------------------------------------------------------- Poseidon-BN128 */
+
+/* F_r, r the BN254 scalar field order: 4 x 64-bit little-endian limbs in
+ * Montgomery form (R = 2^256), as native/poseidon/element_bn128.cu keeps them;
+ * multiplication is the textbook CIOS Montgomery product on u128. */
+typedef struct {
+    u64 v[4];
+} fr_t;
+
+static const u32 BN_R32[8] = {ZK_BN254_R_LIST};
+static const u32 BN_R2_32[8] = {ZK_BN254_R2_LIST};
+static const u32 BN_C32[800] = {ZK_BN128_C_LIST};
+static const u32 BN_S32[4320] = {ZK_BN128_S_LIST};
+static const u32 BN_M32[200] = {ZK_BN128_M_LIST};
+static const u32 BN_P32[200] = {ZK_BN128_P_LIST};
+
+static fr_t fr_load(const u32 *t, int idx)
+{
+    fr_t x;
+    for (int i = 0; i < 4; i++) x.v[i] = (u64)t[8 * idx + 2 * i] | ((u64)t[8 * idx + 2 * i + 1] << 32);
+    return x;
+}
+
+static int fr_geq(const u64 *a, const u64 *b)
+{
+    for (int i = 3; i >= 0; i--)
+        if (a[i] != b[i]) return a[i] > b[i];
+    return 1;
+}
+
+static void fr_sub_in(u64 *a, const u64 *b)
+{
+    u64 borrow = 0;
+    for (int i = 0; i < 4; i++) {
+        u128 d = (u128)a[i] - b[i] - borrow;
+        a[i] = (u64)d;
+        borrow = (u64)(d >> 127);
+    }
+}
+
+static fr_t bn_add(fr_t a, fr_t b)
+{
+    const fr_t r = fr_load(BN_R32, 0);
+    fr_t s;
+    u64 c = 0;
+    for (int i = 0; i < 4; i++) {
+        u128 t = (u128)a.v[i] + b.v[i] + c;
+        s.v[i] = (u64)t;
+        c = (u64)(t >> 64);
+    }
+    if (c || fr_geq(s.v, r.v)) fr_sub_in(s.v, r.v);
+    return s;
+}
+
+static fr_t bn_mul(fr_t a, fr_t b)
+{
+    const fr_t r = fr_load(BN_R32, 0);
+    /* -r^-1 mod 2^64 by Newton's iteration (x <- x (2 - r x)) */
+    u64 inv = 1;
+    for (int i = 0; i < 6; i++) inv *= 2 - r.v[0] * inv;
+    const u64 np = (u64)0 - inv;
+    u64 t[6] = {0, 0, 0, 0, 0, 0};
+    for (int i = 0; i < 4; i++) {
+        u64 c = 0;
+        for (int j = 0; j < 4; j++) {
+            u128 x = (u128)a.v[i] * b.v[j] + t[j] + c;
+            t[j] = (u64)x;
+            c = (u64)(x >> 64);
+        }
+        u128 x = (u128)t[4] + c;
+        t[4] = (u64)x;
+        t[5] = (u64)(x >> 64);
+        const u64 m = t[0] * np;
+        x = (u128)m * r.v[0] + t[0];
+        c = (u64)(x >> 64);
+        for (int j = 1; j < 4; j++) {
+            x = (u128)m * r.v[j] + t[j] + c;
+            t[j - 1] = (u64)x;
+            c = (u64)(x >> 64);
+        }
+        x = (u128)t[4] + c;
+        t[3] = (u64)x;
+        t[4] = t[5] + (u64)(x >> 64);
+    }
+    fr_t z = {{t[0], t[1], t[2], t[3]}};
+    if (t[4] || fr_geq(z.v, r.v)) fr_sub_in(z.v, r.v);
+    return z;
+}
+
+static fr_t bn_exp5(fr_t x)
+{
+    fr_t x2 = bn_mul(x, x), x4 = bn_mul(x2, x2);
+    return bn_mul(x4, x);
+}
+
+static void bn_mix(fr_t st[5], const u32 *m)
+{
+    fr_t ns[5];
+    for (int i = 0; i < 5; i++) {
+        ns[i] = bn_mul(fr_load(m, i), st[0]);
+        for (int j = 1; j < 5; j++) ns[i] = bn_add(ns[i], bn_mul(fr_load(m, 5 * j + i), st[j]));
+    }
+    memcpy(st, ns, sizeof ns);
+}
+
+/* native/poseidon/poseidon_bn128.cu:115-212 (permute_fn + permute): lanes
+ * 3i..3i+2 form element i+1 (big-endian lane order, top limb 0), t = 5,
+ * 4 full rounds (constants, x^5, M; P for the fourth), 60 sparse partial
+ * rounds, 4 full rounds (no constants in the last); slots 0..3 back to the
+ * lanes (low 192 bits), each reduced once mod p. */
+static void zko_poseidon_bn128_permute(u64 s[12])
+{
+    fr_t st[5];
+    memset(st, 0, sizeof st);
+    const fr_t r2 = fr_load(BN_R2_32, 0);
+    for (int i = 0; i < 4; i++) {
+        fr_t x = {{s[3 * i + 2] % P, s[3 * i + 1] % P, s[3 * i] % P, 0}};
+        st[1 + i] = bn_mul(x, r2);
+    }
+    for (int i = 0; i < 5; i++) st[i] = bn_add(st[i], fr_load(BN_C32, i));
+    for (int f = 0; f < 3; f++) {
+        for (int i = 0; i < 5; i++) st[i] = bn_exp5(st[i]);
+        for (int i = 0; i < 5; i++) st[i] = bn_add(st[i], fr_load(BN_C32, 5 * (f + 1) + i));
+        bn_mix(st, BN_M32);
+    }
+    for (int i = 0; i < 5; i++) st[i] = bn_exp5(st[i]);
+    for (int i = 0; i < 5; i++) st[i] = bn_add(st[i], fr_load(BN_C32, 20 + i));
+    bn_mix(st, BN_P32);
+    for (int r = 0; r < 60; r++) {
+        st[0] = bn_add(bn_exp5(st[0]), fr_load(BN_C32, 25 + r));
+        fr_t n0 = bn_mul(fr_load(BN_S32, 9 * r), st[0]);
+        for (int j = 1; j < 5; j++) n0 = bn_add(n0, bn_mul(fr_load(BN_S32, 9 * r + j), st[j]));
+        for (int k = 1; k < 5; k++) st[k] = bn_add(st[k], bn_mul(st[0], fr_load(BN_S32, 9 * r + 4 + k)));
+        st[0] = n0;
+    }
+    for (int f = 0; f < 3; f++) {
+        for (int i = 0; i < 5; i++) st[i] = bn_exp5(st[i]);
+        for (int i = 0; i < 5; i++) st[i] = bn_add(st[i], fr_load(BN_C32, 85 + 5 * f + i));
+        bn_mix(st, BN_M32);
+    }
+    for (int i = 0; i < 5; i++) st[i] = bn_exp5(st[i]);
+    bn_mix(st, BN_M32);
+    const fr_t one = {{1, 0, 0, 0}};
+    for (int i = 0; i < 4; i++) {
+        fr_t v = bn_mul(st[i], one);
+        s[3 * i] = v.v[2] % P;
+        s[3 * i + 1] = v.v[1] % P;
+        s[3 * i + 2] = v.v[0] % P;
+    }
+}
+
 /* ---------------------------------------------------------------- sponges */
 
 enum { H_POSEIDON = 0, H_KECCAK = 1, H_POSEIDON_BN128 = 2, H_POSEIDON2 = 3, H_MONOLITH = 4 };
@@ -388,6 +539,7 @@ static void permute(int h, u64 s[12])
 {
     if (h == H_POSEIDON) zko_poseidon_permute(s);
     else if (h == H_POSEIDON2) zko_poseidon2_permute(s);
+    else if (h == H_POSEIDON_BN128) zko_poseidon_bn128_permute(s);
     else zko_monolith_permute(s);
 }
 
@@ -408,7 +560,7 @@ int zko_hash_one(int h, const u64 *in, u64 n, u64 out[4])
         out[3] &= 0xFF;
         return 0;
     }
-    if (h != H_POSEIDON && h != H_POSEIDON2 && h != H_MONOLITH) return -1;
+    if (h != H_POSEIDON && h != H_POSEIDON2 && h != H_MONOLITH && h != H_POSEIDON_BN128) return -1;
     if (n <= 4) {
         for (u64 i = 0; i < 4; i++) out[i] = i < n ? in[i] : 0;
         return 0;
@@ -436,7 +588,7 @@ int zko_hash_two(int h, const u64 l[4], const u64 r[4], u64 out[4])
         out[3] &= 0xFF;
         return 0;
     }
-    if (h != H_POSEIDON && h != H_POSEIDON2 && h != H_MONOLITH) return -1;
+    if (h != H_POSEIDON && h != H_POSEIDON2 && h != H_MONOLITH && h != H_POSEIDON_BN128) return -1;
     u64 s[12] = {0};
     memcpy(s, l, 32);
     memcpy(s + 4, r, 32);
@@ -447,7 +599,7 @@ int zko_hash_two(int h, const u64 l[4], const u64 r[4], u64 out[4])
 
 int zko_permute(int h, u64 s[12])
 {
-    if (h != H_POSEIDON && h != H_POSEIDON2 && h != H_MONOLITH) return -1;
+    if (h != H_POSEIDON && h != H_POSEIDON2 && h != H_MONOLITH && h != H_POSEIDON_BN128) return -1;
     permute(h, s);
     return 0;
 }

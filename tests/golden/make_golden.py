@@ -9,7 +9,8 @@ Run in a checkout that has the zeknox reference tree and its CPU library built
 Produces
   kat.json        known-answer vectors copied as data from the reference's own
                   tests (native/tests/tests.cu:164-173 Keccak, :204 Monolith,
-                  :279-292 Poseidon, :425-428 Poseidon2) plus the 4-leaf x 7
+                  :279-292 Poseidon, :425-428 Poseidon2, :492-501 Poseidon-BN128)
+                  plus the 4-leaf x 7
                   trees of :241-274 / :338-375 / :451-489 hashed by the
                   reference CPU hashers, and the root tables of
                   native/ff/gl64_params.hpp.
@@ -33,7 +34,7 @@ ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, ROOT)
 from oracle import oracle as O  # noqa: E402
 
-HASHES = {"poseidon": 0, "keccak": 1, "poseidon2": 3, "monolith": 4}
+HASHES = {"poseidon": 0, "keccak": 1, "poseidon2": 3, "monolith": 4, "poseidon_bn128": 2}
 
 # (n_leaves, leaf_size, cap_height) per hash: special cases (caps == leaves,
 # 2-leaf subtrees), odd leaf sizes, <= 4-element leaves and several levels.
@@ -96,6 +97,10 @@ def main():
         kat["poseidon2_input"].append(kat["poseidon2_input"][-1] + kat["poseidon2_input"][-2])
     kat["poseidon2_expected"] = [int(x, 16) for x in re.findall(r"h1\[\d\] == (0x[0-9a-fA-F]+)", seg)]
     assert len(kat["poseidon2_expected"]) == 4
+    # Poseidon-BN128 (tests.cu:492-501)
+    seg = tests[tests.index("TEST(LIBCUDA, poseidonbn128_test1)"):]
+    kat["poseidon_bn128_input"] = parse_u64_list(block_after(seg, "u64 inp[12]"))
+    kat["poseidon_bn128_expected"] = parse_u64_list(block_after(seg, "expected[4]"))
     # 4 leaves x 7 test tree (tests.cu:241-244), hashed by the reference CPU hashers
     seg = tests[tests.index("TEST(LIBCUDA, monolith_test2)"):]
     leaves = parse_u64_list(block_after(seg, "u64 test_leaves[28]"))
@@ -114,6 +119,8 @@ def main():
     kat["group_generator"] = 7
     # reference CPU agrees with its own KATs
     assert [int(x) for x in O.ref_hash_one(3, np.array(kat["poseidon2_input"], dtype=np.uint64))] == kat["poseidon2_expected"]
+    assert [int(x) for x in O.ref_hash_one(2, np.array(kat["poseidon_bn128_input"], dtype=np.uint64))] == \
+        kat["poseidon_bn128_expected"]
     with open(os.path.join(HERE, "kat.json"), "w") as f:
         json.dump(kat, f, indent=1)
 

@@ -6,7 +6,7 @@ import numpy as np
 from oracle import oracle as O
 from tests.golden.make_golden import MERKLE_CASES, FULL_DIGESTS_MAX, merkle_seed  # noqa: F401
 
-HASHES = {"poseidon": 0, "keccak": 1, "poseidon2": 3, "monolith": 4}
+HASHES = {"poseidon": 0, "keccak": 1, "poseidon2": 3, "monolith": 4, "poseidon_bn128": 2}
 
 
 def to_dev(arr, device="cuda"):

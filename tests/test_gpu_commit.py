@@ -29,7 +29,7 @@ def expect(coeffs, lg, rate, cols, cap, h, gen=7):
 
 @pytest.mark.parametrize("lg,rate,cols,cap,h", [
     (1, 1, 1, 0, 3), (2, 2, 3, 1, 0), (4, 3, 16, 2, 3), (6, 1, 17, 0, 4), (9, 3, 8, 4, 1), (10, 2, 33, 3, 3),
-    (12, 1, 5, 12, 0), (13, 3, 20, 4, 3), (14, 2, 64, 16, 3), (15, 3, 24, 4, 3)])
+    (12, 1, 5, 12, 0), (13, 3, 20, 4, 3), (14, 2, 64, 16, 3), (15, 3, 24, 4, 3), (8, 2, 12, 2, 2)])
 def test_commit_matches_oracle(lg, rate, cols, cap, h):
     c = O.field_data(lg * 100 + cols, cols << lg)
     job, (leaves, dig, caps, n_dig) = alloc_job(lg, rate, cols, cap, h, to_dev(c))
@@ -113,7 +113,7 @@ def test_commit_argument_errors():
     with pytest.raises(zk.ZeknoxError):
         zk.commit(0, job)
     job.rate_bits = 1
-    job.hash_type = 2
+    job.hash_type = 5  # no such hash
     with pytest.raises(zk.ZeknoxError):
         zk.commit(0, job)
 

@@ -66,6 +66,8 @@ def test_kat_single_hashes(kat):
     assert [int(x) for x in cap[0]] == kat["poseidon2_expected"]
     _, cap = run_gpu(np.array(kat["monolith_input"], dtype=np.uint64), 1, 12, 0, 4)
     assert [int(x) for x in cap[0]] == kat["monolith_expected"]
+    _, cap = run_gpu(np.array(kat["poseidon_bn128_input"], dtype=np.uint64), 1, 12, 0, 2)
+    assert [int(x) for x in cap[0]] == kat["poseidon_bn128_expected"]
     for size in (4, 5, 6):
         _, cap = run_gpu(np.array(kat["keccak_data"][:size], dtype=np.uint64), 1, size, 0, 1)
         assert [int(x) for x in cap[0]] == kat["keccak_expected"][size]
@@ -80,7 +82,7 @@ def test_rejects_bad_geometry_without_writing():
                                                             0, 0)
         raise zk.ZeknoxError(1, zk.last_error() or "")
     with pytest.raises(zk.ZeknoxError):
-        zk.fill_digests_buf_linear_gpu(dig, cap, leaves, 16, 5, 1, 2)  # Poseidon-BN128 is not built
+        zk.fill_digests_buf_linear_gpu(dig, cap, leaves, 16, 5, 1, 7)  # no hash type 7
     torch.cuda.synchronize()
     assert bool((dig == 7).all()) and bool((cap == 7).all())
 

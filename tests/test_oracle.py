@@ -46,6 +46,11 @@ def test_poseidon2_monolith_kat(kat):
     assert [int(x) for x in O.hash_one(4, np.array(kat["monolith_input"], dtype=np.uint64))] == kat["monolith_expected"]
 
 
+def test_poseidon_bn128_kat(kat):
+    inp = np.array(kat["poseidon_bn128_input"], dtype=np.uint64)
+    assert [int(x) for x in O.hash_one(2, inp)] == kat["poseidon_bn128_expected"]
+
+
 @pytest.mark.parametrize("name", list(HASHES))
 def test_tree4x7(kat, name):
     h = HASHES[name]

@@ -19,8 +19,7 @@ void check_job(const zk_commit_job &j)
     if (j.cap_height > j.lg_n + j.rate_bits) throw arg_failure("cap_height above log2 of the leaf count");
     if (!j.input || !j.leaves || !j.caps || (!j.digests && j.cap_height < j.lg_n + j.rate_bits))
         throw arg_failure("null buffer");
-    if (j.hash_type != 0 && j.hash_type != 1 && j.hash_type != 3 && j.hash_type != 4)
-        throw arg_failure("unsupported hash_type");
+    if (j.hash_type > 4) throw arg_failure("unsupported hash_type");
 }
 
 uint64_t commit_scratch_words(uint32_t lg_n, uint32_t rate_bits, uint32_t cols, bool values, bool host_input)
@@ -245,8 +244,7 @@ void merkle_batch_graph(DeviceCtx &c, const zk_merkle_job *jobs, uint32_t njobs)
         const uint64_t n_caps = 1ULL << j.cap_height;
         if (j.cap_height >= 63 || !merkle_geometry_ok(2 * (j.n_leaves - n_caps), n_caps, j.n_leaves, j.cap_height, err))
             throw arg_failure("tree " + std::to_string(i) + ": " + (err.empty() ? "bad cap_height" : err));
-        if (j.hash_type != 0 && j.hash_type != 1 && j.hash_type != 3 && j.hash_type != 4)
-            throw arg_failure("tree " + std::to_string(i) + ": unsupported hash_type");
+        if (j.hash_type > 4) throw arg_failure("tree " + std::to_string(i) + ": unsupported hash_type");
         if (!j.leaves || !j.caps || (!j.digests && n_caps < j.n_leaves)) throw arg_failure("null buffer");
         cost[i] = (double)j.n_leaves * ((j.leaf_size + 7) / 8 + 1);
         for (uint64_t v : {(uint64_t)j.leaves, (uint64_t)j.digests, (uint64_t)j.caps, j.n_leaves, j.leaf_size,

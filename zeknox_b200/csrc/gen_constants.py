@@ -17,6 +17,11 @@ way they are produced are this project's own:
   scalars, the dense initial matrix and the per-round row/column vectors) are
   *derived* from the MDS matrix and round constants (derive_poseidon_fast) and
   cross-checked against native/poseidon/poseidon.hpp:38-801.
+* BN254 Montgomery parameters (modulus limbs, R^2 mod r, -r^-1) are *derived*
+  from the field order and cross-checked against native/poseidon/element_bn128.cu;
+  the Poseidon-BN128 round constants and matrices (iden3's t = 5 parameters in
+  Montgomery form) are read as numbers from
+  native/poseidon/poseidon_bn128_constants.h.
 * Poseidon round constants (native/poseidon/poseidon.hpp:803-1164, 360 values,
   MDS circulant row and diagonal :35-36), Poseidon2 round constants and internal
   diagonal (native/poseidon2/poseidon2.cu:8-59) and Monolith round constants and
@@ -97,6 +102,23 @@ def _block(src, start_pat):
         j += 1
 
 
+# BN254 scalar field order (the Poseidon-BN128 hash works over it)
+BN_R = 21888242871839275222246405745257275088548364400416034343698204186575808495617
+
+
+def derive_bn254():
+    """Montgomery parameters of F_r with R = 2^256: r's 32-bit limbs,
+    R^2 mod r (to enter Montgomery form) and -r^-1 mod 2^32."""
+    limbs32 = [(BN_R >> (32 * i)) & 0xFFFFFFFF for i in range(8)]
+    r2 = (1 << 512) % BN_R
+    nprime32 = (-pow(BN_R, -1, 1 << 32)) % (1 << 32)
+    return limbs32, r2, nprime32
+
+
+def _limbs64(x):
+    return [(x >> (64 * i)) & 0xFFFFFFFFFFFFFFFF for i in range(4)]
+
+
 def read_reference(ref):
     nat = os.path.join(ref, "native")
     with open(os.path.join(nat, "poseidon/poseidon.hpp")) as f:
@@ -109,6 +131,12 @@ def read_reference(ref):
         params = f.read()
     with open(os.path.join(nat, "keccak/keccak.cu")) as f:
         kec = f.read()
+    with open(os.path.join(nat, "poseidon/poseidon_bn128_constants.h")) as f:
+        bnc = f.read()
+    with open(os.path.join(nat, "poseidon/element_bn128.cu")) as f:
+        bne = f.read()
+    with open(os.path.join(nat, "poseidon/poseidon_bn128.cu")) as f:
+        bnp = f.read()
 
     out = {}
     out["poseidon_rc"] = _numbers(_block(pos, r"ALL_ROUND_CONSTANTS\[[^\]]*\]\s*=\s*{"))
@@ -135,6 +163,19 @@ def read_reference(ref):
     out["k_rndc"] = _numbers(_block(kec, r"keccakf_rndc\)\[24\]\s*=\s*{"))
     out["k_rotc"] = _numbers(_block(kec, r"keccakf_rotc\)\[24\]\s*=\s*{"))
     out["k_piln"] = _numbers(_block(kec, r"keccakf_piln\)\[24\]\s*=\s*{"))
+    # Poseidon-BN128 (t = 5): round constants, sparse partial-round matrices,
+    # full-round matrix M and the pre-partial matrix P, all 4 x u64 little-endian
+    # limbs in Montgomery form (native/poseidon/poseidon_bn128_constants.h:16-737)
+    out["bn_c"] = _numbers(_block(bnc, r"C\[100\]\[4\]\s*=\s*{"))
+    out["bn_s"] = _numbers(_block(bnc, r"S\[540\]\[4\]\s*=\s*{"))
+    out["bn_m"] = _numbers(_block(bnc, r"M\[5\]\[5\]\[4\]\s*=\s*{"))
+    out["bn_p"] = _numbers(_block(bnc, r"P\[5\]\[5\]\[4\]\s*=\s*{"))
+    out["bn_r2"] = _numbers(_block(bne, r"rSquare\[4\]\s*#endif\s*=\s*{"))
+    out["bn_modulus"] = [int(x) for x in re.findall(r"madd3\(m, (\d+)u", bne)[:1]] + \
+        [int(x) for x in re.findall(r"madd2\(m, (\d+)u", bne)[:2]]
+    out["bn_m0"] = [int(x) for x in re.findall(r"madd0\(m, (\d+)u", bne)[:1]]
+    out["bn_np64"] = [int(x) for x in re.findall(r"m = c\[0\] \* (\d+)u", bne)[:1]]
+    out["bn_rounds_p"] = _numbers(_block(bnp, r"NROUNDSP\[16\]\s*=\s*{"))
     return out
 
 
@@ -246,7 +287,8 @@ def fmt_list(name, vals, per_line=4, hexw=16):
     for i in range(0, len(vals), per_line):
         chunk = vals[i:i + per_line]
         if hexw:
-            lines.append("    " + ", ".join("0x%0*xULL" % (hexw, v) for v in chunk))
+            suffix = "u" if hexw == 8 else "ULL"
+            lines.append("    " + ", ".join("0x%0*x%s" % (hexw, v, suffix) for v in chunk))
         else:
             lines.append("    " + ", ".join("%d" % v for v in chunk))
     return "#define %s \\\n" % name + ", \\\n".join(lines) + "\n"
@@ -280,6 +322,19 @@ def main():
     for r in range(12):
         for c in range(12):
             assert mat[12 * r + c] == row0[(c - r) % 12], "monolith matrix is not circulant"
+
+    # BN254 Montgomery parameters: derived, checked against the reference's literals
+    bn_limbs32, bn_r2, bn_np32 = derive_bn254()
+    r64 = _limbs64(BN_R)
+    assert ref["bn_m0"] == [r64[0]] and ref["bn_modulus"] == [r64[3], r64[1], r64[2]], "BN254 modulus mismatch"
+    assert ref["bn_r2"] == _limbs64(bn_r2), "BN254 R^2 mismatch"
+    assert ref["bn_np64"] == [(-pow(BN_R, -1, 1 << 64)) % (1 << 64)], "BN254 -r^-1 mismatch"
+    assert ref["bn_rounds_p"][3] == 60, "Poseidon-BN128 t = 5 partial rounds"
+    for name, count in (("bn_c", 100), ("bn_s", 540), ("bn_m", 25), ("bn_p", 25)):
+        v = ref[name]
+        assert len(v) == 4 * count, (name, len(v))
+        for i in range(0, len(v), 4):
+            assert v[i] | v[i + 1] << 64 | v[i + 2] << 128 | v[i + 3] << 192 < BN_R, name
 
     hdr = []
     hdr.append("/* Generated by gen_constants.py -- do not edit.\n"
@@ -321,6 +376,21 @@ def main():
                " * (entry [r][c] = row[(c - r) mod 12]). */\n")
     hdr.append(fmt_list("ZK_MONOLITH_RC_LIST", mono_rc))
     hdr.append(fmt_list("ZK_MONOLITH_CIRC_LIST", row0, 12, 0))
+    hdr.append("\n/* Poseidon-BN128 over F_r (BN254 scalar field), t = 5, 8 full + 60 partial rounds.\n"
+               " * Elements: 8 little-endian 32-bit limbs in Montgomery form (R = 2^256).\n"
+               " * C: 100 round constants; S: 60 x 9 sparse partial-round entries; M, P: 5 x 5\n"
+               " * matrices stored [j][i] (new_i = sum_j m[j][i] * s_j). */\n")
+    hdr.append(fmt_list("ZK_BN254_R_LIST", bn_limbs32, 8, 8))
+    hdr.append(fmt_list("ZK_BN254_R2_LIST", [(bn_r2 >> (32 * i)) & 0xFFFFFFFF for i in range(8)], 8, 8))
+    hdr.append("#define ZK_BN254_NP 0x%08xu\n" % bn_np32)
+
+    def to32(v64):
+        return [(x >> sh) & 0xFFFFFFFF for x in v64 for sh in (0, 32)]
+
+    hdr.append(fmt_list("ZK_BN128_C_LIST", to32(ref["bn_c"]), 8, 8))
+    hdr.append(fmt_list("ZK_BN128_S_LIST", to32(ref["bn_s"]), 8, 8))
+    hdr.append(fmt_list("ZK_BN128_M_LIST", to32(ref["bn_m"]), 8, 8))
+    hdr.append(fmt_list("ZK_BN128_P_LIST", to32(ref["bn_p"]), 8, 8))
     hdr.append("\n/* Keccak-f[1600]: iota constants, rho offsets along the pi walk, pi lanes */\n")
     hdr.append(fmt_list("ZK_KECCAK_RNDC_LIST", rndc))
     hdr.append(fmt_list("ZK_KECCAK_ROTC_LIST", rotc, 12, 0))

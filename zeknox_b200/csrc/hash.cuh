@@ -9,6 +9,7 @@
 #include <stdint.h>
 #include <string.h>
 
+#include "bn254.cuh"
 #include "gl64.cuh"
 #include "zk_constants.h"
 
@@ -40,6 +41,10 @@ ZK_CONST_TABLE(uint64_t, POSEIDON2_RC, 360, ZK_POSEIDON2_RC_LIST)
 ZK_CONST_TABLE(uint64_t, POSEIDON2_DIAG, 12, ZK_POSEIDON2_DIAG_LIST)
 ZK_CONST_TABLE(uint64_t, MONOLITH_RC, 84, ZK_MONOLITH_RC_LIST)
 ZK_CONST_TABLE(uint64_t, KECCAK_RNDC, 24, ZK_KECCAK_RNDC_LIST)
+ZK_CONST_TABLE(uint32_t, BN128_C, 800, ZK_BN128_C_LIST)
+ZK_CONST_TABLE(uint32_t, BN128_S, 4320, ZK_BN128_S_LIST)
+ZK_CONST_TABLE(uint32_t, BN128_M, 200, ZK_BN128_M_LIST)
+ZK_CONST_TABLE(uint32_t, BN128_P, 200, ZK_BN128_P_LIST)
 
 // Small circulant rows and the Keccak lane tables are compile-time constants
 // (folded into the code once the loops are unrolled).
@@ -370,6 +375,93 @@ ZK_HD void keccak_f(uint64_t st[25])
     }
 }
 
+// ----------------------------------------------------------- Poseidon-BN128
+//
+// native/poseidon/poseidon_bn128.cu:115-200: the 12 canonical Goldilocks lanes
+// become four 192-bit F_r elements (element i = lane 3i * 2^128 + lane 3i+1 *
+// 2^64 + lane 3i+2) in state slots 1..4 (slot 0 = 0); round constants before
+// every full round but the last, x^5 S-boxes, the full-round matrix M (P
+// before the partial rounds), 60 partial rounds in iden3's sparse form (S-box
+// on slot 0, + constant, new slot 0 = row . state, slot k += slot0 * column);
+// the low 192 bits of slots 0..3 go back to the lanes, each reduced once mod p.
+// Constant element idx of a table (read straight from the constant bank on
+// the device).
+#define ZK_BN_CONST(tab, idx)                                                \
+    ([&]() {                                                                 \
+        Fr x_;                                                               \
+        _Pragma("unroll") for (int k_ = 0; k_ < 8; k_++) x_.w[k_] = ZKC(tab)[8 * (idx) + k_]; \
+        return x_;                                                           \
+    }())
+
+// new_i = sum_j m[j][i] * s_j with m = P (pre = true) or M
+ZK_HD void bn128_mix(Fr st[5], bool pre)
+{
+    Fr ns[5];
+#pragma unroll
+    for (int i = 0; i < 5; i++) {
+#pragma unroll
+        for (int j = 0; j < 5; j++) {
+            const Fr m = pre ? ZK_BN_CONST(BN128_P, 5 * j + i) : ZK_BN_CONST(BN128_M, 5 * j + i);
+            const Fr t = fr_mul(m, st[j]);
+            ns[i] = j == 0 ? t : fr_add(ns[i], t);
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < 5; i++) st[i] = ns[i];
+}
+
+ZK_HD void poseidon_bn128_permute(uint64_t s[12])
+{
+    Fr st[5];
+    st[0] = fr_zero();
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+        Fr x;
+        const uint64_t l[3] = {gl_canon(s[3 * i + 2]), gl_canon(s[3 * i + 1]), gl_canon(s[3 * i])};
+#pragma unroll
+        for (int k = 0; k < 3; k++) {
+            x.w[2 * k] = (uint32_t)l[k];
+            x.w[2 * k + 1] = (uint32_t)(l[k] >> 32);
+        }
+        x.w[6] = x.w[7] = 0;
+        st[1 + i] = fr_to_mont(x);
+    }
+#pragma unroll
+    for (int i = 0; i < 5; i++) st[i] = fr_add(st[i], ZK_BN_CONST(BN128_C, i));
+#pragma unroll 1
+    for (int f = 0; f < 8; f++) {
+#pragma unroll
+        for (int i = 0; i < 5; i++) st[i] = fr_exp5(st[i]);
+        if (f != 7) {
+            const int c0 = f < 4 ? 5 * (f + 1) : 85 + 5 * (f - 4);
+#pragma unroll
+            for (int i = 0; i < 5; i++) st[i] = fr_add(st[i], ZK_BN_CONST(BN128_C, c0 + i));
+        }
+        bn128_mix(st, f == 3);
+        if (f == 3) {
+#pragma unroll 1
+            for (int r = 0; r < 60; r++) {
+                const Fr x0 = fr_add(fr_exp5(st[0]), ZK_BN_CONST(BN128_C, 25 + r));
+                Fr n0 = fr_mul(ZK_BN_CONST(BN128_S, 9 * r), x0);
+#pragma unroll
+                for (int j = 1; j < 5; j++) n0 = fr_add(n0, fr_mul(ZK_BN_CONST(BN128_S, 9 * r + j), st[j]));
+#pragma unroll
+                for (int k = 1; k < 5; k++) st[k] = fr_add(st[k], fr_mul(x0, ZK_BN_CONST(BN128_S, 9 * r + 4 + k)));
+                st[0] = n0;
+            }
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+        const Fr v = fr_from_mont(st[i]);
+#pragma unroll
+        for (int k = 0; k < 3; k++) {
+            const uint64_t limb = ((uint64_t)v.w[2 * k + 1] << 32) | v.w[2 * k];
+            s[3 * i + 2 - k] = gl_canon(limb);
+        }
+    }
+}
+
 // ------------------------------------------------------------------ sponges
 
 template <int H>
@@ -377,6 +469,7 @@ ZK_HD void permute(uint64_t s[12])
 {
     if (H == HASH_POSEIDON) poseidon_permute(s);
     else if (H == HASH_POSEIDON2) poseidon2_permute(s);
+    else if (H == HASH_POSEIDON_BN128) poseidon_bn128_permute(s);
     else monolith_permute(s);
 }
 

@@ -95,10 +95,11 @@ bool merkle_device(uint64_t *digests, uint64_t *caps, const uint64_t *leaves, ui
     switch (hash_type) {
     case HASH_POSEIDON: merkle_launch<HASH_POSEIDON>(digests, caps, leaves, g, stream); break;
     case HASH_KECCAK: merkle_launch<HASH_KECCAK>(digests, caps, leaves, g, stream); break;
+    case HASH_POSEIDON_BN128: merkle_launch<HASH_POSEIDON_BN128>(digests, caps, leaves, g, stream); break;
     case HASH_POSEIDON2: merkle_launch<HASH_POSEIDON2>(digests, caps, leaves, g, stream); break;
     case HASH_MONOLITH: merkle_launch<HASH_MONOLITH>(digests, caps, leaves, g, stream); break;
     default:
-        err = "unsupported hash_type " + std::to_string(hash_type) + " (Poseidon-BN128 is not built)";
+        err = "unsupported hash_type " + std::to_string(hash_type);
         return false;
     }
     cudaError_t e = cudaGetLastError();

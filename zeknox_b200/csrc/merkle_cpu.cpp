@@ -49,6 +49,9 @@ bool zk_merkle_cpu(void *digests, void *caps, const void *leaves, uint64_t n_dig
     switch (hash_type) {
     case zk::HASH_POSEIDON: build<zk::HASH_POSEIDON>(d, c, l, n_dig, n_cap, n_leaves, leaf_size, cap_height); break;
     case zk::HASH_KECCAK: build<zk::HASH_KECCAK>(d, c, l, n_dig, n_cap, n_leaves, leaf_size, cap_height); break;
+    case zk::HASH_POSEIDON_BN128:
+        build<zk::HASH_POSEIDON_BN128>(d, c, l, n_dig, n_cap, n_leaves, leaf_size, cap_height);
+        break;
     case zk::HASH_POSEIDON2: build<zk::HASH_POSEIDON2>(d, c, l, n_dig, n_cap, n_leaves, leaf_size, cap_height); break;
     case zk::HASH_MONOLITH: build<zk::HASH_MONOLITH>(d, c, l, n_dig, n_cap, n_leaves, leaf_size, cap_height); break;
     default: err = "unsupported hash_type " + std::to_string(hash_type); return false;
@@ -62,6 +65,7 @@ bool zk_hash_one_cpu(uint64_t hash_type, const uint64_t *in, uint64_t n, uint64_
     switch (hash_type) {
     case zk::HASH_POSEIDON: zk::hash_one<zk::HASH_POSEIDON>(in, n, out); return true;
     case zk::HASH_KECCAK: zk::hash_one<zk::HASH_KECCAK>(in, n, out); return true;
+    case zk::HASH_POSEIDON_BN128: zk::hash_one<zk::HASH_POSEIDON_BN128>(in, n, out); return true;
     case zk::HASH_POSEIDON2: zk::hash_one<zk::HASH_POSEIDON2>(in, n, out); return true;
     case zk::HASH_MONOLITH: zk::hash_one<zk::HASH_MONOLITH>(in, n, out); return true;
     default: return false;
@@ -73,6 +77,7 @@ bool zk_hash_two_cpu(uint64_t hash_type, const uint64_t *l, const uint64_t *r, u
     switch (hash_type) {
     case zk::HASH_POSEIDON: zk::hash_two<zk::HASH_POSEIDON>(l, r, out); return true;
     case zk::HASH_KECCAK: zk::hash_two<zk::HASH_KECCAK>(l, r, out); return true;
+    case zk::HASH_POSEIDON_BN128: zk::hash_two<zk::HASH_POSEIDON_BN128>(l, r, out); return true;
     case zk::HASH_POSEIDON2: zk::hash_two<zk::HASH_POSEIDON2>(l, r, out); return true;
     case zk::HASH_MONOLITH: zk::hash_two<zk::HASH_MONOLITH>(l, r, out); return true;
     default: return false;
