@@ -5,6 +5,7 @@
 // project's: a handful of multi-stage DIF passes (ntt.cuh) plus one tiled
 // reorder, instead of one HBM pass per radix-2 stage.
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <cstdlib>
 #include <cstring>
@@ -24,25 +25,47 @@ static constexpr int PASS_TILE = 8192;
 
 // ------------------------------------------------------------- pass dispatch
 
-template <int LOGR, int INV, int LOADM, int STOREM>
+template <int LOGR, int INV, int LOADM, int STOREM, int DIRECT>
 static void launch_one(const NttPassArgs &a, uint64_t grid, uint32_t smem, cudaStream_t s)
 {
-    auto k = ntt_pass_kernel<LOGR, INV, PASS_NT, PASS_TILE, LOADM, STOREM>;
-    static bool attr = false;
-    if (!attr) {
+    auto k = ntt_pass_kernel<LOGR, INV, PASS_NT, PASS_TILE, LOADM, STOREM, DIRECT>;
+    // the 64 KiB dynamic shared-memory opt-in is per device
+    static std::atomic<uint64_t> attr_set{0};
+    int dev = 0;
+    ZK_CUDA(cudaGetDevice(&dev));
+    const uint64_t bit = 1ULL << (dev & 63);
+    if (!(attr_set.load(std::memory_order_relaxed) & bit)) {
         ZK_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, PASS_TILE * 8));
         ZK_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared));
-        attr = true;
+        attr_set.fetch_or(bit, std::memory_order_relaxed);
     }
     k<<<(unsigned)grid, PASS_NT, smem, s>>>(a);
     note_launch();
 }
 
+// Whether a pass reads its first sub-step (and, for STORE_SAME, writes its
+// last) straight between global memory and registers: only where a warp's
+// accesses then stay sector-complete -- row tiles of at least 8 consecutive
+// positions per task, or STORE_SAME tiles that are runs of >= 4 consecutive
+// offsets.
+static bool direct_io(uint32_t logr, const NttPassArgs &a, bool rows)
+{
+    if (rows) return logr >= 7;
+    const uint32_t log_tile = std::min<uint32_t>(a.L, __builtin_ctz(PASS_TILE));
+    if (log_tile < logr) return false;
+    const uint32_t log_g = log_tile - logr;
+    return a.s_lo >= log_g && log_g >= 2;
+}
+
 template <int INV, int LOADM, int STOREM>
 static void launch_pass(uint32_t logr, const NttPassArgs &a, uint64_t grid, uint32_t smem, cudaStream_t s)
 {
-#define ZK_CASE(r) \
-    case r: launch_one<(STOREM == STORE_ROWS && r > 9) ? 9 : r, INV, LOADM, STOREM>(a, grid, smem, s); break;
+    const bool direct = direct_io(logr, a, STOREM == STORE_ROWS);
+#define ZK_CASE(r)                                                                                \
+    case r:                                                                                       \
+        if (direct) launch_one<(STOREM == STORE_ROWS && r > 9) ? 9 : r, INV, LOADM, STOREM, 1>(a, grid, smem, s); \
+        else launch_one<(STOREM == STORE_ROWS && r > 9) ? 9 : r, INV, LOADM, STOREM, 0>(a, grid, smem, s);   \
+        break;
     switch (logr) {
         ZK_CASE(1) ZK_CASE(2) ZK_CASE(3) ZK_CASE(4) ZK_CASE(5) ZK_CASE(6)
         ZK_CASE(7) ZK_CASE(8) ZK_CASE(9) ZK_CASE(10) ZK_CASE(11) ZK_CASE(12)

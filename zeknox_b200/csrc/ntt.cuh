@@ -147,6 +147,38 @@ __device__ __forceinline__ void dif_substeps(uint64_t *sm, uint32_t tile, const 
     if constexpr (LOG_RCUR > 4) dif_substeps<LOGR, INV, NT, LOG_RCUR - 4>(sm, tile, tw_small);
 }
 
+// log2 of the block size of the last sub-step of an R = 2^LOGR point DIF
+// (16-point sub-steps first): LOGR - 4 * floor((LOGR - 1) / 4).
+__host__ __device__ constexpr int last_substep_log(int logr) { return logr - 4 * ((logr - 1) / 4); }
+
+// The sub-steps strictly between the first (LOG_RCUR = LOGR) and the last
+// (LOG_RCUR = last_substep_log(LOGR)), smem to smem.
+template <int INV, int NT, int LOG_RCUR, int LAST>
+__device__ __forceinline__ void dif_middle_substeps(uint64_t *sm, uint32_t tile, const uint64_t *__restrict__ tw_small)
+{
+    if constexpr (LOG_RCUR > LAST) {
+        dif_substep<4, INV, NT, LOG_RCUR>(sm, tile, tw_small);
+        __syncthreads();
+        dif_middle_substeps<INV, NT, LOG_RCUR - 4, LAST>(sm, tile, tw_small);
+    }
+}
+
+// The inner twiddles after the first sub-step's E-point DIFs: position p of
+// task m_lo gets w_R^(m_lo * rev_e(p)), w_R = w_4096^(4096 / R).
+template <int LOGE, int LOGR>
+__device__ __forceinline__ void first_substep_twiddles(uint64_t *x, uint32_t m_lo, const uint64_t *__restrict__ tw_small)
+{
+    constexpr int E = 1 << LOGE;
+    if constexpr (LOGR > LOGE) {
+        const uint32_t step = m_lo << (12 - LOGR);
+#pragma unroll
+        for (int p = 1; p < E; p++) {
+            const uint32_t f = bitrev32((uint32_t)p, LOGE);
+            x[p] = gl_mul(x[p], __ldg(tw_small + ((step * f) & 4095u)));
+        }
+    }
+}
+
 // One pass: LOGR stages on groups of R = 2^LOGR elements; at most TILE
 // elements per CTA (dynamic shared memory of TILE words).
 //   STORE_SAME tiles: min(TILE, n) positions of one virtual column; when the
@@ -156,17 +188,23 @@ __device__ __forceinline__ void dif_substeps(uint64_t *sm, uint32_t tile, const 
 //   STORE_ROWS tiles (last pass, S == 1): 16 virtual columns of one coset and
 //     consecutive source columns x W positions, so every output leaf row gets
 //     16 consecutive 8-byte words.
-template <int LOGR, int INV, int NT, int TILE, int LOADM, int STOREM>
+// DIRECT (chosen by the host when a warp's accesses stay sector-complete:
+// STORE_ROWS, or STORE_SAME with row-run tiles of >= 4 groups): the first
+// sub-step loads its elements straight from global memory into registers and,
+// for STORE_SAME, the last sub-step stores straight from registers, instead of
+// separate load / store loops through shared memory.
+template <int LOGR, int INV, int NT, int TILE, int LOADM, int STOREM, int DIRECT>
 __global__ void __launch_bounds__(NT, 2) ntt_pass_kernel(NttPassArgs a)
 {
     extern __shared__ uint64_t sm[];
     constexpr uint32_t R = 1u << LOGR;
     constexpr uint32_t LOG_CW = 4, CW = 1u << LOG_CW;
     constexpr uint32_t LOG_TILE = __builtin_ctz(TILE);
+    constexpr int E0 = LOGR >= 4 ? 4 : LOGR;     // log2 size of the first sub-step
+    constexpr int LAST = last_substep_log(LOGR);  // log2 size of the last sub-step
     // all sizes are powers of two: index math is shifts and masks
     const uint32_t s_lo = a.s_lo;
     const uint32_t S = 1u << s_lo;
-    const uint64_t n = 1ULL << a.L;
     const uint32_t log_m = s_lo + LOGR;  // log2 M, M = R * S
     const uint32_t rmask = (1u << a.rate) - 1;
     const uint32_t log_w = (STOREM == STORE_ROWS) ? (a.L < LOG_TILE - LOG_CW ? a.L : LOG_TILE - LOG_CW) : 0;
@@ -203,6 +241,35 @@ __global__ void __launch_bounds__(NT, 2) ntt_pass_kernel(NttPassArgs a)
             pos = ((gid >> s_lo) << log_m) + ((uint64_t)m << s_lo) + (gid & (S - 1));
         }
     };
+    auto col_ok = [&](uint64_t vcol) {
+        return (STOREM == STORE_ROWS) ? ((vcol >> a.rate) < a.cols) : (vcol < a.vcols);
+    };
+    // the load-mode transform of the element at (vcol, pos); elements of one
+    // group member run m -> m + q are `step` positions apart
+    auto load_elem = [&](uint64_t vcol, uint64_t pos) -> uint64_t {
+        if (LOADM == LOAD_PLAIN) return a.src[vcol * a.src_stride + pos];
+        if (LOADM == LOAD_SCALE) return gl_mul(a.src[vcol * a.src_stride + pos], __ldg(a.tab + pos));
+        if (LOADM == LOAD_COSETS)
+            return gl_mul(a.src[(vcol >> a.rate) * a.src_stride + pos], __ldg(a.tab + ((vcol & rmask) << a.L) + pos));
+        return pos < a.n_src ? a.src[vcol * a.src_stride + pos] : 0;  // LOAD_EXTEND
+    };
+    // pass twiddle (S > 1) and the store of one element
+    auto store_elem = [&](uint64_t vcol, uint64_t pos, uint32_t m, uint64_t val) {
+        if (S > 1) {
+            const uint64_t o = pos & (S - 1);
+            const uint64_t f = bitrev32(m, LOGR);
+            val = gl_mul(val, __ldg(a.tw_pass + o * f));
+        }
+        if (STOREM == STORE_ROWS) {
+            const uint64_t b = vcol >> a.rate;
+            if (b < a.cols) {
+                const uint64_t row = ((uint64_t)bitrev32((uint32_t)(vcol & rmask), a.rate) << a.L) + pos;
+                a.dst[row * a.row_stride + b] = val;
+            }
+        } else if (vcol < a.vcols) {
+            a.dst[vcol * a.dst_stride + pos] = val;
+        }
+    };
     // linear index e -> (g, m) so that consecutive e are consecutive addresses
     auto split_in = [&](uint32_t e, uint32_t &g, uint32_t &m) {
         if (STOREM == STORE_ROWS) {
@@ -219,33 +286,81 @@ __global__ void __launch_bounds__(NT, 2) ntt_pass_kernel(NttPassArgs a)
         }
     };
 
-    // ---- load
-    for (uint32_t e = threadIdx.x; e < tile; e += NT) {
-        uint32_t g, m;
-        split_in(e, g, m);
-        uint64_t vcol, pos;
-        gpos(g, m, vcol, pos);
-        uint64_t val = 0;
-        const bool ok = (STOREM == STORE_ROWS) ? ((vcol >> a.rate) < a.cols) : (vcol < a.vcols);
-        if (ok) {
-            if (LOADM == LOAD_PLAIN) {
-                val = a.src[vcol * a.src_stride + pos];
-            } else if (LOADM == LOAD_SCALE) {
-                val = gl_mul(a.src[vcol * a.src_stride + pos], __ldg(a.tab + pos));
-            } else if (LOADM == LOAD_COSETS) {
-                val = gl_mul(a.src[(vcol >> a.rate) * a.src_stride + pos], __ldg(a.tab + ((vcol & rmask) << a.L) + pos));
-            } else {  // LOAD_EXTEND
-                val = pos < a.n_src ? a.src[vcol * a.src_stride + pos] : 0;
+    if constexpr (!DIRECT) {
+        // ---- load
+        for (uint32_t e = threadIdx.x; e < tile; e += NT) {
+            uint32_t g, m;
+            split_in(e, g, m);
+            uint64_t vcol, pos;
+            gpos(g, m, vcol, pos);
+            sm[swz((g << LOGR) + m)] = col_ok(vcol) ? load_elem(vcol, pos) : 0;
+        }
+        __syncthreads();
+        // ---- R-point DIF in sub-steps of up to 16 points
+        dif_substeps<LOGR, INV, NT, LOGR>(sm, tile, a.tw_small);
+    } else {
+        // ---- first sub-step straight from global memory: task (g, m_lo)
+        // holds members m_lo + e * Q0; lanes of a warp take consecutive
+        // positions (consecutive m_lo for row tiles, consecutive g otherwise)
+        constexpr uint32_t Q0 = 1u << (LOGR - E0);
+        constexpr bool FUSED = (STOREM == STORE_SAME) && (LAST == LOGR);  // one sub-step, global to global
+        const uint32_t tasks = tile >> E0;
+        for (uint32_t t = threadIdx.x; t < tasks; t += NT) {
+            uint32_t g, m_lo;
+            if (STOREM == STORE_ROWS) {
+                m_lo = t & (Q0 - 1);
+                g = t >> (LOGR - E0);
+            } else {
+                g = t & ((1u << log_g) - 1);
+                m_lo = t >> log_g;
+            }
+            uint64_t vcol, pos;
+            gpos(g, m_lo, vcol, pos);
+            const uint64_t step = (STOREM == STORE_ROWS) ? (uint64_t)Q0 : ((uint64_t)Q0 << s_lo);
+            const bool ok = col_ok(vcol);
+            uint64_t x[1 << E0];
+#pragma unroll
+            for (int e = 0; e < (1 << E0); e++) x[e] = ok ? load_elem(vcol, pos + e * step) : 0;
+            dif_regs<E0, INV>(x);
+            if constexpr (FUSED) {
+                // block of R consecutive members, bit-reversed in place
+#pragma unroll
+                for (int e = 0; e < (1 << E0); e++) store_elem(vcol, pos + e * step, (uint32_t)e, x[e]);
+            } else {
+                first_substep_twiddles<E0, LOGR>(x, m_lo, a.tw_small);
+                const uint32_t sb = swz((g << LOGR) + m_lo);
+#pragma unroll
+                for (int e = 0; e < (1 << E0); e++) sm[sb ^ swz_c(e * Q0)] = x[e];
             }
         }
-        sm[swz((g << LOGR) + m)] = val;
+        if constexpr (FUSED) return;
+        __syncthreads();
+        if constexpr (STOREM == STORE_ROWS) {
+            if constexpr (LOGR > 4) dif_substeps<LOGR, INV, NT, LOGR - 4>(sm, tile, a.tw_small);
+        } else {
+            dif_middle_substeps<INV, NT, LOGR - 4, LAST>(sm, tile, a.tw_small);
+            // ---- last sub-step (blocks of 2^LAST consecutive members) straight
+            // to global memory with the pass twiddle; lanes take consecutive g
+            constexpr uint32_t EL = 1u << LAST;
+            const uint32_t ltasks = tile >> LAST;
+            for (uint32_t t = threadIdx.x; t < ltasks; t += NT) {
+                const uint32_t g = t & ((1u << log_g) - 1);
+                const uint32_t mb = (t >> log_g) << LAST;
+                const uint32_t sb = swz((g << LOGR) + mb);
+                uint64_t x[EL];
+#pragma unroll
+                for (int e = 0; e < (int)EL; e++) x[e] = sm[sb ^ swz_c((uint32_t)e)];
+                dif_regs<LAST, INV>(x);
+                uint64_t vcol, pos;
+                gpos(g, mb, vcol, pos);
+#pragma unroll
+                for (int e = 0; e < (int)EL; e++) store_elem(vcol, pos + ((uint64_t)e << s_lo), mb + e, x[e]);
+            }
+            return;
+        }
     }
-    __syncthreads();
 
-    // ---- R-point DIF in sub-steps of up to 16 points
-    dif_substeps<LOGR, INV, NT, LOGR>(sm, tile, a.tw_small);
-
-    // ---- pass twiddle + store
+    // ---- pass twiddle + store through shared memory
     for (uint32_t e = threadIdx.x; e < tile; e += NT) {
         uint32_t g, m;
         if (STOREM == STORE_ROWS) {
@@ -257,21 +372,7 @@ __global__ void __launch_bounds__(NT, 2) ntt_pass_kernel(NttPassArgs a)
         }
         uint64_t vcol, pos;
         gpos(g, m, vcol, pos);
-        uint64_t val = sm[swz((g << LOGR) + m)];
-        if (S > 1) {
-            const uint64_t o = pos & (S - 1);
-            const uint64_t f = bitrev32(m, LOGR);
-            val = gl_mul(val, __ldg(a.tw_pass + o * f));
-        }
-        if (STOREM == STORE_ROWS) {
-            const uint64_t b = vcol >> a.rate;
-            if (b < a.cols) {
-                const uint64_t row = ((uint64_t)bitrev32((uint32_t)(vcol & rmask), a.rate) << a.L) + pos;
-                a.dst[row * a.row_stride + b] = val;
-            }
-        } else if (vcol < a.vcols) {
-            a.dst[vcol * a.dst_stride + pos] = val;
-        }
+        store_elem(vcol, pos, m, sm[swz((g << LOGR) + m)]);
     }
 }
 
