@@ -158,8 +158,9 @@ __device__ __forceinline__ void sqr_wide(uint64_t a, uint32_t &r0, uint32_t &r1,
         : "r"(a0), "r"(a1));
 }
 
-// r1:r0 + 2^64 (r2 + 2^32 r3)  ->  64-bit representative
-__device__ __forceinline__ uint64_t reduce_nc(uint32_t r0, uint32_t r1, uint32_t r2, uint32_t r3)
+// r1:r0 + 2^64 (r2 + 2^32 r3)  ->  64-bit representative, all on the integer
+// ALU: lo - r3 + r2 * EPS with the borrow / carry folded in.
+__device__ __forceinline__ uint64_t reduce_nc_alu(uint32_t r0, uint32_t r1, uint32_t r2, uint32_t r3)
 {
     uint32_t t0, t1, b, e0, e1, c;
     asm("{\n\t"
@@ -181,33 +182,70 @@ __device__ __forceinline__ uint64_t reduce_nc(uint32_t r0, uint32_t r1, uint32_t
         : "r"(r0), "r"(r1), "r"(r2), "r"(r3));
     return ((uint64_t)t1 << 32) | t0;
 }
+
+// The same reduction with r2 * EPS taken by one wide multiply (the multiply
+// pipe) and two fewer ALU instructions: e = r2 * EPS - r3 (< 2^64; it
+// borrows only when r2 == 0, and then e + p = 2^64 - r3 - EPS), t = lo + e,
+// one EPS when that carries.  Which form is faster depends on the permutation's
+// mix of multiplies and additions (measured per hash on B200).
+__device__ __forceinline__ uint64_t reduce_nc_imad(uint32_t r0, uint32_t r1, uint32_t r2, uint32_t r3)
+{
+    uint64_t e;
+    asm("mul.wide.u32 %0, %1, 0xffffffff;" : "=l"(e) : "r"(r2));
+    uint32_t e0 = (uint32_t)e, e1 = (uint32_t)(e >> 32), b, t0, t1;
+    asm("{\n\t"
+        "sub.cc.u32      %0, %0, %5;\n\t"
+        "subc.cc.u32     %1, %1, 0;\n\t"
+        "subc.u32        %2, 0, 0;\n\t"    // b = borrow ? 0xffffffff : 0
+        "sub.cc.u32      %0, %0, %2;\n\t"  // borrow: e -= EPS
+        "subc.u32        %1, %1, 0;\n\t"
+        "add.cc.u32      %3, %6, %0;\n\t"  // t = lo + e
+        "addc.cc.u32     %4, %7, %1;\n\t"
+        "addc.u32        %2, 0, 0;\n\t"
+        "neg.s32         %2, %2;\n\t"      // carry: t += EPS
+        "add.cc.u32      %3, %3, %2;\n\t"
+        "addc.u32        %4, %4, 0;\n\t"
+        "}"
+        : "+r"(e0), "+r"(e1), "=&r"(b), "=&r"(t0), "=&r"(t1)
+        : "r"(r3), "r"(r0), "r"(r1));
+    return ((uint64_t)t1 << 32) | t0;
+}
+
+template <bool IMAD = false>
+__device__ __forceinline__ uint64_t reduce_nc(uint32_t r0, uint32_t r1, uint32_t r2, uint32_t r3)
+{
+    return IMAD ? reduce_nc_imad(r0, r1, r2, r3) : reduce_nc_alu(r0, r1, r2, r3);
+}
 #endif
 
 // a * b for any 64-bit representatives; result any 64-bit representative.
+template <bool IMAD = false>
 ZK_HD uint64_t gl_mul_nc(uint64_t a, uint64_t b)
 {
 #ifdef __CUDA_ARCH__
     uint32_t r0, r1, r2, r3;
     mul_wide(a, b, r0, r1, r2, r3);
-    return reduce_nc(r0, r1, r2, r3);
+    return reduce_nc<IMAD>(r0, r1, r2, r3);
 #else
     unsigned __int128 x = (unsigned __int128)a * b;
     return gl_reduce128((uint64_t)x, (uint64_t)(x >> 64));
 #endif
 }
 
+template <bool IMAD = false>
 ZK_HD uint64_t gl_sqr_nc(uint64_t a)
 {
 #ifdef __CUDA_ARCH__
     uint32_t r0, r1, r2, r3;
     sqr_wide(a, r0, r1, r2, r3);
-    return reduce_nc(r0, r1, r2, r3);
+    return reduce_nc<IMAD>(r0, r1, r2, r3);
 #else
     return gl_mul_nc(a, a);
 #endif
 }
 
 // a * b + c (c any 64-bit value) reduced once.
+template <bool IMAD = false>
 ZK_HD uint64_t gl_mul_add_nc(uint64_t a, uint64_t b, uint64_t c)
 {
 #ifdef __CUDA_ARCH__
@@ -221,7 +259,7 @@ ZK_HD uint64_t gl_mul_add_nc(uint64_t a, uint64_t b, uint64_t c)
         "}"
         : "+r"(r0), "+r"(r1), "+r"(r2), "+r"(r3)
         : "r"((uint32_t)c), "r"((uint32_t)(c >> 32)));
-    return reduce_nc(r0, r1, r2, r3);
+    return reduce_nc<IMAD>(r0, r1, r2, r3);
 #else
     unsigned __int128 x = (unsigned __int128)a * b + c;
     return gl_reduce128((uint64_t)x, (uint64_t)(x >> 64));
@@ -270,10 +308,11 @@ struct WideAcc {
 #endif
     }
     // any 64-bit representative of the sum
+    template <bool IMAD = false>
     ZK_HD uint64_t reduce() const
     {
 #ifdef __CUDA_ARCH__
-        const uint64_t t = reduce_nc(r0, r1, r2, r3);
+        const uint64_t t = reduce_nc<IMAD>(r0, r1, r2, r3);
 #else
         const uint64_t t = gl_reduce128(lo, hi);
 #endif
@@ -352,12 +391,13 @@ ZK_HD uint64_t gl_sbox7(uint64_t x)
 #ifndef ZK_SBOX_SQR
 #define ZK_SBOX_SQR 0
 #endif
+template <bool IMAD = false>
 ZK_HD uint64_t gl_sbox7_nc(uint64_t x)
 {
-    uint64_t x2 = ZK_SBOX_SQR ? gl_sqr_nc(x) : gl_mul_nc(x, x);
-    uint64_t x4 = ZK_SBOX_SQR ? gl_sqr_nc(x2) : gl_mul_nc(x2, x2);
-    uint64_t x3 = gl_mul_nc(x2, x);
-    return gl_mul_nc(x3, x4);
+    uint64_t x2 = ZK_SBOX_SQR ? gl_sqr_nc<IMAD>(x) : gl_mul_nc<IMAD>(x, x);
+    uint64_t x4 = ZK_SBOX_SQR ? gl_sqr_nc<IMAD>(x2) : gl_mul_nc<IMAD>(x2, x2);
+    uint64_t x3 = gl_mul_nc<IMAD>(x2, x);
+    return gl_mul_nc<IMAD>(x3, x4);
 }
 
 ZK_HD uint32_t bitrev32(uint32_t x, unsigned bits)
