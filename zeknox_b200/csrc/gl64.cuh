@@ -249,16 +249,24 @@ template <bool IMAD = false>
 ZK_HD uint64_t gl_mul_add_nc(uint64_t a, uint64_t b, uint64_t c)
 {
 #ifdef __CUDA_ARCH__
+    // c enters the first partial product's chain (a*b + c < 2^128)
+    const uint32_t a0 = (uint32_t)a, a1 = (uint32_t)(a >> 32), b0 = (uint32_t)b, b1 = (uint32_t)(b >> 32);
     uint32_t r0, r1, r2, r3;
-    mul_wide(a, b, r0, r1, r2, r3);
     asm("{\n\t"
-        "add.cc.u32   %0, %0, %4;\n\t"
-        "addc.cc.u32  %1, %1, %5;\n\t"
-        "addc.cc.u32  %2, %2, 0;\n\t"
-        "addc.u32     %3, %3, 0;\n\t"
+        "mad.lo.cc.u32   %0, %4, %6, %8;\n\t"
+        "madc.hi.cc.u32  %1, %4, %6, %9;\n\t"
+        "addc.u32        %2, 0, 0;\n\t"
+        "mad.lo.cc.u32   %1, %5, %6, %1;\n\t"
+        "madc.hi.cc.u32  %2, %5, %6, %2;\n\t"
+        "addc.u32        %3, 0, 0;\n\t"
+        "mad.lo.cc.u32   %1, %4, %7, %1;\n\t"
+        "madc.hi.cc.u32  %2, %4, %7, %2;\n\t"
+        "addc.u32        %3, %3, 0;\n\t"
+        "mad.lo.cc.u32   %2, %5, %7, %2;\n\t"
+        "madc.hi.u32     %3, %5, %7, %3;\n\t"
         "}"
-        : "+r"(r0), "+r"(r1), "+r"(r2), "+r"(r3)
-        : "r"((uint32_t)c), "r"((uint32_t)(c >> 32)));
+        : "=&r"(r0), "=&r"(r1), "=&r"(r2), "=&r"(r3)
+        : "r"(a0), "r"(a1), "r"(b0), "r"(b1), "r"((uint32_t)c), "r"((uint32_t)(c >> 32)));
     return reduce_nc<IMAD>(r0, r1, r2, r3);
 #else
     unsigned __int128 x = (unsigned __int128)a * b + c;

@@ -103,8 +103,20 @@ struct Sum64 {
     ZK_HD void set(uint64_t x) { lo = x; c = 0; }
     ZK_HD void add(uint64_t x)
     {
+#ifdef __CUDA_ARCH__
+        uint32_t l0 = (uint32_t)lo, l1 = (uint32_t)(lo >> 32);
+        asm("{\n\t"
+            "add.cc.u32   %0, %0, %3;\n\t"
+            "addc.cc.u32  %1, %1, %4;\n\t"
+            "addc.u32     %2, %2, 0;\n\t"
+            "}"
+            : "+r"(l0), "+r"(l1), "+r"(c)
+            : "r"((uint32_t)x), "r"((uint32_t)(x >> 32)));
+        lo = ((uint64_t)l1 << 32) | l0;
+#else
         lo += x;
         c += lo < x;
+#endif
     }
     // lo + c * EPS, one wrap correction (c * EPS < 2^36)
     ZK_HD uint64_t reduce() const { return gl_add_nc(lo, ((uint64_t)c << 32) - c); }
