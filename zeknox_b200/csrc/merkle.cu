@@ -33,13 +33,13 @@ static void merkle_launch(uint64_t *digests, uint64_t *caps, const uint64_t *lea
     uint64_t blocks;
     if (lt == 64) {
         blocks = (g.n_leaves + 63) / 64;
-        merkle_leaf_kernel<H, 64><<<(unsigned)blocks, 64, 0, s>>>(leaves, digests, caps, g);
+        merkle_leaf_kernel_for<H, 64>()<<<(unsigned)blocks, 64, 0, s>>>(leaves, digests, caps, g);
     } else if (lt == 128) {
         blocks = (g.n_leaves + 127) / 128;
-        merkle_leaf_kernel<H, 128><<<(unsigned)blocks, 128, 0, s>>>(leaves, digests, caps, g);
+        merkle_leaf_kernel_for<H, 128>()<<<(unsigned)blocks, 128, 0, s>>>(leaves, digests, caps, g);
     } else {
         blocks = (g.n_leaves + LEAF_T - 1) / LEAF_T;
-        merkle_leaf_kernel<H, LEAF_T><<<(unsigned)blocks, LEAF_T, 0, s>>>(leaves, digests, caps, g);
+        merkle_leaf_kernel_for<H, LEAF_T>()<<<(unsigned)blocks, LEAF_T, 0, s>>>(leaves, digests, caps, g);
     }
     note_launch();
     const uint64_t wide = tune_get("wide_level_nodes." + std::to_string(H), lg_leaves, WIDE_LEVEL_NODES);
