@@ -505,7 +505,11 @@ extern "C" RustError zeknox_lde_rows(size_t device_id, uint64_t *rows, const uin
 }
 
 // Register-resident Goldilocks multiply throughput: every thread runs 8
-// independent chains x <- x * y of `iters` multiplies.
+// independent chains x <- x * y of `iters` multiplies, with the lazily reduced
+// product the permutations use (any 64-bit representative; IMAD selects the
+// multiply-assisted reduction).  The faster of the two reductions is the
+// ceiling of the permutations' multiply work.
+template <bool IMAD>
 __global__ void mul_rate_kernel(uint64_t *out, uint64_t seed, uint32_t iters)
 {
     uint64_t x[8], y[8];
@@ -516,12 +520,30 @@ __global__ void mul_rate_kernel(uint64_t *out, uint64_t seed, uint32_t iters)
     }
     for (uint32_t k = 0; k < iters; k++) {
 #pragma unroll
-        for (int i = 0; i < 8; i++) x[i] = zk::gl_mul(x[i], y[i]);
+        for (int i = 0; i < 8; i++) x[i] = zk::gl_mul_nc<IMAD>(x[i], y[i]);
     }
     uint64_t acc = 0;
 #pragma unroll
     for (int i = 0; i < 8; i++) acc ^= x[i];
     out[blockIdx.x * blockDim.x + threadIdx.x] = acc;
+}
+
+template <bool IMAD>
+static double mul_rate_of(zk::DeviceCtx &c, uint64_t *out, int blocks, int threads, uint32_t iters)
+{
+    cudaEvent_t a, b;
+    ZK_CUDA(cudaEventCreate(&a));
+    ZK_CUDA(cudaEventCreate(&b));
+    mul_rate_kernel<IMAD><<<blocks, threads, 0, c.stream>>>(out, 1, 64);  // warm-up
+    ZK_CUDA(cudaEventRecord(a, c.stream));
+    mul_rate_kernel<IMAD><<<blocks, threads, 0, c.stream>>>(out, 2, iters);
+    ZK_CUDA(cudaEventRecord(b, c.stream));
+    ZK_CUDA(cudaEventSynchronize(b));
+    float ms = 0;
+    ZK_CUDA(cudaEventElapsedTime(&ms, a, b));
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    return (double)blocks * threads * 8.0 * iters / (ms * 1e-3);
 }
 
 extern "C" double zeknox_measure_mul_rate(size_t device_id)
@@ -533,19 +555,9 @@ extern "C" double zeknox_measure_mul_rate(size_t device_id)
         const int blocks = c.sm_count * 8, threads = 256;
         const uint32_t iters = 4096;
         zk::DevBuf out(c, (size_t)blocks * threads);
-        cudaEvent_t a, b;
-        ZK_CUDA(cudaEventCreate(&a));
-        ZK_CUDA(cudaEventCreate(&b));
-        mul_rate_kernel<<<blocks, threads, 0, c.stream>>>(out.p, 1, 64);  // warm-up
-        ZK_CUDA(cudaEventRecord(a, c.stream));
-        mul_rate_kernel<<<blocks, threads, 0, c.stream>>>(out.p, 2, iters);
-        ZK_CUDA(cudaEventRecord(b, c.stream));
-        ZK_CUDA(cudaEventSynchronize(b));
-        float ms = 0;
-        ZK_CUDA(cudaEventElapsedTime(&ms, a, b));
-        cudaEventDestroy(a);
-        cudaEventDestroy(b);
-        rate = (double)blocks * threads * 8.0 * iters / (ms * 1e-3);
+        const double alu = mul_rate_of<false>(c, out.p, blocks, threads, iters);
+        const double imad = mul_rate_of<true>(c, out.p, blocks, threads, iters);
+        rate = alu > imad ? alu : imad;
     });
     if (e.code) free(e.message);
     return rate;

@@ -224,6 +224,42 @@ ZK_HD void p2_m4_pieces(uint32_t *x)
     x[3] = t4;
 }
 
+// p0 + 2^22 p1 + 2^44 p2 (pieces < 2^28) reduced to a 64-bit representative:
+// the sum is lo + 2^64 hi with hi < 2^9, and 2^64 = EPS (mod p).
+ZK_HD uint64_t p2_combine_pieces(uint32_t p0, uint32_t p1, uint32_t p2)
+{
+#ifdef __CUDA_ARCH__
+    uint32_t t0, t1, hi, e0, e1;
+    asm("{\n\t"
+        ".reg .u32 a, b, c, d;\n\t"
+        "shl.b32         a, %6, 22;\n\t"
+        "shr.b32         b, %6, 10;\n\t"
+        "shl.b32         c, %7, 12;\n\t"
+        "shr.b32         d, %7, 20;\n\t"
+        "add.cc.u32      %0, %5, a;\n\t"     // lo = p0 + 2^22 p1 + 2^44 p2
+        "addc.cc.u32     %1, b, c;\n\t"
+        "addc.u32        %2, d, 0;\n\t"      // hi
+        "sub.cc.u32      %3, 0, %2;\n\t"     // e = hi * EPS = 2^32 hi - hi
+        "subc.u32        %4, %2, 0;\n\t"
+        "add.cc.u32      %0, %0, %3;\n\t"    // lo + e, one EPS on carry
+        "addc.cc.u32     %1, %1, %4;\n\t"
+        "addc.u32        %2, 0, 0;\n\t"
+        "neg.s32         %2, %2;\n\t"
+        "add.cc.u32      %0, %0, %2;\n\t"
+        "addc.u32        %1, %1, 0;\n\t"
+        "}"
+        : "=&r"(t0), "=&r"(t1), "=&r"(hi), "=&r"(e0), "=&r"(e1)
+        : "r"(p0), "r"(p1), "r"(p2));
+    return ((uint64_t)t1 << 32) | t0;
+#else
+    const uint64_t l1 = (uint64_t)p0 + ((uint64_t)p1 << 22);
+    const uint64_t l2 = (uint64_t)p2 << 44;
+    const uint64_t lo = l1 + l2;
+    const uint64_t hi = (p2 >> 20) + (lo < l2);
+    return gl_reduce96_nc(lo, hi);
+#endif
+}
+
 ZK_HD void p2_external(uint64_t s[12])
 {
     uint32_t p[3][12];
@@ -245,13 +281,7 @@ ZK_HD void p2_external(uint64_t s[12])
         }
     }
 #pragma unroll
-    for (int j = 0; j < 12; j++) {
-        const uint64_t l1 = (uint64_t)p[0][j] + ((uint64_t)p[1][j] << 22);
-        const uint64_t l2 = (uint64_t)p[2][j] << 44;
-        const uint64_t lo = l1 + l2;
-        const uint64_t hi = (p[2][j] >> 20) + (lo < l2);
-        s[j] = gl_reduce96_nc(lo, hi);
-    }
+    for (int j = 0; j < 12; j++) s[j] = p2_combine_pieces(p[0][j], p[1][j], p[2][j]);
 }
 
 // Lanes hold any 64-bit representative between layers; digests are
