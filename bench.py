@@ -273,6 +273,26 @@ def run_ours(args, rank, world):
                 "achieved": lde_bytes / lde_t / 1e9, "peak": hbm, "unit": "GB/s",
                 "frac": lde_bytes / lde_t / 1e9 / hbm, "traffic": traffic, "peak_source": hbm_src + " hbm_gbs",
                 "algorithmic_bytes": lde_bytes, "ms": lde_t * 1e3}
+    # compute_transpose_rev of the workload's evaluations (column-major 256 x
+    # 2^18 -> bit-reversed leaf-major), the HBM-bound kernel of the unfused path
+    ev_cols = torch.empty(N * COLS, dtype=torch.int64, device="cuda")
+    tr_ms = []
+    for s in range(reps + 1):
+        flush.fill_(s & 0xFF)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(dstream)
+        zk.transpose_rev_batch(dev, leaves, ev_cols, LG_N + RATE, COLS)
+        b.record(dstream)
+        torch.cuda.synchronize()
+        if s:
+            tr_ms.append(a.elapsed_time(b))
+    del ev_cols
+    tr_t = statistics.median(tr_ms) * 1e-3
+    tr_bytes = 16 * N * COLS
+    roofline_transpose = {"bound": "hbm", "kernel": "transpose_rev_kernel (compute_transpose_rev, 256 x 2^18)",
+                          "achieved": tr_bytes / tr_t / 1e9, "peak": hbm, "unit": "GB/s",
+                          "frac": tr_bytes / tr_t / 1e9 / hbm, "algorithmic_bytes": tr_bytes, "ms": tr_t * 1e3,
+                          "peak_source": hbm_src + " hbm_gbs"}
     perms = N * ((COLS + 7) // 8) + (N - 1)
     mul_rate = zk.measure_mul_rate(dev)
     achieved_mul = perms * P2_MULS_PER_PERM / mk_t
@@ -294,7 +314,8 @@ def run_ours(args, rank, world):
             "metric": METRIC, "value": value, "unit": "elems/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "u64", "data": "synthetic (seeded splitmix64 field elements)",
-            "config": config_dict(), "roofline": roofline, "roofline_hash": roofline_hash, "cpu_baseline": cpu,
+            "config": config_dict(), "roofline": roofline, "roofline_hash": roofline_hash,
+            "roofline_transpose": roofline_transpose, "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": "elems/s", "h2d_bytes_per_step": COLS * n * 8,
                     "d2h_bytes_per_step": n_cap * 32},
             "gpu_launches": launches, "clocks": clocks,

@@ -1,0 +1,92 @@
+"""The headline commit (256 columns x 2^15, rate 3, Poseidon2, cap height 4)
+through the reference's own CUDA library and through this one on the same
+GPU: the caps must be identical bit for bit (a full-size parity check against
+the reference itself), and this library's fused commit must not be slower
+than the reference's compute_batched_lde -> compute_transpose_rev ->
+fill_digests_buf_linear_gpu_with_gpu_ptr sequence.
+
+The reference library is oracle/_ref/libzeknox_ref_gpu.so, compiled from the
+reference sources for sm_100a by `make -C oracle ref_gpu`; the test is skipped
+where it has not been built."""
+import ctypes
+import os
+import statistics
+
+import pytest
+import torch
+
+import zeknox_b200 as zk
+
+pytestmark = pytest.mark.gpu
+
+REF_GPU = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "oracle", "_ref",
+                       "libzeknox_ref_gpu.so")
+
+
+def ref_lib():
+    R = ctypes.CDLL(REF_GPU)
+    R.init_twiddle_factors.restype = zk.RustError
+    R.init_twiddle_factors.argtypes = [ctypes.c_size_t, ctypes.c_size_t]
+    R.init_coset.restype = zk.RustError
+    R.init_coset.argtypes = [ctypes.c_size_t, ctypes.c_size_t, ctypes.c_uint64]
+    R.compute_batched_lde.restype = zk.RustError
+    R.compute_batched_lde.argtypes = [ctypes.c_size_t, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint32, ctypes.c_int,
+                                      zk.NTTConfig]
+    R.compute_transpose_rev.restype = zk.RustError
+    R.compute_transpose_rev.argtypes = [ctypes.c_size_t, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint32,
+                                        zk.TransposeConfig]
+    R.fill_digests_buf_linear_gpu_with_gpu_ptr.restype = None
+    R.fill_digests_buf_linear_gpu_with_gpu_ptr.argtypes = [ctypes.c_void_p] * 3 + [ctypes.c_uint64] * 7
+    return R
+
+
+def median_ms(fn, flush, reps=3):
+    fn()
+    torch.cuda.synchronize()
+    ts = []
+    for _ in range(reps):
+        flush.fill_(1)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        fn()
+        b.record()
+        torch.cuda.synchronize()
+        ts.append(a.elapsed_time(b))
+    return statistics.median(ts)
+
+
+@pytest.mark.skipif(not os.path.exists(REF_GPU), reason="reference CUDA library not built (make -C oracle ref_gpu)")
+def test_headline_commit_matches_and_beats_reference_cuda_path():
+    lg, rate, cols, cap, h = 15, 3, 256, 4, 3
+    n, N = 1 << lg, 1 << (lg + rate)
+    R = ref_lib()
+    assert R.init_twiddle_factors(0, lg + rate).code == 0
+    assert R.init_coset(0, lg + rate, 7).code == 0
+    g = torch.Generator(device="cuda").manual_seed(11)
+    inp = torch.randint(0, 1 << 62, (cols * n,), dtype=torch.int64, device="cuda", generator=g)
+    ev = torch.empty(cols * N, dtype=torch.int64, device="cuda")
+    leaves = torch.empty(cols * N, dtype=torch.int64, device="cuda")
+    n_dig, n_cap = zk.merkle_sizes(N, cap)
+    dig = torch.empty(n_dig * 4, dtype=torch.int64, device="cuda")
+    caps = torch.empty(n_cap * 4, dtype=torch.int64, device="cuda")
+    flush = torch.empty(32 << 20, dtype=torch.int64, device="cuda")
+    cfg = zk.ntt_config(cols, rate, True, True, True)
+    tcfg = zk.TransposeConfig()
+    tcfg.batches, tcfg.are_inputs_on_device, tcfg.are_outputs_on_device = cols, True, True
+
+    def reference():
+        assert R.compute_batched_lde(0, ev.data_ptr(), inp.data_ptr(), lg, 0, cfg).code == 0
+        assert R.compute_transpose_rev(0, leaves.data_ptr(), ev.data_ptr(), lg + rate, tcfg).code == 0
+        R.fill_digests_buf_linear_gpu_with_gpu_ptr(dig.data_ptr(), caps.data_ptr(), leaves.data_ptr(), n_dig, n_cap,
+                                                   N, cols, cap, h, 0)
+
+    t_ref = median_ms(reference, flush)
+    ref_caps, ref_dig = caps.clone(), dig.clone()
+    job = zk.commit_job(lg, rate, cols, cap, h, inp, leaves, dig, caps)
+    caps.zero_()
+    dig.zero_()
+    t_ours = median_ms(lambda: zk.commit(0, job), flush)
+    assert torch.equal(caps, ref_caps)
+    assert torch.equal(dig, ref_dig)
+    print("headline commit: reference CUDA path %.2f ms, this library %.2f ms (%.2fx)" % (t_ref, t_ours, t_ref / t_ours))
+    assert t_ours <= t_ref
