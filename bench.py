@@ -280,9 +280,9 @@ def run_ours(args, rank, world):
     for s in range(reps + 1):
         flush.fill_(s & 0xFF)
         a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        a.record(dstream)
-        zk.transpose_rev_batch(dev, leaves, ev_cols, LG_N + RATE, COLS)
-        b.record(dstream)
+        a.record(stream)
+        zk.transpose_rev(dev, leaves, ev_cols, LG_N + RATE, COLS, stream=sptr)
+        b.record(stream)
         torch.cuda.synchronize()
         if s:
             tr_ms.append(a.elapsed_time(b))

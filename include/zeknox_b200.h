@@ -78,6 +78,13 @@ RustError zeknox_merkle_batch(size_t device_id, const zk_merkle_job *jobs, uint3
 RustError zeknox_lde_rows(size_t device_id, uint64_t *rows, const uint64_t *coeffs, uint32_t lg_n, uint32_t rate_bits,
                           uint32_t cols, uint64_t coset_gen, void *stream);
 
+/* compute_transpose_rev (native/ntt/ntt.cu:182-226) of device buffers,
+ * out[rev(i) * cols + b] = in[b * 2^lg_n + i], queued on `stream` (a
+ * cudaStream_t; NULL: the device's stream, and the call waits).  No reference
+ * counterpart: the reference call is synchronous. */
+RustError zeknox_transpose_rev(size_t device_id, uint64_t *output, const uint64_t *input, uint32_t lg_n,
+                               uint32_t cols, void *stream);
+
 /* zeknox_lde_rows for callers that cannot allocate device memory (code being
  * captured into a CUDA graph, code whose device memory is owned by another
  * allocator or arena).  No counterpart in the reference.  It never allocates:

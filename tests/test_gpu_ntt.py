@@ -79,7 +79,7 @@ def test_custom_coset_generator():
         zk.init_coset(0, 20, 7)
 
 
-@pytest.mark.parametrize("lg,b", [(0, 3), (1, 1), (5, 3), (10, 33), (12, 256), (17, 7), (20, 2)])
+@pytest.mark.parametrize("lg,b", [(0, 3), (1, 1), (5, 3), (6, 31), (10, 33), (12, 256), (17, 7), (20, 2)])
 def test_transpose_rev(lg, b):
     x = O.field_data(lg + b, b << lg)
     out = torch.zeros(b << lg, dtype=torch.int64, device="cuda")
@@ -88,6 +88,14 @@ def test_transpose_rev(lg, b):
     out2 = torch.zeros(b << lg, dtype=torch.int64, device="cuda")
     zk.transpose_rev_batch(0, out2, to_dev(x), lg, b, naive=True)
     assert torch.equal(out, out2)
+    # the stream-ordered extension entry point
+    s = torch.cuda.Stream()
+    out3 = torch.zeros(b << lg, dtype=torch.int64, device="cuda")
+    src = to_dev(x)
+    torch.cuda.synchronize()
+    zk.transpose_rev(0, out3, src, lg, b, stream=s.cuda_stream)
+    s.synchronize()
+    assert torch.equal(out, out3)
 
 
 def test_argument_errors():

@@ -35,7 +35,7 @@ EXT_SYMBOLS = ["zeknox_last_error", "zeknox_commit", "zeknox_commit_batch", "zek
                "zeknox_lde_rows", "zeknox_launch_count", "zeknox_measure_mul_rate", "zeknox_merkle_batch",
                "zeknox_lde_rows_noalloc", "zeknox_server_create", "zeknox_server_submit", "zeknox_server_wait",
                "zeknox_server_release", "zeknox_server_stats", "zeknox_server_destroy", "zeknox_tune_set",
-               "zeknox_tune_get", "zeknox_tune_clear", "zeknox_tune_load"]
+               "zeknox_tune_get", "zeknox_tune_clear", "zeknox_tune_load", "zeknox_transpose_rev"]
 
 # Tuning table measured on B200 by ``python -m zeknox_b200.autotune``; loaded
 # by load() unless ZEKNOX_TUNE_FILE names another table ("" or "none": no table).
@@ -190,6 +190,8 @@ def load():
     L.zeknox_server_destroy.argtypes = [vp]
     L.zeknox_merkle_batch.restype = RustError
     L.zeknox_merkle_batch.argtypes = [sz, ctypes.POINTER(MerkleJob), u32]
+    L.zeknox_transpose_rev.restype = RustError
+    L.zeknox_transpose_rev.argtypes = [sz, vp, vp, u32, u32, vp]
     L.zeknox_tune_set.restype = RustError
     L.zeknox_tune_set.argtypes = [ctypes.c_char_p, u32, u64]
     L.zeknox_tune_get.restype = u64
@@ -392,6 +394,14 @@ def lde_rows_noalloc(device_id, rows, coeffs, lg_n, rate_bits, cols, coset_gen=7
     _check(load().zeknox_lde_rows_noalloc(device_id, _ptr(rows), _ptr(coeffs), lg_n, rate_bits, cols, coset_gen,
                                           ctypes.c_void_p(stream) if stream else None))
     return rows
+
+
+def transpose_rev(device_id, output, inp, lg_n, cols, stream=None):
+    """zeknox_transpose_rev: bit-reversed transpose of device columns, queued on
+    `stream` (an int cudaStream_t handle; None waits on the device's stream)."""
+    _check(load().zeknox_transpose_rev(device_id, _ptr(output), _ptr(inp), lg_n, cols,
+                                       ctypes.c_void_p(stream) if stream else None))
+    return output
 
 
 def launch_count():

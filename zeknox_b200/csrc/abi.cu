@@ -289,6 +289,29 @@ extern "C" RustError compute_naive_transpose_rev(size_t device_id, void *output,
     return transpose_impl(device_id, output, input, lg_n, cfg);
 }
 
+// compute_transpose_rev of device buffers queued on the caller's stream
+// (NULL: the device's stream, waited for), for pipelines that overlap it.
+extern "C" RustError zeknox_transpose_rev(size_t device_id, uint64_t *output, const uint64_t *input, uint32_t lg_n,
+                                          uint32_t cols, void *stream)
+{
+    return guarded([&] {
+        if (lg_n > 32) throw zk::arg_failure("lg_n above 32");
+        if (cols && (!input || !output)) throw zk::arg_failure("null buffer");
+        zk::DeviceCtx &c = zk::device(device_id);
+        std::lock_guard<std::recursive_mutex> lk(c.mu);
+        cudaStream_t keep = c.stream;
+        if (stream) c.stream = (cudaStream_t)stream;
+        try {
+            zk::transpose_rev_device(c, output, input, lg_n, cols);
+        } catch (...) {
+            c.stream = keep;
+            throw;
+        }
+        c.stream = keep;
+        if (!stream) c.sync();
+    });
+}
+
 // ------------------------------------------------------------------- Merkle
 
 extern "C" void fill_digests_buf_linear_gpu_with_gpu_ptr(void *digests_buf_gpu_ptr, void *cap_buf_gpu_ptr,

@@ -437,7 +437,7 @@ void transpose_rev_device(DeviceCtx &c, uint64_t *out, const uint64_t *in, uint3
 {
     const uint64_t n = 1ULL << lg;
     if (cols == 0) return;
-    dim3 grid((unsigned)((n + 31) / 32), (unsigned)((cols + 31) / 32));
+    dim3 grid((unsigned)((n + 63) / 64), (unsigned)((cols + 31) / 32));
     if (grid.y > 65535) throw arg_failure("too many columns for transpose");
     transpose_rev_kernel<<<grid, 256, 0, c.stream>>>(in, out, lg, cols);
     note_launch();
