@@ -78,6 +78,19 @@ RustError zeknox_merkle_batch(size_t device_id, const zk_merkle_job *jobs, uint3
 RustError zeknox_lde_rows(size_t device_id, uint64_t *rows, const uint64_t *coeffs, uint32_t lg_n, uint32_t rate_bits,
                           uint32_t cols, uint64_t coset_gen, void *stream);
 
+/* zeknox_lde_rows with the leaf rows spread over n_dst destination buffers
+ * (a power of two): row r of the 2^(lg_n + rate_bits) rows goes to
+ * dst_ptrs[r / R] (R = rows / n_dst) at row r mod R, columns
+ * [col_offset, col_offset + cols) of rows of row_stride words.  The
+ * destinations may be other GPUs' memory mapped for peer access: the rows then
+ * cross NVLink as stores from the row-writing kernel (the LDE and the row
+ * exchange of a multi-GPU commit in one pass).  Queued on `stream` (NULL: the
+ * device's stream, and the call waits).  No reference counterpart (zeknox's
+ * multi-GPU path copies whole columns between GPUs, native/ntt/ntt.cu:315-471). */
+RustError zeknox_lde_rows_scatter(size_t device_id, uint64_t *const *dst_ptrs, uint32_t n_dst, const uint64_t *coeffs,
+                                  uint32_t lg_n, uint32_t rate_bits, uint32_t cols, uint32_t col_offset,
+                                  uint32_t row_stride, uint64_t coset_gen, void *stream);
+
 /* compute_transpose_rev (native/ntt/ntt.cu:182-226) of device buffers,
  * out[rev(i) * cols + b] = in[b * 2^lg_n + i], queued on `stream` (a
  * cudaStream_t; NULL: the device's stream, and the call waits).  No reference

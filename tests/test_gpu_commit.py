@@ -170,3 +170,34 @@ def test_commit_from_host_memory(pinned):
     assert np.array_equal(to_np(leaves), rows)
     assert np.array_equal(to_np(caps).reshape(-1, 4), cp)
     assert np.array_equal(to_np(dig).reshape(-1, 4)[:n_dig], d)
+
+
+@pytest.mark.parametrize("lg,rate,cols,n_dst,n_src", [(10, 2, 24, 4, 3), (15, 3, 40, 2, 2), (6, 1, 5, 1, 2),
+                                                      (12, 3, 17, 8, 4)])
+def test_lde_rows_scatter_assembles_row_shards(lg, rate, cols, n_dst, n_src):
+    """Several column shards (the sources of a multi-GPU commit) each scatter
+    their LDE rows into n_dst row-shard buffers (the destinations, emulated as
+    buffers of this GPU); every destination must end up holding its block of
+    whole leaf rows, exactly the single-call LDE's."""
+    n, N = 1 << lg, 1 << (lg + rate)
+    c = O.field_data(lg * 3 + cols, cols * n)
+    rows = O.lde_rows(c, lg, rate, cols).reshape(N, cols)
+    per = N // n_dst
+    dst = [torch.zeros(per * cols, dtype=torch.int64, device="cuda") for _ in range(n_dst)]
+    base, rem = divmod(cols, n_src)
+    c0 = 0
+    for s in range(n_src):
+        k = base + (1 if s < rem else 0)
+        if k:
+            zk.lde_rows_scatter(0, dst, to_dev(c[c0 * n:(c0 + k) * n]), lg, rate, k, c0, cols)
+        c0 += k
+    for d in range(n_dst):
+        assert np.array_equal(to_np(dst[d]).reshape(per, cols), rows[d * per:(d + 1) * per])
+
+
+def test_lde_rows_scatter_argument_errors():
+    t = torch.zeros(64, dtype=torch.int64, device="cuda")
+    with pytest.raises(zk.ZeknoxError):
+        zk.lde_rows_scatter(0, [t, t, t], t, 3, 1, 1, 0, 1)  # 3 destinations: not a power of two
+    with pytest.raises(zk.ZeknoxError):
+        zk.lde_rows_scatter(0, [t, t], t, 3, 1, 2, 1, 2)  # columns beyond the rows

@@ -35,7 +35,8 @@ EXT_SYMBOLS = ["zeknox_last_error", "zeknox_commit", "zeknox_commit_batch", "zek
                "zeknox_lde_rows", "zeknox_launch_count", "zeknox_measure_mul_rate", "zeknox_merkle_batch",
                "zeknox_lde_rows_noalloc", "zeknox_server_create", "zeknox_server_submit", "zeknox_server_wait",
                "zeknox_server_release", "zeknox_server_stats", "zeknox_server_destroy", "zeknox_tune_set",
-               "zeknox_tune_get", "zeknox_tune_clear", "zeknox_tune_load", "zeknox_transpose_rev"]
+               "zeknox_tune_get", "zeknox_tune_clear", "zeknox_tune_load", "zeknox_transpose_rev",
+               "zeknox_lde_rows_scatter"]
 
 # Tuning table measured on B200 by ``python -m zeknox_b200.autotune``; loaded
 # by load() unless ZEKNOX_TUNE_FILE names another table ("" or "none": no table).
@@ -190,6 +191,8 @@ def load():
     L.zeknox_server_destroy.argtypes = [vp]
     L.zeknox_merkle_batch.restype = RustError
     L.zeknox_merkle_batch.argtypes = [sz, ctypes.POINTER(MerkleJob), u32]
+    L.zeknox_lde_rows_scatter.restype = RustError
+    L.zeknox_lde_rows_scatter.argtypes = [sz, ctypes.POINTER(ctypes.c_void_p), u32, vp, u32, u32, u32, u32, u32, u64, vp]
     L.zeknox_transpose_rev.restype = RustError
     L.zeknox_transpose_rev.argtypes = [sz, vp, vp, u32, u32, vp]
     L.zeknox_tune_set.restype = RustError
@@ -394,6 +397,17 @@ def lde_rows_noalloc(device_id, rows, coeffs, lg_n, rate_bits, cols, coset_gen=7
     _check(load().zeknox_lde_rows_noalloc(device_id, _ptr(rows), _ptr(coeffs), lg_n, rate_bits, cols, coset_gen,
                                           ctypes.c_void_p(stream) if stream else None))
     return rows
+
+
+def lde_rows_scatter(device_id, dst, coeffs, lg_n, rate_bits, cols, col_offset, row_stride, coset_gen=7, stream=None):
+    """zeknox_lde_rows_scatter: the fused LDE of `cols` columns with its leaf
+    rows spread over the destination buffers `dst` (tensors or device
+    addresses; a power of two of them, rows split evenly), written at columns
+    [col_offset, col_offset + cols) of rows of `row_stride` words."""
+    ptrs = [d if isinstance(d, int) else d.data_ptr() for d in dst]
+    arr = (ctypes.c_void_p * len(ptrs))(*ptrs)
+    _check(load().zeknox_lde_rows_scatter(device_id, arr, len(ptrs), _ptr(coeffs), lg_n, rate_bits, cols, col_offset,
+                                          row_stride, coset_gen, ctypes.c_void_p(stream) if stream else None))
 
 
 def transpose_rev(device_id, output, inp, lg_n, cols, stream=None):

@@ -289,6 +289,44 @@ extern "C" RustError compute_naive_transpose_rev(size_t device_id, void *output,
     return transpose_impl(device_id, output, input, lg_n, cfg);
 }
 
+// The fused LDE with its leaf rows scattered over n_dst destination buffers
+// (other GPUs' row shards, mapped for peer access): the LDE and the row
+// exchange of a multi-GPU commit in one pass, the rows crossing NVLink as
+// P2P stores straight from the row-writing kernel.
+extern "C" RustError zeknox_lde_rows_scatter(size_t device_id, uint64_t *const *dst_ptrs, uint32_t n_dst,
+                                             const uint64_t *coeffs, uint32_t lg_n, uint32_t rate_bits, uint32_t cols,
+                                             uint32_t col_offset, uint32_t row_stride, uint64_t coset_gen, void *stream)
+{
+    return guarded([&] {
+        if (lg_n == 0 || rate_bits == 0 || cols == 0) throw zk::arg_failure("lg_n, rate_bits and cols must be >= 1");
+        if (lg_n + rate_bits > 32) throw zk::arg_failure("extended size above 2^32");
+        if (!dst_ptrs || !coeffs) throw zk::arg_failure("null buffer");
+        const uint32_t lg_dst = zk::ilog2_exact(n_dst);
+        if (lg_dst == ~0u || lg_dst > lg_n + rate_bits)
+            throw zk::arg_failure("n_dst must be a power of two no larger than the row count");
+        if ((uint64_t)col_offset + cols > row_stride) throw zk::arg_failure("columns beyond the destination rows");
+        for (uint32_t d = 0; d < n_dst; d++)
+            if (!dst_ptrs[d]) throw zk::arg_failure("null destination buffer");
+        zk::DeviceCtx &c = zk::device(device_id);
+        std::lock_guard<std::recursive_mutex> lk(c.mu);
+        cudaStream_t keep = c.stream;
+        if (stream) c.stream = (cudaStream_t)stream;
+        try {
+            zk::DevBuf tab(c, n_dst);
+            ZK_CUDA(cudaMemcpyAsync(tab.p, dst_ptrs, n_dst * sizeof(uint64_t *), cudaMemcpyHostToDevice, c.stream));
+            zk::RowScatter sc{(uint64_t *const *)tab.p, lg_n + rate_bits - lg_dst, col_offset, row_stride};
+            zk::lde_rows_device(c, nullptr, coeffs, lg_n, rate_bits, cols, coset_gen ? coset_gen : ZK_GENERATOR, nullptr,
+                                nullptr, &sc);
+            // the pointer table is returned to the pool on the stream, after the kernels that read it
+        } catch (...) {
+            c.stream = keep;
+            throw;
+        }
+        c.stream = keep;
+        if (!stream) c.sync();
+    });
+}
+
 // compute_transpose_rev of device buffers queued on the caller's stream
 // (NULL: the device's stream, waited for), for pipelines that overlap it.
 extern "C" RustError zeknox_transpose_rev(size_t device_id, uint64_t *output, const uint64_t *input, uint32_t lg_n,

@@ -126,6 +126,8 @@ struct DifJob {
     bool rows;
     bool inverse;
     uint64_t *scratch;
+    const RowScatter *scatter;  // row output over several buffers (null: dst)
+    uint64_t col0;              // first column of this chunk (scattered row output)
 };
 
 static void run_dif(DeviceCtx &c, const DifJob &j)
@@ -157,6 +159,11 @@ static void run_dif(DeviceCtx &c, const DifJob &j)
         if (store_rows) {
             a.dst = j.dst;
             a.dst_stride = 0;
+            if (j.scatter) {
+                a.dst_tab = j.scatter->dst_tab;
+                a.log_rows_per_dst = j.scatter->log_rows_per_dst;
+                a.col_offset = j.scatter->col_offset + j.col0;
+            }
         } else {
             a.dst = j.rows ? j.scratch : j.dst;
             a.dst_stride = j.rows ? n : j.dst_stride;
@@ -369,7 +376,7 @@ uint64_t lde_rows_scratch_elems(uint32_t lg_n, uint32_t rate, uint64_t cols)
 }
 
 void lde_rows_device(DeviceCtx &c, uint64_t *rows, const uint64_t *coeffs, uint32_t lg_n, uint32_t rate, uint64_t cols,
-                     uint64_t coset_gen, uint64_t *scratch, const uint64_t *host_coeffs)
+                     uint64_t coset_gen, uint64_t *scratch, const uint64_t *host_coeffs, const RowScatter *scatter)
 {
     const uint64_t n = 1ULL << lg_n;
     if (cols == 0) return;
@@ -406,8 +413,10 @@ void lde_rows_device(DeviceCtx &c, uint64_t *rows, const uint64_t *coeffs, uint3
         j.src_stride = n;
         j.load = LOAD_COSETS;
         j.tab = tab;
-        j.dst = rows + c0;
-        j.row_stride = cols;
+        j.dst = scatter ? nullptr : rows + c0;
+        j.row_stride = scatter ? scatter->row_stride : cols;
+        j.scatter = scatter;
+        j.col0 = c0;
         j.vcols = cc << rate;
         j.L = lg_n;
         j.rate = rate;

@@ -100,6 +100,12 @@ struct NttPassArgs {
     uint32_t rate;            // LOAD_COSETS / STORE_ROWS: log2 cosets per column
     uint32_t cols;            // STORE_ROWS: real columns in this launch
     uint64_t row_stride;      // STORE_ROWS: words per output row (>= cols; dst points at the first column)
+    // STORE_ROWS scattered over destination buffers (null: one buffer, dst):
+    // row r goes to dst_tab[r >> log_rows_per_dst] at row r & (2^log_rows_per_dst - 1),
+    // column col_offset + b -- the buffers may be other GPUs' memory (P2P stores)
+    uint64_t *const *dst_tab;
+    uint32_t log_rows_per_dst;
+    uint64_t col_offset;
 };
 
 // Sub-step of the in-CTA R-point DIF: every task owns E elements spaced Q apart
@@ -264,7 +270,12 @@ __global__ void __launch_bounds__(NT, 2) ntt_pass_kernel(NttPassArgs a)
             const uint64_t b = vcol >> a.rate;
             if (b < a.cols) {
                 const uint64_t row = ((uint64_t)bitrev32((uint32_t)(vcol & rmask), a.rate) << a.L) + pos;
-                a.dst[row * a.row_stride + b] = val;
+                if (a.dst_tab) {
+                    uint64_t *d = a.dst_tab[row >> a.log_rows_per_dst];
+                    d[(row & ((1ULL << a.log_rows_per_dst) - 1)) * a.row_stride + a.col_offset + b] = val;
+                } else {
+                    a.dst[row * a.row_stride + b] = val;
+                }
             }
         } else if (vcol < a.vcols) {
             a.dst[vcol * a.dst_stride + pos] = val;

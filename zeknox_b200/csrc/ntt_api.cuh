@@ -25,8 +25,20 @@ void lde_batch_device(DeviceCtx &c, uint64_t *out, const uint64_t *in, uint32_t 
 // memory, staged chunk by chunk into `coeffs` (a device buffer of cols * 2^lg_n
 // words) on the context's copy stream, overlapping the transfer with the
 // transform of the previous chunk.
+// Row output spread over several buffers: row r of the LDE goes to
+// dst_tab[r >> log_rows_per_dst] (a device array of base pointers, which may
+// be other GPUs' memory mapped for peer access) at row r mod 2^log_rows_per_dst,
+// columns [col_offset, col_offset + cols) of rows that are row_stride words long.
+struct RowScatter {
+    uint64_t *const *dst_tab;
+    uint32_t log_rows_per_dst;
+    uint64_t col_offset;
+    uint64_t row_stride;
+};
+
 void lde_rows_device(DeviceCtx &c, uint64_t *rows, const uint64_t *coeffs, uint32_t lg_n, uint32_t rate, uint64_t cols,
-                     uint64_t coset_gen, uint64_t *scratch, const uint64_t *host_coeffs = nullptr);
+                     uint64_t coset_gen, uint64_t *scratch, const uint64_t *host_coeffs = nullptr,
+                     const RowScatter *scatter = nullptr);
 uint64_t lde_rows_scratch_elems(uint32_t lg_n, uint32_t rate, uint64_t cols);
 uint32_t lde_rows_chunk_cols(uint32_t lg_n, uint32_t rate, uint64_t cols);
 
