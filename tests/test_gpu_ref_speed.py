@@ -90,3 +90,36 @@ def test_headline_commit_matches_and_beats_reference_cuda_path():
     assert torch.equal(dig, ref_dig)
     print("headline commit: reference CUDA path %.2f ms, this library %.2f ms (%.2fx)" % (t_ref, t_ours, t_ref / t_ours))
     assert t_ours <= t_ref
+
+
+@pytest.mark.skipif(not os.path.exists(REF_GPU), reason="reference CUDA library not built (make -C oracle ref_gpu)")
+@pytest.mark.parametrize("h,n_leaves,leaf_size,cap", [(3, 1 << 20, 135, 4), (4, 1 << 20, 135, 4), (1, 1 << 20, 135, 4),
+                                                     (0, 1 << 20, 135, 4), (0, 8192, 84, 0)])
+def test_forest_matches_and_beats_reference_cuda_path(h, n_leaves, leaf_size, cap):
+    """The alternative-hash forests (2^20 leaves x 135, cap height 4) and the
+    8192 x 84 Poseidon tree through the reference's
+    fill_digests_buf_linear_gpu_with_gpu_ptr and this library's: identical
+    digests and caps, and this library no slower."""
+    R = ref_lib()
+    g = torch.Generator(device="cuda").manual_seed(100 + h)
+    leaves = torch.randint(0, 1 << 62, (n_leaves * leaf_size,), dtype=torch.int64, device="cuda", generator=g)
+    n_dig, n_cap = zk.merkle_sizes(n_leaves, cap)
+    dig = torch.zeros(max(n_dig, 1) * 4, dtype=torch.int64, device="cuda")
+    caps = torch.zeros(n_cap * 4, dtype=torch.int64, device="cuda")
+    flush = torch.empty(32 << 20, dtype=torch.int64, device="cuda")
+    L = zk.load()
+
+    def run(lib):
+        return lambda: lib.fill_digests_buf_linear_gpu_with_gpu_ptr(zk._ptr(dig), zk._ptr(caps), zk._ptr(leaves), n_dig,
+                                                                    n_cap, n_leaves, leaf_size, cap, h, 0)
+
+    t_ref = median_ms(run(R), flush)
+    ref_dig, ref_caps = dig.clone(), caps.clone()
+    dig.zero_()
+    caps.zero_()
+    t_ours = median_ms(run(L), flush)
+    assert torch.equal(caps, ref_caps)
+    assert torch.equal(dig, ref_dig)
+    print("forest hash %d, %d x %d: reference %.2f ms, this library %.2f ms (%.2fx)" %
+          (h, n_leaves, leaf_size, t_ref, t_ours, t_ref / t_ours))
+    assert t_ours <= t_ref
