@@ -94,7 +94,7 @@ def test_headline_commit_matches_and_beats_reference_cuda_path():
 
 @pytest.mark.skipif(not os.path.exists(REF_GPU), reason="reference CUDA library not built (make -C oracle ref_gpu)")
 @pytest.mark.parametrize("h,n_leaves,leaf_size,cap", [(3, 1 << 20, 135, 4), (4, 1 << 20, 135, 4), (1, 1 << 20, 135, 4),
-                                                     (0, 1 << 20, 135, 4), (0, 8192, 84, 0)])
+                                                     (0, 1 << 20, 135, 4), (0, 8192, 84, 0), (2, 1 << 14, 135, 2)])
 def test_forest_matches_and_beats_reference_cuda_path(h, n_leaves, leaf_size, cap):
     """The alternative-hash forests (2^20 leaves x 135, cap height 4) and the
     8192 x 84 Poseidon tree through the reference's
