@@ -1,9 +1,12 @@
 // merkle.cu -- host driver of the Merkle forest builder.
 //
 // Follows native/merkle/merkle.cu:166-280 of zeknox for the layout and the
-// special cases (caps == leaves; subtrees of 1 or 2 leaves); launches a leaf
-// kernel that also folds the lower levels, then (for subtrees larger than a
-// CTA) a tail kernel per subtree -- 1 or 2 launches instead of one per level.
+// special cases (caps == leaves; subtrees of 1 or 2 leaves).  Launches: the
+// leaf kernel; one node-parallel level kernel per level while a level still
+// has >= wide_level_nodes nodes; the fold kernel (the next 8 levels inside
+// CTAs, and the caps when whole subtrees fit); for subtrees still above 1024
+// nodes, level kernels, then one tail CTA per subtree -- 2 to 6 launches where
+// the reference launches one per level.
 #include <cstdio>
 #include <string>
 

@@ -10,10 +10,12 @@
 // Kernel structure (B200-first instead of one launch per level):
 //   * leaf kernel: one thread per leaf runs the sponge with the state in
 //     registers (nothing else, so no warp idles on a barrier);
-//   * fold kernel: each CTA folds T consecutive leaf digests log2(T) levels up
-//     in shared memory, writing every node, and the caps of subtrees that fit;
+//   * level kernel: one thread per node of one level, for the wide levels
+//     just above the leaves (and for levels a tail CTA cannot hold);
+//   * fold kernel: each CTA folds T consecutive nodes log2(T) levels up in
+//     shared memory, writing every node, and the caps of subtrees that fit;
 //   * tail kernel: one CTA per subtree folds the remaining levels in shared
-//     memory and writes the cap (only when L > T).
+//     memory and writes the cap.
 #pragma once
 #include <stdint.h>
 
