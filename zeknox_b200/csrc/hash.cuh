@@ -1,10 +1,12 @@
 // hash.cuh -- width-12 Goldilocks permutations and the Plonky2 sponge.
 //
-// Replaces zeknox's native/poseidon (Plonky2 Poseidon), native/poseidon2,
-// native/monolith and native/keccak hashers.  State is 12 uint64_t in
-// registers; every loop is fully unrolled so round constants become
-// constant-bank operands (device) or immediates.  The same code runs on the
-// host (for the exported CPU Merkle builder) and on the device.
+// Replaces zeknox's native/poseidon (Plonky2 Poseidon and Poseidon-BN128),
+// native/poseidon2, native/monolith and native/keccak hashers.  State is 12
+// uint64_t in registers; the work inside a round is unrolled (lane indices are
+// constants), the rounds themselves are rolled loops that read their round
+// constants from the constant bank, so a permutation's code fits the
+// instruction cache.  The same code runs on the host (for the exported CPU
+// Merkle builder) and on the device.
 #pragma once
 #include <stdint.h>
 #include <string.h>
