@@ -184,30 +184,31 @@ __device__ __forceinline__ uint64_t reduce_nc_alu(uint32_t r0, uint32_t r1, uint
 }
 
 // The same reduction with r2 * EPS taken by one wide multiply (the multiply
-// pipe) and two fewer ALU instructions: e = r2 * EPS - r3 (< 2^64; it
-// borrows only when r2 == 0, and then e + p = 2^64 - r3 - EPS), t = lo + e,
-// one EPS when that carries.  Which form is faster depends on the permutation's
-// mix of multiplies and additions (measured per hash on B200).
+// pipe) and three fewer ALU instructions: (top:t) = (r1:r0) + r2 * EPS - r3
+// with a signed top limb in {-1, 0, 1}, then one correction t + top * EPS
+// (2^64 = EPS mod p; +EPS cannot wrap again because t <= 2^64 - 2^33 when
+// top = 1, and t >= 2^64 - 2^32 when top = -1).  Which form is faster depends
+// on the permutation's mix of multiplies and additions (measured per hash on
+// B200).
 __device__ __forceinline__ uint64_t reduce_nc_imad(uint32_t r0, uint32_t r1, uint32_t r2, uint32_t r3)
 {
     uint64_t e;
     asm("mul.wide.u32 %0, %1, 0xffffffff;" : "=l"(e) : "r"(r2));
-    uint32_t e0 = (uint32_t)e, e1 = (uint32_t)(e >> 32), b, t0, t1;
+    uint32_t t0, t1, top, cl, ch;
     asm("{\n\t"
-        "sub.cc.u32      %0, %0, %5;\n\t"
-        "subc.cc.u32     %1, %1, 0;\n\t"
-        "subc.u32        %2, 0, 0;\n\t"    // b = borrow ? 0xffffffff : 0
-        "sub.cc.u32      %0, %0, %2;\n\t"  // borrow: e -= EPS
-        "subc.u32        %1, %1, 0;\n\t"
-        "add.cc.u32      %3, %6, %0;\n\t"  // t = lo + e
-        "addc.cc.u32     %4, %7, %1;\n\t"
+        "add.cc.u32      %0, %5, %7;\n\t"   // t = lo + r2 * EPS
+        "addc.cc.u32     %1, %6, %8;\n\t"
         "addc.u32        %2, 0, 0;\n\t"
-        "neg.s32         %2, %2;\n\t"      // carry: t += EPS
-        "add.cc.u32      %3, %3, %2;\n\t"
-        "addc.u32        %4, %4, 0;\n\t"
+        "sub.cc.u32      %0, %0, %9;\n\t"   // - r3
+        "subc.cc.u32     %1, %1, 0;\n\t"
+        "subc.u32        %2, %2, 0;\n\t"    // top in {-1, 0, 1}
+        "neg.s32         %3, %2;\n\t"       // top * EPS mod 2^64 = (-top) + 2^32 * (top >> 31)
+        "shr.s32         %4, %2, 31;\n\t"
+        "add.cc.u32      %0, %0, %3;\n\t"
+        "addc.u32        %1, %1, %4;\n\t"
         "}"
-        : "+r"(e0), "+r"(e1), "=&r"(b), "=&r"(t0), "=&r"(t1)
-        : "r"(r3), "r"(r0), "r"(r1));
+        : "=&r"(t0), "=&r"(t1), "=&r"(top), "=&r"(cl), "=&r"(ch)
+        : "r"(r0), "r"(r1), "r"((uint32_t)e), "r"((uint32_t)(e >> 32)), "r"(r3));
     return ((uint64_t)t1 << 32) | t0;
 }
 
