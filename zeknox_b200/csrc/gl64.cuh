@@ -187,9 +187,11 @@ __device__ __forceinline__ uint64_t reduce_nc_alu(uint32_t r0, uint32_t r1, uint
 // pipe) and three fewer ALU instructions: (top:t) = (r1:r0) + r2 * EPS - r3
 // with a signed top limb in {-1, 0, 1}, then one correction t + top * EPS
 // (2^64 = EPS mod p; +EPS cannot wrap again because t <= 2^64 - 2^33 when
-// top = 1, and t >= 2^64 - 2^32 when top = -1).  Which form is faster depends
-// on the permutation's mix of multiplies and additions (measured per hash on
-// B200).
+// top = 1, and t >= 2^64 - 2^32 when top = -1).  The default of the lazy
+// products below: measured 1.03-1.05x on the Poseidon, Poseidon2 and Monolith
+// forests and 1.02-1.03x on the NTT passes on B200, whose integer ALU is the
+// busier pipe in all of them (the all-ALU form stays for comparison and the
+// multiply-rate probe).
 __device__ __forceinline__ uint64_t reduce_nc_imad(uint32_t r0, uint32_t r1, uint32_t r2, uint32_t r3)
 {
     uint64_t e;
@@ -212,7 +214,7 @@ __device__ __forceinline__ uint64_t reduce_nc_imad(uint32_t r0, uint32_t r1, uin
     return ((uint64_t)t1 << 32) | t0;
 }
 
-template <bool IMAD = false>
+template <bool IMAD = true>
 __device__ __forceinline__ uint64_t reduce_nc(uint32_t r0, uint32_t r1, uint32_t r2, uint32_t r3)
 {
     return IMAD ? reduce_nc_imad(r0, r1, r2, r3) : reduce_nc_alu(r0, r1, r2, r3);
@@ -220,7 +222,7 @@ __device__ __forceinline__ uint64_t reduce_nc(uint32_t r0, uint32_t r1, uint32_t
 #endif
 
 // a * b for any 64-bit representatives; result any 64-bit representative.
-template <bool IMAD = false>
+template <bool IMAD = true>
 ZK_HD uint64_t gl_mul_nc(uint64_t a, uint64_t b)
 {
 #ifdef __CUDA_ARCH__
@@ -233,7 +235,7 @@ ZK_HD uint64_t gl_mul_nc(uint64_t a, uint64_t b)
 #endif
 }
 
-template <bool IMAD = false>
+template <bool IMAD = true>
 ZK_HD uint64_t gl_sqr_nc(uint64_t a)
 {
 #ifdef __CUDA_ARCH__
@@ -246,7 +248,7 @@ ZK_HD uint64_t gl_sqr_nc(uint64_t a)
 }
 
 // a * b + c (c any 64-bit value) reduced once.
-template <bool IMAD = false>
+template <bool IMAD = true>
 ZK_HD uint64_t gl_mul_add_nc(uint64_t a, uint64_t b, uint64_t c)
 {
 #ifdef __CUDA_ARCH__
@@ -317,7 +319,7 @@ struct WideAcc {
 #endif
     }
     // any 64-bit representative of the sum
-    template <bool IMAD = false>
+    template <bool IMAD = true>
     ZK_HD uint64_t reduce() const
     {
 #ifdef __CUDA_ARCH__
@@ -400,7 +402,7 @@ ZK_HD uint64_t gl_sbox7(uint64_t x)
 #ifndef ZK_SBOX_SQR
 #define ZK_SBOX_SQR 0
 #endif
-template <bool IMAD = false>
+template <bool IMAD = true>
 ZK_HD uint64_t gl_sbox7_nc(uint64_t x)
 {
     uint64_t x2 = ZK_SBOX_SQR ? gl_sqr_nc<IMAD>(x) : gl_mul_nc<IMAD>(x, x);

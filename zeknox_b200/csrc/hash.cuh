@@ -165,30 +165,27 @@ ZK_HD void poseidon_partial_rounds(uint64_t s[12])
         a.zero();
 #pragma unroll
         for (int j = 0; j < 11; j++) a.mac(s[1 + j], ZKC(POSEIDON_FAST_INIT)[11 * i + j]);
-        t[i] = a.reduce<true>();
+        t[i] = a.reduce();
     }
 #pragma unroll
     for (int i = 0; i < 11; i++) s[1 + i] = t[i];
 #pragma unroll 1
     for (int r = 0; r < 22; r++) {
-        const uint64_t x0 = gl_add_nc(gl_sbox7_nc<true>(s[0]), ZKC(POSEIDON_FAST_K)[r]);
+        const uint64_t x0 = gl_add_nc(gl_sbox7_nc(s[0]), ZKC(POSEIDON_FAST_K)[r]);
         WideAcc a;
         a.zero();
         a.mac(x0, ZK_POSEIDON_FAST_M00);
 #pragma unroll
         for (int i = 0; i < 11; i++) a.mac(s[1 + i], ZKC(POSEIDON_FAST_W)[11 * r + i]);
-        s[0] = a.reduce<true>();
+        s[0] = a.reduce();
 #pragma unroll
-        for (int i = 0; i < 11; i++) s[1 + i] = gl_mul_add_nc<true>(x0, ZKC(POSEIDON_FAST_V)[11 * r + i], s[1 + i]);
+        for (int i = 0; i < 11; i++) s[1 + i] = gl_mul_add_nc(x0, ZKC(POSEIDON_FAST_V)[11 * r + i], s[1 + i]);
     }
 }
 
 // Lanes hold any 64-bit representative between rounds (round constants are
 // < p, so one wrap correction suffices when adding them); the caller
-// canonicalises the digest.  The permutations reduce products with the
-// multiply-assisted reduction (reduce_nc_imad: measured 1.02-1.03x on
-// Poseidon, Poseidon2 and Monolith forests on B200, whose integer ALU is the
-// busier pipe).  One rolled loop over the 8 full rounds, the
+// canonicalises the digest.  One rolled loop over the 8 full rounds, the
 // partial rounds after the fourth, so the full-round code exists once.
 ZK_HD void poseidon_permute(uint64_t s[12])
 {
@@ -196,7 +193,7 @@ ZK_HD void poseidon_permute(uint64_t s[12])
     for (int f = 0; f < 8; f++) {
         const int r = f < 4 ? f : f + 22;
 #pragma unroll
-        for (int i = 0; i < 12; i++) s[i] = gl_sbox7_nc<true>(gl_add_nc(s[i], ZKC(POSEIDON_RC)[12 * r + i]));
+        for (int i = 0; i < 12; i++) s[i] = gl_sbox7_nc(gl_add_nc(s[i], ZKC(POSEIDON_RC)[12 * r + i]));
         poseidon_mds(s);
         if (f == 3) poseidon_partial_rounds(s);
     }
@@ -298,10 +295,10 @@ ZK_HD void poseidon2_permute(uint64_t s[12])
     for (int r = 0; r < 30; r++) {
         if (r < 4 || r >= 26) {
 #pragma unroll
-            for (int i = 0; i < 12; i++) s[i] = gl_sbox7_nc<true>(gl_add_nc(s[i], ZKC(POSEIDON2_RC)[12 * r + i]));
+            for (int i = 0; i < 12; i++) s[i] = gl_sbox7_nc(gl_add_nc(s[i], ZKC(POSEIDON2_RC)[12 * r + i]));
             p2_external(s);
         } else {
-            s[0] = gl_sbox7_nc<true>(gl_add_nc(s[0], ZKC(POSEIDON2_RC)[12 * r]));
+            s[0] = gl_sbox7_nc(gl_add_nc(s[0], ZKC(POSEIDON2_RC)[12 * r]));
             Sum64 acc;
             acc.set(s[0]);
 #pragma unroll
@@ -309,7 +306,7 @@ ZK_HD void poseidon2_permute(uint64_t s[12])
             const uint64_t sum = acc.reduce();
             // s_i * d_i + sum as one 128-bit value, reduced once
 #pragma unroll
-            for (int i = 0; i < 12; i++) s[i] = gl_mul_add_nc<true>(s[i], ZKC(POSEIDON2_DIAG)[i], sum);
+            for (int i = 0; i < 12; i++) s[i] = gl_mul_add_nc(s[i], ZKC(POSEIDON2_DIAG)[i], sum);
         }
     }
 }
@@ -370,7 +367,7 @@ ZK_HD void monolith_permute(uint64_t s[12])
         for (int i = 0; i < 4; i++) s[i] = mono_bar(gl_canon(s[i]));
         uint64_t sq[11];
 #pragma unroll
-        for (int i = 0; i < 11; i++) sq[i] = gl_sqr_nc<true>(s[i]);
+        for (int i = 0; i < 11; i++) sq[i] = gl_sqr_nc(s[i]);
         hi[0] = 0;
 #pragma unroll
         for (int i = 1; i < 12; i++) {
