@@ -6,7 +6,7 @@ tuning table that ``zeknox_b200.load()`` reads.
 Knobs (all shape choices only; results are bit-identical for every value, and
 the tuner checks that for each candidate against the default's output):
 
-* ``lde_last_logr`` (per log2 n): radix exponent 7..9 of the fused LDE's last
+* ``lde_last_logr`` (per log2 n): radix exponent 6..8 of the fused LDE's last
   pass, the one that writes bit-reversed leaf rows;
 * ``lde_chunk_mib`` (per log2 N = log2 n + rate_bits): column-chunk budget of
   the fused LDE, i.e. how much of the inter-pass intermediate is meant to stay
@@ -36,9 +36,9 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.dirname(HERE))
 
-DEFAULTS = {"lde_last_logr": 9, "lde_chunk_mib": 64, "leaf_threads": 256, "wide_level_nodes": 1 << 15}
+DEFAULTS = {"lde_last_logr": 8, "lde_chunk_mib": 64, "leaf_threads": 256, "wide_level_nodes": 1 << 15}
 CANDIDATES = {
-    "lde_last_logr": [9, 8, 7],
+    "lde_last_logr": [8, 7, 6],
     "lde_chunk_mib": [64, 16, 32, 96],
     "leaf_threads": [256, 128, 64],
     "wide_level_nodes": [1 << 15, 1 << 13, 1 << 17, 1 << 40],

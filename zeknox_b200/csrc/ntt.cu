@@ -20,8 +20,11 @@ namespace zk {
 static const uint64_t H_SIZE_INV[33] = {ZK_DOMAIN_SIZE_INV_LIST};
 static const uint64_t H_OMEGA_N[33] = {ZK_OMEGA_LIST};
 
-static constexpr int PASS_NT = 512;
-static constexpr int PASS_TILE = 8192;
+static constexpr int PASS_NT = 256;
+static constexpr int PASS_TILE = 4096;  // 32 KiB of shared memory; measured 1.07-1.14x over 512 x 8192
+static constexpr uint32_t LOG_PASS_TILE = __builtin_ctz(PASS_TILE);
+static constexpr uint32_t MAX_SPLIT_LOGR = LOG_PASS_TILE - 2;  // passes before the last (see plan_passes)
+static constexpr uint32_t MAX_ROWS_LOGR = LOG_PASS_TILE - 4;   // row-output passes: 16 columns x 2^LOGR
 
 // ------------------------------------------------------------- pass dispatch
 
@@ -61,10 +64,12 @@ template <int INV, int LOADM, int STOREM>
 static void launch_pass(uint32_t logr, const NttPassArgs &a, uint64_t grid, uint32_t smem, cudaStream_t s)
 {
     const bool direct = direct_io(logr, a, STOREM == STORE_ROWS);
-#define ZK_CASE(r)                                                                                \
-    case r:                                                                                       \
-        if (direct) launch_one<(STOREM == STORE_ROWS && r > 9) ? 9 : r, INV, LOADM, STOREM, 1>(a, grid, smem, s); \
-        else launch_one<(STOREM == STORE_ROWS && r > 9) ? 9 : r, INV, LOADM, STOREM, 0>(a, grid, smem, s);   \
+    // row-output passes never exceed MAX_ROWS_LOGR (plan_passes): no kernels above it
+#define ZK_R(r) ((STOREM == STORE_ROWS && (r) > (int)MAX_ROWS_LOGR) ? (int)MAX_ROWS_LOGR : (r))
+#define ZK_CASE(r)                                                                       \
+    case r:                                                                              \
+        if (direct) launch_one<ZK_R(r), INV, LOADM, STOREM, 1>(a, grid, smem, s);        \
+        else launch_one<ZK_R(r), INV, LOADM, STOREM, 0>(a, grid, smem, s);               \
         break;
     switch (logr) {
         ZK_CASE(1) ZK_CASE(2) ZK_CASE(3) ZK_CASE(4) ZK_CASE(5) ZK_CASE(6)
@@ -72,28 +77,34 @@ static void launch_pass(uint32_t logr, const NttPassArgs &a, uint64_t grid, uint
     default: throw arg_failure("bad pass radix");
     }
 #undef ZK_CASE
+#undef ZK_R
 }
 
 struct Pass {
     uint32_t s_lo, logr;
 };
 
-// Split L stages into passes of at most 12 (the last at most 9 for row output).
+// Split L stages into passes.  A pass of 2^LOGR points on a tile of 2^LT
+// elements holds 2^(LT - LOGR) groups; passes other than the last are kept to
+// LOGR <= LT - 2 so a tile's rows are runs of >= 4 consecutive offsets (whole
+// 32-byte sectors); a row-output pass spans at most 2^(LT - 4) positions of 16
+// columns.  Single-pass transforms may use the whole tile.
+
 static std::vector<Pass> plan_passes(uint32_t L, bool rows)
 {
     std::vector<uint32_t> sizes;
-    // last pass of a row-output transform: radix 2^lde_last_logr (tuned, <= 9)
-    uint32_t last_rows = (uint32_t)tune_get("lde_last_logr", L, 9);
-    last_rows = last_rows < 1 ? 1 : (last_rows > 9 ? 9 : last_rows);
-    const uint32_t last_max = rows ? last_rows : 12;
+    // last pass of a row-output transform: radix 2^lde_last_logr (tuned)
+    uint32_t last_rows = (uint32_t)tune_get("lde_last_logr", L, MAX_ROWS_LOGR);
+    last_rows = last_rows < 1 ? 1 : (last_rows > MAX_ROWS_LOGR ? MAX_ROWS_LOGR : last_rows);
+    const uint32_t last_max = rows ? last_rows : LOG_PASS_TILE;
     if (L <= last_max) {
         sizes.push_back(L);
     } else if (!rows) {
-        uint32_t np = (L + 11) / 12;
+        uint32_t np = (L + MAX_SPLIT_LOGR - 1) / MAX_SPLIT_LOGR;
         for (uint32_t i = 0; i < np; i++) sizes.push_back(L / np + (i < L % np ? 1 : 0));
     } else {
         uint32_t rem = L - last_rows;
-        uint32_t np = (rem + 11) / 12;
+        uint32_t np = (rem + MAX_SPLIT_LOGR - 1) / MAX_SPLIT_LOGR;
         for (uint32_t i = 0; i < np; i++) sizes.push_back(rem / np + (i < rem % np ? 1 : 0));
         sizes.push_back(last_rows);
     }
@@ -169,7 +180,7 @@ static void run_dif(DeviceCtx &c, const DifJob &j)
             a.dst_stride = j.rows ? n : j.dst_stride;
         }
         const int load = first ? j.load : LOAD_PLAIN;
-        if (store_rows && ps.logr > 9) throw arg_failure("row-output pass radix above 2^9");
+        if (store_rows && ps.logr > MAX_ROWS_LOGR) throw arg_failure("row-output pass radix above the tile");
         uint64_t grid;
         uint32_t tile;
         if (store_rows) {

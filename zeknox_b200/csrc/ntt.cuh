@@ -200,7 +200,7 @@ __device__ __forceinline__ void first_substep_twiddles(uint64_t *x, uint32_t m_l
 // for STORE_SAME, the last sub-step stores straight from registers, instead of
 // separate load / store loops through shared memory.
 template <int LOGR, int INV, int NT, int TILE, int LOADM, int STOREM, int DIRECT>
-__global__ void __launch_bounds__(NT, 2) ntt_pass_kernel(NttPassArgs a)
+__global__ void __launch_bounds__(NT, 1024 / NT) ntt_pass_kernel(NttPassArgs a)
 {
     extern __shared__ uint64_t sm[];
     constexpr uint32_t R = 1u << LOGR;
