@@ -336,9 +336,12 @@ def run_stage(args):
     dig = torch.empty(n_dig * 4, dtype=torch.int64, device="cuda")
     caps = torch.empty(n_cap * 4, dtype=torch.int64, device="cuda")
     zk.lde_rows(0, leaves, inp, lg, RATE, COLS)
+    ev_cols = torch.empty(N * COLS, dtype=torch.int64, device="cuda") if args.only == "transpose" else None
     for _ in range(args.warmup + args.steps):
         if args.only == "lde":
             zk.lde_rows(0, leaves, inp, lg, RATE, COLS)
+        elif args.only == "transpose":
+            zk.transpose_rev(0, leaves, ev_cols, lg + RATE, COLS)
         else:
             zk.fill_digests_buf_linear_gpu(dig, caps, leaves, N, COLS, CAP, HASH)
     torch.cuda.synchronize()
@@ -567,7 +570,7 @@ def main():
     ap.add_argument("--cpu-lg", type=int, default=15, help="log2 coefficients per column of the CPU sample")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     ap.add_argument("--lg-n", type=int, default=LG_N, help="log2 coefficients per column (profiling cases)")
-    ap.add_argument("--only", default=None, choices=["lde", "merkle"],
+    ap.add_argument("--only", default=None, choices=["lde", "merkle", "transpose"],
                     help="profiling: run only this stage for warmup+steps iterations and exit")
     ap.add_argument("--requests", type=int, default=16, help="serve workload: number of requests")
     ap.add_argument("--workload", default="commit", choices=["commit", "batch", "hashes", "serve"],
