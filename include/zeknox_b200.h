@@ -151,6 +151,8 @@ RustError zeknox_server_destroy(void *server);
  *   "lde_chunk_mib"             fused-LDE column chunk budget in MiB (lg = log2 N)
  *   "lde_last_logr"             radix exponent of the fused LDE's row-output pass, 1..8 (lg = log2 n)
  *   "wide_level_nodes.<hash_type>"  Merkle levels at least this wide run node-parallel (lg = log2 leaves)
+ *   "coop_leaves.<hash_type>"   forests of at most this many leaves hash them with four threads per
+ *                               permutation (Poseidon, Poseidon2; lg = log2 leaves)
  * Unset knobs keep the built-in defaults.  Results never depend on the knobs. */
 RustError zeknox_tune_set(const char *name, uint32_t lg, uint64_t value);
 RustError zeknox_tune_clear(void);

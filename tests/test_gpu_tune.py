@@ -37,7 +37,8 @@ def test_lde_rows_independent_of_knobs(knob, value, lg, rate, cols):
 
 @pytest.mark.parametrize("h", [0, 1, 2, 3, 4])
 @pytest.mark.parametrize("knob,value", [("leaf_threads", 64), ("leaf_threads", 128), ("wide_level_nodes", 1),
-                                        ("wide_level_nodes", 1 << 8), ("wide_level_nodes", 1 << 40)])
+                                        ("wide_level_nodes", 1 << 8), ("wide_level_nodes", 1 << 40),
+                                        ("coop_leaves", 0), ("coop_leaves", 1 << 40)])
 def test_merkle_independent_of_knobs(h, knob, value):
     n, leaf, cap = 1 << 12, 7, 2
     zk.tune_set("%s.%d" % (knob, h), value)

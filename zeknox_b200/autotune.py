@@ -15,7 +15,9 @@ the tuner checks that for each candidate against the default's output):
   (one thread per leaf, a CTA of 64 / 128 / 256 leaves);
 * ``wide_level_nodes.<hash>`` (per log2 leaves): Merkle levels with at least this
   many nodes run one launch per level (one thread per node) before the
-  in-CTA fold takes over.
+  in-CTA fold takes over;
+* ``coop_leaves.<hash>`` (per log2 leaves; Poseidon and Poseidon2): forests of at
+  most this many leaves hash their leaves with four threads per permutation.
 
 Each candidate is timed with CUDA events on the launching stream, median of
 several repetitions after warm-up, with the L2 flushed (a 256 MiB write)
@@ -36,13 +38,16 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.dirname(HERE))
 
-DEFAULTS = {"lde_last_logr": 8, "lde_chunk_mib": 64, "leaf_threads": 256, "wide_level_nodes": 1 << 15}
+DEFAULTS = {"lde_last_logr": 8, "lde_chunk_mib": 64, "leaf_threads": 256, "wide_level_nodes": 1 << 15,
+            "coop_leaves": 1 << 13}
 CANDIDATES = {
     "lde_last_logr": [8, 7, 6],
     "lde_chunk_mib": [64, 16, 32, 96],
     "leaf_threads": [256, 128, 64],
     "wide_level_nodes": [1 << 15, 1 << 13, 1 << 17, 1 << 40],
+    "coop_leaves": [1 << 13, 0, 1 << 40],
 }
+COOP_HASHES = (0, 3)  # hashes with the cooperative (four threads per permutation) kernels
 HASH_NAMES = {0: "poseidon", 1: "keccak", 3: "poseidon2", 4: "monolith"}
 RATE = 3
 
@@ -59,6 +64,7 @@ def merkle_shapes(quick):
     out = [(3, 18, 256)]
     if not quick:
         out += [(3, 20, 135), (0, 20, 135), (4, 20, 135), (1, 20, 135), (0, 13, 84), (3, 16, 256)]
+        out += [(h, lg, 135) for h in COOP_HASHES for lg in (12, 14, 15, 16)]
     return out
 
 
@@ -164,6 +170,9 @@ def tune_merkle(zk, torch, timer, h, lg, leaf_size, margin, log):
            margin, log)
     search(zk, timer, "wide_level_nodes.%d" % h, lg, CANDIDATES["wide_level_nodes"], DEFAULTS["wide_level_nodes"],
            run, check, margin, log)
+    if h in COOP_HASHES:
+        search(zk, timer, "coop_leaves.%d" % h, lg, CANDIDATES["coop_leaves"], DEFAULTS["coop_leaves"], run, check,
+               margin, log)
     del leaves, dig, caps, ref_d, ref_c
 
 

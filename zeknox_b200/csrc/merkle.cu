@@ -6,7 +6,10 @@
 // has >= wide_level_nodes nodes; the fold kernel (the next 8 levels inside
 // CTAs, and the caps when whole subtrees fit); for subtrees still above 1024
 // nodes, level kernels, then one tail CTA per subtree -- 2 to 6 launches where
-// the reference launches one per level.
+// the reference launches one per level.  For Poseidon and Poseidon2 the fold
+// and tail kernels (and the leaf kernel of forests of at most coop_leaves
+// leaves) run one permutation per group of four threads (coop.cuh): the fold
+// kernel then takes 6 levels per launch.
 #include <cstdio>
 #include <string>
 
@@ -20,6 +23,9 @@ namespace zk {
 static constexpr int LEAF_T = 256;     // default leaves (threads) per CTA of the leaf kernel ("leaf_threads.<hash>")
 static constexpr int FOLD_T = 256;     // leaf digests per CTA of the fold kernel
 static constexpr int TAIL_MAXM = 1024; // nodes a tail CTA can take
+static constexpr int COOP_T = 256;     // threads (64 groups of four) per CTA of the cooperative kernels
+static constexpr uint64_t COOP_LEAVES = 1ULL << 13;  // default: forests up to this many leaves hash their leaves
+                                                     // with the cooperative kernel ("coop_leaves.<hash>")
 static constexpr uint64_t WIDE_LEVEL_NODES = 1ULL << 15;  // default: levels at least this wide run node-parallel
                                                           // ("wide_level_nodes.<hash>")
 
@@ -31,10 +37,18 @@ bool merkle_geometry_ok(uint64_t n_digests, uint64_t n_caps, uint64_t n_leaves, 
 template <int H>
 static void merkle_launch(uint64_t *digests, uint64_t *caps, const uint64_t *leaves, const MerkleGeom &g, cudaStream_t s)
 {
+    constexpr bool COOP = HasCoop<H>::value;
     const uint32_t lg_leaves = ilog2_exact(g.n_leaves);
     const uint64_t lt = tune_get("leaf_threads." + std::to_string(H), lg_leaves, LEAF_T);
     uint64_t blocks;
-    if (lt == 64) {
+    bool coop_leaf = false;
+    if constexpr (COOP) coop_leaf = g.n_leaves <= tune_get("coop_leaves." + std::to_string(H), lg_leaves, COOP_LEAVES);
+    if (coop_leaf) {
+        if constexpr (COOP) {
+            blocks = (g.n_leaves + COOP_T / 4 - 1) / (COOP_T / 4);
+            merkle_leaf_coop_kernel<H, COOP_T><<<(unsigned)blocks, COOP_T, 0, s>>>(leaves, digests, caps, g);
+        }
+    } else if (lt == 64) {
         blocks = (g.n_leaves + 63) / 64;
         merkle_leaf_kernel_for<H, 64>()<<<(unsigned)blocks, 64, 0, s>>>(leaves, digests, caps, g);
     } else if (lt == 128) {
@@ -56,16 +70,18 @@ static void merkle_launch(uint64_t *digests, uint64_t *caps, const uint64_t *lea
         merkle_level_kernel<H><<<(unsigned)((total + 255) / 256), 256, 0, s>>>(digests, g, u0);
         note_launch();
     }
-    // Narrow levels: folded inside CTAs of FOLD_T nodes.
+    // Narrow levels: folded inside CTAs of fold_nodes nodes.
+    const uint32_t fold_nodes = COOP ? COOP_T / 4 : FOLD_T;
     const uint64_t count = g.n_leaves >> u0;
-    blocks = (count + FOLD_T - 1) / FOLD_T;
-    merkle_fold_kernel<H, FOLD_T><<<(unsigned)blocks, FOLD_T, 0, s>>>(digests, caps, g, u0);
+    blocks = (count + fold_nodes - 1) / fold_nodes;
+    if constexpr (COOP) merkle_fold_coop_kernel<H, COOP_T><<<(unsigned)blocks, COOP_T, 0, s>>>(digests, caps, g, u0);
+    else merkle_fold_kernel<H, FOLD_T><<<(unsigned)blocks, FOLD_T, 0, s>>>(digests, caps, g, u0);
     note_launch();
     const uint64_t sub_nodes = g.sub_leaves >> u0;
-    if (sub_nodes <= (uint64_t)FOLD_T) return;  // caps written by the fold kernel
+    if (sub_nodes <= (uint64_t)fold_nodes) return;  // caps written by the fold kernel
     // heights folded by the fold kernel
     uint32_t U = 0;
-    while ((1u << (U + 1)) <= (uint32_t)FOLD_T && u0 + U + 1 <= top) U++;
+    while ((1u << (U + 1)) <= fold_nodes && u0 + U + 1 <= top) U++;
     u0 += U;
     while ((g.sub_leaves >> u0) > (uint64_t)TAIL_MAXM) {
         u0++;
@@ -75,7 +91,8 @@ static void merkle_launch(uint64_t *digests, uint64_t *caps, const uint64_t *lea
         merkle_level_kernel<H><<<(unsigned)nb, 256, 0, s>>>(digests, g, u0);
         note_launch();
     }
-    merkle_tail_kernel<H, TAIL_MAXM><<<g.n_caps, 256, 0, s>>>(digests, caps, g, u0);
+    if constexpr (COOP) merkle_tail_coop_kernel<H, TAIL_MAXM><<<g.n_caps, 256, 0, s>>>(digests, caps, g, u0);
+    else merkle_tail_kernel<H, TAIL_MAXM><<<g.n_caps, 256, 0, s>>>(digests, caps, g, u0);
     note_launch();
 }
 

@@ -19,6 +19,7 @@
 #pragma once
 #include <stdint.h>
 
+#include "coop.cuh"
 #include "hash.cuh"
 
 namespace zk {
@@ -206,6 +207,145 @@ __global__ void merkle_level_kernel(uint64_t *__restrict__ digests, MerkleGeom g
         hash_two<H>(sub + 4 * (child + 2 * j), sub + 4 * (child + 2 * j + 1), h);
 #pragma unroll
         for (int q = 0; q < 4; q++) sub[4 * (start + j) + q] = h[q];
+    }
+}
+
+// ------------------------------------------------------ cooperative kernels
+//
+// Poseidon and Poseidon2 with one permutation per group of four threads
+// (coop.cuh): the leaves of forests too small to fill the GPU with one leaf
+// per thread, and the tree levels below the wide ones, whose time is the
+// latency of one permutation per level.  A warp holds eight groups; a group
+// with nothing to do hashes a copy of its warp's first task and writes
+// nothing, and a warp with nothing to do skips the level, so the full-warp
+// shuffles always see all 32 threads.
+
+// Leaf digests, one leaf per group.
+template <int H, int T>
+__global__ void __launch_bounds__(T)
+    merkle_leaf_coop_kernel(const uint64_t *__restrict__ leaves, uint64_t *__restrict__ digests,
+                            uint64_t *__restrict__ caps, MerkleGeom g)
+{
+    CoopGroup c;
+    c.init();
+    const uint64_t gi = ((uint64_t)blockIdx.x * T + threadIdx.x) >> 2;
+    if ((gi & ~7ULL) >= g.n_leaves) return;  // the whole warp is past the end
+    const uint64_t i = gi < g.n_leaves ? gi : g.n_leaves - 1;
+    uint64_t d[4];
+    sponge_hash_one_coop<H>(leaves + i * g.leaf_size, g.leaf_size, d, c);
+    if (c.q == 0 && gi < g.n_leaves) {
+        uint64_t *dst = g.sub_leaves == 1 ? caps + 4 * gi : digests + 4 * merkle_node_index(g, gi, 0);
+#pragma unroll
+        for (int q = 0; q < 4; q++) dst[q] = d[q];
+    }
+}
+
+// merkle_fold_kernel with T / 4 nodes of height u0 per CTA.
+template <int H, int T>
+__global__ void __launch_bounds__(T) merkle_fold_coop_kernel(uint64_t *__restrict__ digests, uint64_t *__restrict__ caps,
+                                                             MerkleGeom g, uint32_t u0)
+{
+    constexpr uint32_t NG = T / 4;
+    __shared__ uint64_t node[NG][4];
+    CoopGroup c;
+    c.init();
+    const uint32_t grp = threadIdx.x >> 2;
+    const uint32_t wg = grp & ~7u;  // first group of this warp
+    const uint64_t count = g.n_leaves >> u0;
+    const uint64_t i0 = (uint64_t)blockIdx.x * NG;
+    const uint64_t cta_nodes = count - i0 < (uint64_t)NG ? count - i0 : (uint64_t)NG;
+    for (uint32_t t = threadIdx.x; t < 4 * cta_nodes; t += T)
+        node[t >> 2][t & 3] = digests[4 * merkle_node_index(g, (i0 + (t >> 2)) << u0, u0) + (t & 3)];
+    const uint32_t top = g.log_sub - 1;
+    uint32_t U = 0;
+    while ((1u << (U + 1)) <= NG && u0 + U + 1 <= top) U++;
+    for (uint32_t v = 1; v <= U; v++) {
+        __syncthreads();
+        const uint32_t nodes = NG >> v;
+        const bool act = grp < nodes && ((uint64_t)grp << v) < cta_nodes;
+        const bool wact = wg < nodes && ((uint64_t)wg << v) < cta_nodes;
+        uint64_t h[4];
+        if (wact) {
+            const uint32_t src = act ? grp : wg;
+            sponge_hash_two_coop<H>(node[2 * src], node[2 * src + 1], h, c);
+            if (act && c.q == 0) {
+                const uint64_t di = merkle_node_index(g, (i0 + ((uint64_t)grp << v)) << u0, u0 + v);
+#pragma unroll
+                for (int q = 0; q < 4; q++) digests[4 * di + q] = h[q];
+            }
+        }
+        __syncthreads();
+        if (act && c.q == 0) {
+#pragma unroll
+            for (int q = 0; q < 4; q++) node[grp][q] = h[q];
+        }
+    }
+    const uint64_t sub_nodes = g.sub_leaves >> u0;
+    if (u0 + U == top && sub_nodes <= (uint64_t)NG) {
+        __syncthreads();
+        const uint32_t subs = (uint32_t)(cta_nodes / sub_nodes);
+        if (wg < subs) {
+            const bool act = grp < subs;
+            const uint32_t src = act ? grp : wg;
+            uint64_t h[4];
+            sponge_hash_two_coop<H>(node[2 * src], node[2 * src + 1], h, c);
+            if (act && c.q == 0) {
+                const uint64_t k = ((i0 << u0) >> g.log_sub) + grp;
+#pragma unroll
+                for (int q = 0; q < 4; q++) caps[4 * k + q] = h[q];
+            }
+        }
+    }
+}
+
+// merkle_tail_kernel with one permutation per group: one CTA of 256 threads
+// (64 groups) per subtree.
+template <int H, int MAXM>
+__global__ void __launch_bounds__(256) merkle_tail_coop_kernel(uint64_t *__restrict__ digests, uint64_t *__restrict__ caps,
+                                                               MerkleGeom g, uint32_t u0)
+{
+    constexpr uint32_t NG = 256 / 4;
+    __shared__ uint64_t bufa[MAXM][4];
+    __shared__ uint64_t bufb[MAXM / 2][4];
+    CoopGroup c;
+    c.init();
+    const uint32_t grp = threadIdx.x >> 2;
+    const uint64_t k = blockIdx.x;
+    uint64_t *sub = digests + k * g.sub_digests * 4;
+    uint32_t m = (uint32_t)(g.sub_leaves >> u0);
+    for (uint32_t j = threadIdx.x; j < 4 * m; j += 256) bufa[j >> 2][j & 3] = sub[4 * (m - 2) + j];
+    uint64_t(*src)[4] = bufa;
+    uint64_t(*dst)[4] = bufb;
+    while (m > 2) {
+        __syncthreads();
+        const uint32_t half = m / 2;
+        for (uint32_t base = grp & ~7u; base < half; base += NG) {
+            const uint32_t j = base + (grp & 7u);
+            const bool act = j < half;
+            const uint32_t jj = act ? j : base;
+            uint64_t h[4];
+            sponge_hash_two_coop<H>(src[2 * jj], src[2 * jj + 1], h, c);
+            if (act && c.q == 0) {
+#pragma unroll
+                for (int q = 0; q < 4; q++) {
+                    sub[4 * (half - 2 + j) + q] = h[q];
+                    dst[j][q] = h[q];
+                }
+            }
+        }
+        uint64_t(*tmp)[4] = src;
+        src = dst;
+        dst = tmp;
+        m = half;
+    }
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        uint64_t h[4];
+        sponge_hash_two_coop<H>(src[0], src[1], h, c);
+        if (threadIdx.x == 0) {
+#pragma unroll
+            for (int q = 0; q < 4; q++) caps[4 * k + q] = h[q];
+        }
     }
 }
 
