@@ -53,4 +53,15 @@ ZK_EXTERNC void fill_digests_buf_linear_cpu(void *digests_buf_ptr, void *cap_buf
                                             u64 digests_buf_size, u64 cap_buf_size, u64 leaves_buf_size, u64 leaf_size,
                                             u64 cap_height, u64 hash_type);
 
+/* Vector host builders, Poseidon only (replace native/merkle/merkle.h:64-88, which the
+ * reference declares and exports only in USE_AVX / USE_AVX512 builds; always exported here).
+ * Same forest as fill_digests_buf_linear_cpu; W = 8 (AVX-512) or 4 (AVX2) leaves per
+ * permutation, the portable builder on CPUs without the instruction set. */
+ZK_EXTERNC void fill_digests_buf_linear_cpu_avx(void *digests_buf_ptr, void *cap_buf_ptr, const void *leaves_buf_ptr,
+                                                u64 digests_buf_size, u64 cap_buf_size, u64 leaves_buf_size,
+                                                u64 leaf_size, u64 cap_height, u64 hash_type);
+ZK_EXTERNC void fill_digests_buf_linear_cpu_avx512(void *digests_buf_ptr, void *cap_buf_ptr,
+                                                   const void *leaves_buf_ptr, u64 digests_buf_size, u64 cap_buf_size,
+                                                   u64 leaves_buf_size, u64 leaf_size, u64 cap_height, u64 hash_type);
+
 #endif /* ZEKNOX_MERKLE_MERKLE_H */

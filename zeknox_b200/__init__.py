@@ -29,7 +29,8 @@ ABI_SYMBOLS = [
     "init_twiddle_factors", "init_coset", "compute_batched_ntt", "compute_batched_lde",
     "compute_batched_lde_multi_gpu", "compute_transpose_rev", "compute_naive_transpose_rev",
     "fill_digests_buf_linear_gpu_with_gpu_ptr", "fill_digests_buf_linear_multigpu_with_gpu_ptr",
-    "fill_digests_buf_linear_cpu", "cuda_available",
+    "fill_digests_buf_linear_cpu", "cuda_available", "fill_digests_buf_linear_cpu_avx",
+    "fill_digests_buf_linear_cpu_avx512",
 ]
 EXT_SYMBOLS = ["zeknox_last_error", "zeknox_commit", "zeknox_commit_batch", "zeknox_commit_scratch_words",
                "zeknox_lde_rows", "zeknox_launch_count", "zeknox_measure_mul_rate", "zeknox_merkle_batch",
@@ -160,8 +161,9 @@ def load():
     L.fill_digests_buf_linear_gpu_with_gpu_ptr.argtypes = [vp, vp, vp] + [u64] * 7
     L.fill_digests_buf_linear_multigpu_with_gpu_ptr.restype = None
     L.fill_digests_buf_linear_multigpu_with_gpu_ptr.argtypes = [vp, vp, vp] + [u64] * 6
-    L.fill_digests_buf_linear_cpu.restype = None
-    L.fill_digests_buf_linear_cpu.argtypes = [vp, vp, vp] + [u64] * 6
+    for f in (L.fill_digests_buf_linear_cpu, L.fill_digests_buf_linear_cpu_avx, L.fill_digests_buf_linear_cpu_avx512):
+        f.restype = None
+        f.argtypes = [vp, vp, vp] + [u64] * 6
     L.cuda_available.restype = ctypes.c_bool
     L.zeknox_last_error.restype = ctypes.c_char_p
     L.zeknox_commit.restype = RustError
@@ -346,11 +348,15 @@ def fill_digests_buf_linear_multigpu(digests, caps, leaves, n_leaves, leaf_size,
         raise ZeknoxError(1, after)
 
 
-def fill_digests_buf_linear_cpu(digests, caps, leaves, n_leaves, leaf_size, cap_height, hash_type):
+def fill_digests_buf_linear_cpu(digests, caps, leaves, n_leaves, leaf_size, cap_height, hash_type, vector=None):
+    """Host forest builder.  vector: None (fill_digests_buf_linear_cpu), "avx" or
+    "avx512" (the vector builders, Poseidon only)."""
     n_dig, n_caps = merkle_sizes(n_leaves, cap_height)
+    L = load()
+    fn = {None: L.fill_digests_buf_linear_cpu, "avx": L.fill_digests_buf_linear_cpu_avx,
+          "avx512": L.fill_digests_buf_linear_cpu_avx512}[vector]
     before = last_error()
-    load().fill_digests_buf_linear_cpu(_ptr(digests), _ptr(caps), _ptr(leaves), n_dig, n_caps, n_leaves, leaf_size,
-                                       cap_height, hash_type)
+    fn(_ptr(digests), _ptr(caps), _ptr(leaves), n_dig, n_caps, n_leaves, leaf_size, cap_height, hash_type)
     after = last_error()
     if after is not None and after != before:
         raise ZeknoxError(1, after)

@@ -14,6 +14,7 @@
 #include "../../include/lib.h"
 #include "../../include/zeknox_b200.h"
 #include "batch.cuh"
+#include "geom.h"
 #include "gl64.cuh"
 #include "ntt_api.cuh"
 #include "runtime.cuh"
@@ -21,6 +22,11 @@
 
 bool zk_merkle_cpu(void *digests, void *caps, const void *leaves, uint64_t n_dig, uint64_t n_cap, uint64_t n_leaves,
                    uint64_t leaf_size, uint64_t cap_height, uint64_t hash_type, std::string &err);
+// merkle_avx.cpp, compiled for AVX-512 and for AVX2 (call only on CPUs that have them)
+extern "C" void zk_merkle_poseidon_avx512(uint64_t *dig, uint64_t *cap, const uint64_t *leaves, uint64_t n_dig,
+                                          uint64_t n_cap, uint64_t n_leaves, uint64_t leaf_size, uint64_t cap_height);
+extern "C" void zk_merkle_poseidon_avx2(uint64_t *dig, uint64_t *cap, const uint64_t *leaves, uint64_t n_dig,
+                                        uint64_t n_cap, uint64_t n_leaves, uint64_t leaf_size, uint64_t cap_height);
 
 namespace {
 
@@ -442,6 +448,60 @@ extern "C" void fill_digests_buf_linear_cpu(void *digests_buf_ptr, void *cap_buf
     if (!zk_merkle_cpu(digests_buf_ptr, cap_buf_ptr, leaves_buf_ptr, digests_buf_size, cap_buf_size, leaves_buf_size,
                        leaf_size, cap_height, hash_type, err))
         record_error("fill_digests_buf_linear_cpu", err);
+}
+
+// The reference's vector host builders (native/merkle/merkle.h:64-88,
+// native/merkle/merkle_avx.cpp:189-276 and 451-538; exported there only from
+// USE_AVX / USE_AVX512 builds): Poseidon only.  Here always exported; the
+// forest is the one fill_digests_buf_linear_cpu builds (caps, digests and
+// their layout), hashed W leaves per permutation on the vector units, or
+// without them on a CPU that lacks the instruction set.  Unlike the reference:
+// with caps == leaves the leaf hashes go to the caps (the reference's vector
+// builders write them to the digests, which are empty then), and the AVX2
+// builder hashes every leaf and node (the reference's steps by two, skipping
+// odd ones).
+static void merkle_cpu_vector(const char *who, bool avx512, void *digests_buf_ptr, void *cap_buf_ptr,
+                              const void *leaves_buf_ptr, u64 digests_buf_size, u64 cap_buf_size, u64 leaves_buf_size,
+                              u64 leaf_size, u64 cap_height, u64 hash_type)
+{
+    std::string err;
+    if (!digests_buf_ptr || !cap_buf_ptr || !leaves_buf_ptr) {
+        record_error(who, "null pointer");
+        return;
+    }
+    if (!zk::merkle_geometry_check(digests_buf_size, cap_buf_size, leaves_buf_size, cap_height, err)) {
+        record_error(who, err);
+        return;
+    }
+    if (hash_type != 0) {  // HashPoseidon
+        record_error(who, "only Poseidon (hash_type 0) has a vector host builder, got " + std::to_string(hash_type));
+        return;
+    }
+    uint64_t *d = (uint64_t *)digests_buf_ptr, *c = (uint64_t *)cap_buf_ptr;
+    const uint64_t *l = (const uint64_t *)leaves_buf_ptr;
+    if (avx512 && __builtin_cpu_supports("avx512f"))
+        zk_merkle_poseidon_avx512(d, c, l, digests_buf_size, cap_buf_size, leaves_buf_size, leaf_size, cap_height);
+    else if (__builtin_cpu_supports("avx2"))
+        zk_merkle_poseidon_avx2(d, c, l, digests_buf_size, cap_buf_size, leaves_buf_size, leaf_size, cap_height);
+    else if (!zk_merkle_cpu(digests_buf_ptr, cap_buf_ptr, leaves_buf_ptr, digests_buf_size, cap_buf_size,
+                            leaves_buf_size, leaf_size, cap_height, hash_type, err))
+        record_error(who, err);
+}
+
+extern "C" void fill_digests_buf_linear_cpu_avx(void *digests_buf_ptr, void *cap_buf_ptr, const void *leaves_buf_ptr,
+                                                u64 digests_buf_size, u64 cap_buf_size, u64 leaves_buf_size,
+                                                u64 leaf_size, u64 cap_height, u64 hash_type)
+{
+    merkle_cpu_vector("fill_digests_buf_linear_cpu_avx", false, digests_buf_ptr, cap_buf_ptr, leaves_buf_ptr,
+                      digests_buf_size, cap_buf_size, leaves_buf_size, leaf_size, cap_height, hash_type);
+}
+
+extern "C" void fill_digests_buf_linear_cpu_avx512(void *digests_buf_ptr, void *cap_buf_ptr, const void *leaves_buf_ptr,
+                                                   u64 digests_buf_size, u64 cap_buf_size, u64 leaves_buf_size,
+                                                   u64 leaf_size, u64 cap_height, u64 hash_type)
+{
+    merkle_cpu_vector("fill_digests_buf_linear_cpu_avx512", true, digests_buf_ptr, cap_buf_ptr, leaves_buf_ptr,
+                      digests_buf_size, cap_buf_size, leaves_buf_size, leaf_size, cap_height, hash_type);
 }
 
 // -------------------------------------------------------------- extensions
