@@ -347,13 +347,66 @@ ZK_HD uint64_t gl_mul(uint64_t a, uint64_t b) { return gl_canon(gl_mul_nc(a, b))
 
 ZK_HD uint64_t gl_sqr(uint64_t a) { return gl_canon(gl_sqr_nc(a)); }
 
-// a * 2^s for 0 <= s < 64: the 128-bit shift then the special reduction.
+// a * 2^s for 0 <= s < 64: the 128-bit shift then the special reduction.  On
+// the device the shift is two wide multiplies of a's 32-bit halves by
+// 2^(s mod 32) -- the multiply pipe, which the NTT passes leave mostly idle,
+// instead of 64-bit shifts on the integer ALU they are bound by -- and the
+// reduction knows which limbs are zero: for s < 32 the value is below 2^96
+// (lo + EPS * r2), for s >= 32 its low word is 0.
 ZK_HD uint64_t gl_mul_pow2_lt64(uint64_t a, unsigned s)
 {
     if (s == 0) return a;
 #ifdef __CUDA_ARCH__
-    const uint64_t lo = a << s, hi = a >> (64 - s);
-    return gl_canon(reduce_nc((uint32_t)lo, (uint32_t)(lo >> 32), (uint32_t)hi, (uint32_t)(hi >> 32)));
+    const uint32_t m = 1u << (s & 31);
+    uint32_t q0, q1, q2;  // a * m = q0 + 2^32 q1 + 2^64 q2
+    asm("{\n\t"
+        ".reg .u64 p0, p1;\n\t"
+        ".reg .u32 h0, l1, h1;\n\t"
+        "mul.wide.u32    p0, %3, %5;\n\t"
+        "mul.wide.u32    p1, %4, %5;\n\t"
+        "mov.b64         {%0, h0}, p0;\n\t"
+        "mov.b64         {l1, h1}, p1;\n\t"
+        "add.cc.u32      %1, h0, l1;\n\t"
+        "addc.u32        %2, h1, 0;\n\t"
+        "}"
+        : "=r"(q0), "=r"(q1), "=r"(q2)
+        : "r"((uint32_t)a), "r"((uint32_t)(a >> 32)), "r"(m));
+    uint32_t t0, t1;
+    if (s < 32) {
+        // q0 + 2^32 q1 + EPS q2, one correction (no second wrap: the sum is < 2^65 - 2^33)
+        uint64_t e;
+        asm("mul.wide.u32 %0, %1, 0xffffffff;" : "=l"(e) : "r"(q2));
+        asm("{\n\t"
+            ".reg .u32 top;\n\t"
+            "add.cc.u32      %0, %2, %4;\n\t"
+            "addc.cc.u32     %1, %3, %5;\n\t"
+            "addc.u32        top, 0, 0;\n\t"
+            "neg.s32         top, top;\n\t"
+            "add.cc.u32      %0, %0, top;\n\t"
+            "addc.u32        %1, %1, 0;\n\t"
+            "}"
+            : "=&r"(t0), "=&r"(t1)
+            : "r"(q0), "r"(q1), "r"((uint32_t)e), "r"((uint32_t)(e >> 32)));
+    } else {
+        // 2^32 q0 + EPS q1 - q2 with a signed top limb, as reduce_nc_imad
+        uint64_t e;
+        asm("mul.wide.u32 %0, %1, 0xffffffff;" : "=l"(e) : "r"(q1));
+        asm("{\n\t"
+            ".reg .u32 top, cl, ch;\n\t"
+            "add.cc.u32      %1, %2, %4;\n\t"
+            "addc.u32        top, 0, 0;\n\t"
+            "sub.cc.u32      %0, %3, %5;\n\t"
+            "subc.cc.u32     %1, %1, 0;\n\t"
+            "subc.u32        top, top, 0;\n\t"
+            "neg.s32         cl, top;\n\t"
+            "shr.s32         ch, top, 31;\n\t"
+            "add.cc.u32      %0, %0, cl;\n\t"
+            "addc.u32        %1, %1, ch;\n\t"
+            "}"
+            : "=&r"(t0), "=&r"(t1)
+            : "r"(q0), "r"((uint32_t)e), "r"((uint32_t)(e >> 32)), "r"(q2));
+    }
+    return gl_canon(((uint64_t)t1 << 32) | t0);
 #else
     return gl_reduce128(a << s, a >> (64 - s));
 #endif
