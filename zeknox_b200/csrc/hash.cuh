@@ -295,10 +295,10 @@ ZK_HD void poseidon2_permute(uint64_t s[12])
     for (int r = 0; r < 30; r++) {
         if (r < 4 || r >= 26) {
 #pragma unroll
-            for (int i = 0; i < 12; i++) s[i] = gl_sbox7_nc(gl_add_nc(s[i], ZKC(POSEIDON2_RC)[12 * r + i]));
+            for (int i = 0; i < 12; i++) s[i] = gl_sbox7_nc<true, true>(gl_add_nc(s[i], ZKC(POSEIDON2_RC)[12 * r + i]));
             p2_external(s);
         } else {
-            s[0] = gl_sbox7_nc(gl_add_nc(s[0], ZKC(POSEIDON2_RC)[12 * r]));
+            s[0] = gl_sbox7_nc<true, true>(gl_add_nc(s[0], ZKC(POSEIDON2_RC)[12 * r]));
             Sum64 acc;
             acc.set(s[0]);
 #pragma unroll
