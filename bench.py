@@ -526,15 +526,29 @@ def run_serve(args):
     done_t = [None] * len(reqs)
     with zk.Server(0, 120 << 30, 8) as srv:
         tickets = [None] * len(reqs)
-        ready = th.Semaphore(0)
+        submitted = []  # indices, in submission order
+        lock = th.Lock()
 
         def reaper():
-            for i in range(len(reqs)):
-                ready.acquire()
-                r = srv.wait(tickets[i])
-                assert r.status == 2, r.status
-                lat[i], queue[i], done_t[i] = r.latency_ms, r.queue_ms, time.perf_counter()
-                srv.release(tickets[i])
+            # a client that takes each result as soon as it is ready, in
+            # completion order, and releases its memory back to the budget
+            outstanding, seen, n_done = set(), 0, 0
+            while n_done < len(reqs):
+                with lock:
+                    outstanding.update(submitted[seen:])
+                    seen = len(submitted)
+                finished = []
+                for i in outstanding:
+                    r = srv.wait(tickets[i], 0.0)
+                    if r.status == 2 or r.status < 0:
+                        assert r.status == 2, r.status
+                        lat[i], queue[i], done_t[i] = r.latency_ms, r.queue_ms, time.perf_counter()
+                        srv.release(tickets[i])
+                        finished.append(i)
+                outstanding.difference_update(finished)
+                n_done += len(finished)
+                if not finished:
+                    time.sleep(0.0002)
 
         rt = th.Thread(target=reaper)
         rt.start()
@@ -546,7 +560,8 @@ def run_serve(args):
             if delay > 0:
                 time.sleep(delay)
             tickets[i] = srv.submit(lg, r, c, cap, h, inp, caps_host=caps_host[i])
-            ready.release()
+            with lock:
+                submitted.append(i)
         rt.join()
         st = srv.stats()
     span = max(done_t) - t0

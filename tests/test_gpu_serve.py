@@ -55,3 +55,35 @@ def test_rejects_request_larger_than_budget():
     with zk.Server(0, 1 << 20, 2) as srv:
         with pytest.raises(zk.ZeknoxError):
             srv.submit(12, 3, 64, 4, 0, inp)
+
+
+def job_bytes(lg, rate, cols, cap):
+    """The server's accounting of one request's device memory."""
+    N, caps = 1 << (lg + rate), 1 << cap
+    t = torch.zeros(1, dtype=torch.int64)
+    words = zk.commit_scratch_words(zk.commit_job(lg, rate, cols, cap, 0, t, t, t, t))
+    return 8 * (N * cols + 8 * (N - caps) + 4 * caps + words)
+
+
+def test_small_request_passes_a_head_that_waits_for_memory():
+    big, small = (14, 3, 64, 4, 3), (10, 2, 16, 2, 3)
+    budget = job_bytes(*big[:4]) * 3 // 2  # one big request at a time
+    assert job_bytes(*small[:4]) <= budget // 8
+    shapes = [big, big, small]
+    inputs = [to_dev(O.field_data(900 + i, s[2] << s[0])) for i, s in enumerate(shapes)]
+    solo = [alone(*s, inp)[0] for s, inp in zip(shapes, inputs)]
+    caps_host = [torch.zeros((1 << s[3]) * 4, dtype=torch.int64).pin_memory() for s in shapes]
+    with zk.Server(0, budget, 4) as srv:
+        tickets = [srv.submit(*s, inp, caps_host=ch) for s, inp, ch in zip(shapes, inputs, caps_host)]
+        res = []
+        for t in tickets:
+            r = srv.wait(t)
+            assert r.status == 2, r.status
+            res.append((r.queue_ms, r.latency_ms))
+            srv.release(t)
+        assert srv.stats()["peak"] <= budget
+    for ch, caps in zip(caps_host, solo):
+        assert np.array_equal(ch.numpy().view(np.uint64), caps)
+    # the small request, submitted last, started before the second big one
+    # (which waited for the first one's memory)
+    assert res[2][0] < res[1][0], res

@@ -4,9 +4,14 @@
 // server admits the head of the queue whenever a slot stream is idle and the
 // job's device memory fits the budget, enqueues the whole commit (allocation,
 // LDE, Merkle, caps copy-out) on that slot's stream, and polls the slot
-// events to retire finished jobs.  Device side: jobs on different slots
-// overlap; twiddle, coset and round-constant tables stay resident in the
-// device context across requests.
+// events to retire finished jobs.  While the head waits for memory (not for a
+// slot), small requests behind it (at most 1/8 of the budget each) that fit
+// now may start ahead of it, at most `slots` of them per waiting head: a large
+// request then holds up no small one, and waits for at most `slots` small
+// ones itself.  Device side: jobs on different slots overlap; twiddle, coset
+// and round-constant tables stay resident in the device context across
+// requests (small requests on high-priority streams measured lower delivered
+// throughput and a 8x higher p50 on the 16-request stream).
 #include <cuda_runtime.h>
 #include <string.h>
 
@@ -48,6 +53,8 @@ struct Server {
     std::deque<uint64_t> queue;
     std::map<uint64_t, Ticket> tickets;
     uint64_t next_id = 1;
+    uint64_t blocked_head = 0;  // head of the queue that waits for memory
+    uint32_t bypassed = 0;      // small requests started ahead of it
     bool stop = false;
     std::thread worker;
 
@@ -131,18 +138,32 @@ struct Server {
                 progressed = true;
             }
             if (progressed) cv.notify_all();
-            // admit in arrival order
+            // admit in arrival order, small requests past a head that waits for memory
             while (!queue.empty()) {
-                const uint64_t id = queue.front();
-                Ticket &t = tickets[id];
                 int slot = -1;
                 for (size_t k = 0; k < slot_ticket.size(); k++)
                     if (!slot_ticket[k]) {
                         slot = (int)k;
                         break;
                     }
-                if (slot < 0 || in_use + t.bytes > budget) break;
-                queue.pop_front();
+                if (slot < 0) break;
+                auto pick = queue.begin();
+                if (in_use + tickets[*pick].bytes > budget) {
+                    if (blocked_head != *pick) {
+                        blocked_head = *pick;
+                        bypassed = 0;
+                    }
+                    if (bypassed >= slot_ticket.size()) break;
+                    for (++pick; pick != queue.end(); ++pick) {
+                        const uint64_t b = tickets[*pick].bytes;
+                        if (b <= budget / 8 && in_use + b <= budget) break;
+                    }
+                    if (pick == queue.end()) break;
+                    bypassed++;
+                }
+                const uint64_t id = *pick;
+                Ticket &t = tickets[id];
+                queue.erase(pick);
                 in_use += t.bytes;
                 peak = in_use > peak ? in_use : peak;
                 t.slot = slot;
