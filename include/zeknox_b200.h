@@ -116,10 +116,13 @@ RustError zeknox_lde_rows_noalloc(size_t device_id, uint64_t *rows, const uint64
  * A server owns a device-memory budget and `slots` streams.  Requests
  * (zk_serve_request) are queued by any host thread; a server thread admits
  * them in arrival order whenever a slot is free and the job's memory (its
- * leaves, digests, caps and scratch) fits the budget, runs the commit on the
- * slot's stream -- so admitted jobs overlap on the device -- copies the caps to
- * the request's host buffer, and records the latency (submit -> caps on host).
- * Results stay in server-owned device memory until released. */
+ * leaves, digests, caps and scratch) fits the budget -- while the head waits
+ * for memory, up to `slots` small requests (<= budget / 8) behind it that fit
+ * may start first -- runs the commit on the slot's stream -- so admitted jobs
+ * overlap on the device -- copies the caps to the request's host buffer, and
+ * records the latency (submit -> caps on host).  Results stay in server-owned
+ * device memory until released: release them as they complete, the budget
+ * counts them until then. */
 typedef struct {
     uint32_t lg_n, rate_bits, cols, cap_height, hash_type, input_is_values;
     uint64_t coset_gen;       /* 0 means 7 */
