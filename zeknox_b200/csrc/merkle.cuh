@@ -89,6 +89,38 @@ __global__ void __launch_bounds__(T, 1024 / T)
     merkle_leaf_body<H, T>(leaves, digests, caps, g);
 }
 
+// Leaf digests plus the LV tree levels above them inside the CTA (sponge
+// hashes only; needs T leaves per CTA inside one subtree and LV < log2 T,
+// LV <= the subtree's top height).  A node is the sponge hash of its two
+// children's 8 consecutive words, so leaves and nodes go through the same
+// call site and the permutation's code exists once.
+template <int H, int T, int LV>
+__global__ void __launch_bounds__(T, 1024 / T)
+    merkle_leaf_levels_kernel(const uint64_t *__restrict__ leaves, uint64_t *__restrict__ digests, MerkleGeom g)
+{
+    __shared__ uint64_t nd[T][4];
+    const uint64_t i0 = (uint64_t)blockIdx.x * T;
+    const uint32_t t = threadIdx.x;
+#pragma unroll 1
+    for (int v = 0; v <= LV; v++) {
+        const uint32_t nodes = T >> v;
+        uint64_t h[4];
+        if (t < nodes) {
+            const uint64_t *src = v == 0 ? leaves + (i0 + t) * g.leaf_size : &nd[2 * t][0];
+            sponge_hash_one<H>(src, v == 0 ? g.leaf_size : 8, h);
+            const uint64_t di = merkle_node_index(g, i0 + ((uint64_t)t << v), (uint32_t)v);
+#pragma unroll
+            for (int q = 0; q < 4; q++) digests[4 * di + q] = h[q];
+        }
+        __syncthreads();
+        if (t < nodes) {
+#pragma unroll
+            for (int q = 0; q < 4; q++) nd[t][q] = h[q];
+        }
+        __syncthreads();
+    }
+}
+
 // Leaf kernel of hash H with CTAs of T threads.
 template <int H, int T>
 constexpr auto merkle_leaf_kernel_for()
