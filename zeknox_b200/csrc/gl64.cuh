@@ -114,7 +114,8 @@ ZK_HD uint64_t gl_reduce96(uint64_t lo, uint64_t hi) { return gl_canon(gl_reduce
 // Lazily reduced arithmetic ("nc" = any 64-bit representative, not
 // necessarily < p).  On the device these are 32-bit PTX carry chains: the
 // 64x64 product is 8 multiply-adds, the reduction of lo + 2^64*(h0 + 2^32*h1)
-// to lo - h1 + EPS*h0 is 13 integer ops with no compares or selects.
+// to lo - h1 + EPS*h0 is one wide multiply and 10 integer ops (or 13 integer
+// ops in the all-ALU form) with no compares or selects.
 
 #ifdef __CUDACC__
 __device__ __forceinline__ void mul_wide(uint64_t a, uint64_t b, uint32_t &r0, uint32_t &r1, uint32_t &r2, uint32_t &r3)
