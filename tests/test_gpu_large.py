@@ -107,3 +107,36 @@ def test_commit_past_2_31_leaf_elements(h):
     for k in (0, n_cap - 1):
         assert np.array_equal(u64(caps[4 * k:4 * k + 4]), O.hash_two(h, digest(k, 0), digest(k, 1))), k
     del coeffs, rows, dig, caps
+
+
+@pytest.mark.parametrize("lg,b", [(24, 4), (22, 16)])
+def test_ntt_round_trip_large(lg, b):
+    """compute_batched_ntt then its inverse is the identity (2^24-point transforms)."""
+    x = torch.randint(0, 1 << 62, (b << lg,), dtype=torch.int64, device="cuda")
+    y = x.clone()
+    zk.ntt_batch(0, y, lg, b)
+    assert not torch.equal(x, y)
+    zk.intt_batch(0, y, lg, b)
+    assert torch.equal(x, y)
+
+
+def test_lde_rows_additive_at_headline_size():
+    """The fused LDE is linear: rows(a + b) = rows(a) + rows(b) mod p, at the
+    headline shape (256 columns x 2^15, rate 3)."""
+    lg, rate, cols = 15, 3, 256
+    N = 1 << (lg + rate)
+    a = torch.randint(0, 1 << 62, (cols << lg,), dtype=torch.int64, device="cuda")
+    b = torch.randint(0, 1 << 62, (cols << lg,), dtype=torch.int64, device="cuda")
+    p = np.uint64(P)
+
+    def add(x, y):
+        s = x + y
+        return np.where((s < x) | (s >= p), s - p, s)
+
+    c = torch.from_numpy(add(u64(a), u64(b)).view(np.int64)).cuda()
+    rows = [torch.empty(cols * N, dtype=torch.int64, device="cuda") for _ in range(3)]
+    for r, x in zip(rows, (a, b, c)):
+        zk.lde_rows(0, r, x, lg, rate, cols)
+    torch.cuda.synchronize()
+    with np.errstate(over="ignore"):
+        assert np.array_equal(u64(rows[2]), add(u64(rows[0]), u64(rows[1])))
