@@ -152,6 +152,7 @@ RustError zeknox_server_destroy(void *server);
  * Knobs, each optionally per log2 size (lg = 0xFFFFFFFF: any size):
  *   "leaf_threads.<hash_type>"  Merkle leaf kernel CTA size, 64/128/256 (lg = log2 leaves)
  *   "lde_chunk_mib"             fused-LDE column chunk budget in MiB (lg = log2 N)
+ *   "lde_host_chunk_mib"        the same for inputs in host memory (copies overlap the chunks)
  *   "lde_last_logr"             radix exponent of the fused LDE's row-output pass, 1..8 (lg = log2 n)
  *   "wide_level_nodes.<hash_type>"  Merkle levels at least this wide run node-parallel (lg = log2 leaves)
  *   "coop_leaves.<hash_type>"   forests of at most this many leaves hash them with four threads per

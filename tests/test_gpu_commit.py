@@ -159,8 +159,8 @@ def test_commit_on_caller_stream():
 @pytest.mark.parametrize("lg,rate,cols", [(13, 3, 72), (15, 3, 100), (16, 2, 81)])
 def test_commit_from_host_memory(pinned, lg, rate, cols):
     """zeknox_commit with a host input pointer stages the coefficients itself
-    (chunked copies overlapping the LDE; the larger shapes get 16-column first
-    and last chunks around the L2-sized ones); same commitment as a device input."""
+    (chunked copies overlapping the LDE; the larger shapes take several
+    chunks); same commitment as a device input."""
     cap, h = 4, 3
     c = O.field_data(88, cols << lg)
     host = torch.from_numpy(c.view(np.int64).copy())

@@ -14,7 +14,7 @@ from zeknox_b200 import autotune
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 KNOBS = {"leaf_threads": {64, 128, 256}, "lde_chunk_mib": None, "lde_last_logr": set(range(1, 9)),
-         "wide_level_nodes": None, "coop_leaves": None}
+         "wide_level_nodes": None, "coop_leaves": None, "lde_host_chunk_mib": None}
 
 
 @pytest.fixture

@@ -9,8 +9,7 @@ the tuner checks that for each candidate against the default's output):
 * ``lde_last_logr`` (per log2 n): radix exponent 6..8 of the fused LDE's last
   pass, the one that writes bit-reversed leaf rows;
 * ``lde_chunk_mib`` (per log2 N = log2 n + rate_bits): column-chunk budget of
-  the fused LDE, i.e. how much of the inter-pass intermediate is meant to stay
-  in the 126 MB L2 between the two passes;
+  the fused LDE (its scratch: the inter-pass intermediate of one chunk);
 * ``leaf_threads.<hash>`` (per log2 leaves): CTA size of the Merkle leaf kernel
   (one thread per leaf, a CTA of 64 / 128 / 256 leaves);
 * ``wide_level_nodes.<hash>`` (per log2 leaves): Merkle levels with at least this
@@ -38,11 +37,11 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.dirname(HERE))
 
-DEFAULTS = {"lde_last_logr": 8, "lde_chunk_mib": 64, "leaf_threads": 256, "wide_level_nodes": 1 << 15,
+DEFAULTS = {"lde_last_logr": 8, "lde_chunk_mib": 512, "leaf_threads": 256, "wide_level_nodes": 1 << 15,
             "coop_leaves": 1 << 13}
 CANDIDATES = {
     "lde_last_logr": [8, 7, 6],
-    "lde_chunk_mib": [64, 16, 32, 96],
+    "lde_chunk_mib": [512, 96, 128, 256, 2048],
     "leaf_threads": [256, 128, 64],
     "wide_level_nodes": [1 << 15, 1 << 13, 1 << 17, 1 << 40],
     "coop_leaves": [1 << 13, 0, 1 << 40],

@@ -310,16 +310,28 @@ void lde_batch_device(DeviceCtx &c, uint64_t *out, const uint64_t *in, uint32_t 
 }
 
 // Columns per chunk of the fused LDE: the intermediate of a chunk (2^(lg_n +
-// rate) words per column) is kept within lde_chunk_mib MiB so the second pass
-// reads it back from L2 instead of HBM.  A multiple of the 16-column row tile.
-static constexpr uint64_t ZK_L2_CHUNK_MIB = 64;  // default; the autotuner may set "lde_chunk_mib"
+// rate) words per column) is kept within lde_chunk_mib MiB, which bounds the
+// scratch whatever the job size.  A multiple of the 16-column row tile.
+// Larger chunks are faster: the intermediate does not stay in the 126 MB L2
+// anyway (the streaming row output shares it), and fewer, larger launches
+// lose less to their last partial wave (256 x 2^15 at rate 3: 1.21 ms in one
+// chunk against 1.32 ms in 48-column chunks).  Inputs in host memory use
+// lde_host_chunk_mib instead: there each chunk's copy overlaps the transform of
+// the one before, so a whole-input chunk would expose the whole copy.
+static constexpr uint64_t ZK_CHUNK_MIB = 512;       // default; the autotuner may set "lde_chunk_mib"
+static constexpr uint64_t ZK_HOST_CHUNK_MIB = 96;   // "lde_host_chunk_mib"
+
+static uint32_t chunk_cols_for(uint64_t mib, uint32_t lg_n, uint32_t rate, uint64_t cols)
+{
+    const uint64_t per_col = 8ULL << (lg_n + rate);
+    uint64_t c = (mib << 20) / per_col;
+    c = c < 16 ? 16 : (c / 16) * 16;
+    return (uint32_t)(c < cols ? c : ((cols + 15) / 16) * 16);
+}
 
 uint32_t lde_rows_chunk_cols(uint32_t lg_n, uint32_t rate, uint64_t cols)
 {
-    const uint64_t per_col = 8ULL << (lg_n + rate);
-    uint64_t c = (tune_get("lde_chunk_mib", lg_n + rate, ZK_L2_CHUNK_MIB) << 20) / per_col;
-    c = c < 16 ? 16 : (c / 16) * 16;
-    return (uint32_t)(c < cols ? c : ((cols + 15) / 16) * 16);
+    return chunk_cols_for(tune_get("lde_chunk_mib", lg_n + rate, ZK_CHUNK_MIB), lg_n, rate, cols);
 }
 
 // ------------------------------------------------- explicit-table variant
@@ -392,7 +404,12 @@ void lde_rows_device(DeviceCtx &c, uint64_t *rows, const uint64_t *coeffs, uint3
     const uint64_t n = 1ULL << lg_n;
     if (cols == 0) return;
     const bool multi = plan_passes(lg_n, true).size() > 1;
-    const uint64_t chunk = multi ? lde_rows_chunk_cols(lg_n, rate, cols) : cols;
+    uint64_t chunk = multi ? lde_rows_chunk_cols(lg_n, rate, cols) : cols;
+    if (multi && host_coeffs) {
+        // never above the scratch sized by lde_rows_chunk_cols
+        const uint64_t h = chunk_cols_for(tune_get("lde_host_chunk_mib", lg_n + rate, ZK_HOST_CHUNK_MIB), lg_n, rate, cols);
+        chunk = h < chunk ? h : chunk;
+    }
     DevBuf tmp;
     if (multi && !scratch) {
         tmp.ctx = &c;

@@ -90,7 +90,8 @@ uint32_t ilog2_exact(uint64_t x);  // -1u if x is not a power of two
 // Tuning table: named knobs, optionally per log2 size, set by the autotuner
 // (zeknox_tune_set / zeknox_tune_load); tune_get falls back to the size-free
 // entry and then to `dflt`.  Knobs: "leaf_threads.<hash>" (64/128/256),
-// "lde_chunk_mib", "lde_last_logr" (1..8), "wide_level_nodes.<hash>".
+// "lde_chunk_mib", "lde_host_chunk_mib", "lde_last_logr" (1..8), "wide_level_nodes.<hash>",
+// "coop_leaves.<hash>".
 uint64_t tune_get(const std::string &name, uint32_t lg, uint64_t dflt);
 void tune_set(const std::string &name, uint32_t lg, uint64_t value);
 void tune_clear();
