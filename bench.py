@@ -62,7 +62,8 @@ class ClockSampler:
     def __init__(self, gpu_index):
         self.gpu = gpu_index
         self.proc = None
-        self.lines = []
+        self.lines = []  # (monotonic time, csv line)
+        self.window = None
 
     def start(self):
         try:
@@ -71,12 +72,22 @@ class ClockSampler:
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
+            # nvidia-smi takes a while to start sampling: wait for its first
+            # line so the timed region that follows is covered
+            t_end = time.monotonic() + 5.0
+            while not self.lines and time.monotonic() < t_end and self.proc.poll() is None:
+                time.sleep(0.01)
         except Exception:
             self.proc = None
 
     def _read(self):
         for line in self.proc.stdout:
-            self.lines.append(line.strip())
+            self.lines.append((time.monotonic(), line.strip()))
+
+    def mark(self, t0, t1):
+        """The timed region, in time.monotonic() seconds: only samples taken
+        inside it count (all samples when none fell inside)."""
+        self.window = (t0, t1)
 
     def stop(self):
         if not self.proc:
@@ -89,7 +100,11 @@ class ClockSampler:
         self.t.join(timeout=2)
         sm, mx, reasons = [], [], set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
+        lines = [ln for t, ln in self.lines]
+        if self.window:
+            inside = [ln for t, ln in self.lines if self.window[0] <= t <= self.window[1]]
+            lines = inside or lines
+        for ln in lines:
             f = [x.strip() for x in ln.split(",")]
             if len(f) < 9:
                 continue
@@ -200,12 +215,14 @@ def run_ours(args, rank, world):
     torch.cuda.synchronize()
     sampler.start()
     launches0 = zk.launch_count()
+    t_timed0 = time.monotonic()
     for s in range(args.steps):
         flush.fill_(s & 0xFF)  # evict the previous step's data from L2 (untimed)
         ev[s][0].record(stream)
         zk.commit(dev, job, stream=sptr)
         ev[s][1].record(stream)
     torch.cuda.synchronize()
+    sampler.mark(t_timed0, time.monotonic())
     launches = zk.launch_count() - launches0
     barrier()
     clocks = sampler.stop()
