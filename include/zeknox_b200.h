@@ -98,16 +98,21 @@ RustError zeknox_lde_rows_scatter(size_t device_id, uint64_t *const *dst_ptrs, u
 RustError zeknox_transpose_rev(size_t device_id, uint64_t *output, const uint64_t *input, uint32_t lg_n,
                                uint32_t cols, void *stream);
 
-/* zeknox_lde_rows for callers that cannot allocate device memory (code being
- * captured into a CUDA graph, code whose device memory is owned by another
- * allocator or arena).  No counterpart in the reference.  It never allocates:
- * its inter-pass scratch (32 MiB) and the tables it reads live in file-scope
- * device arrays that every GPU loading the library holds until exit.  Limit:
- * lg_n + rate_bits <= 18; larger sizes are rejected with
- * cudaErrorInvalidValue.  The first call on a device looks up those arrays'
- * addresses (make it before any stream capture).  All calls share the
- * scratch, so calls that overlap on the GPU race; stream NULL means the legacy
- * default stream and a synchronous call. */
+/* zeknox_lde_rows for callers that cannot allocate device memory: code whose
+ * device memory all belongs to another allocator (a framework's caching
+ * allocator, or an arena reserved at start-up) or a thread that must not enter
+ * the driver's allocator, which can synchronise the device.  No counterpart
+ * in the reference.  It never allocates: its inter-pass scratch (32 MiB) and
+ * the tables it reads live in file-scope device arrays that every GPU loading
+ * the library holds until exit.  Limit: lg_n + rate_bits <= 18; larger sizes
+ * are rejected with cudaErrorInvalidValue.  The first call on a device looks
+ * up those arrays' addresses and fills the twiddle tables, and waits for that
+ * on `stream`.  Every call rebuilds the coset table for its own shape and
+ * generator, ahead of its transform on the same stream.  All calls share the
+ * scratch and the coset table, so calls that overlap on the GPU race; stream
+ * NULL means the legacy default stream and a synchronous call.  A CUDA error
+ * pending from earlier work is reported (and left pending) instead of being
+ * taken for this call's. */
 RustError zeknox_lde_rows_noalloc(size_t device_id, uint64_t *rows, const uint64_t *coeffs, uint32_t lg_n,
                                   uint32_t rate_bits, uint32_t cols, uint64_t coset_gen, void *stream);
 

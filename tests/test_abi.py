@@ -99,3 +99,40 @@ def test_cpu_builder_rejects_bad_geometry():
         zk.load().fill_digests_buf_linear_cpu(zk._ptr(dig), zk._ptr(cap), zk._ptr(leaves), 26, 3, 16, 5, 1, 0)
         raise zk.ZeknoxError(1, zk.last_error() or "")
     assert "cap_buf_size" in zk.last_error()
+
+
+def _rejects(fn, *args):
+    """Call an entry point that must refuse its arguments before touching a GPU."""
+    e = fn(*args)
+    msg = ctypes.string_at(e.message).decode() if e.message else ""
+    if e.message:
+        zk._libc.free(e.message)
+    return e.code, msg
+
+
+@pytest.mark.parametrize("lg_n,rate", [(1, 0xFFFFFFFF), (0xFFFFFFFF, 1), (16, 0xFFFFFFF0), (31, 2), (33, 1)])
+def test_size_checks_do_not_wrap(lg_n, rate):
+    """lg_n + rate_bits in 32-bit arithmetic can wrap to a small value; each
+    term is checked on its own, so these sizes are refused with
+    cudaErrorInvalidValue (1) before any kernel could be launched."""
+    L = zk.load()
+    dummy = ctypes.c_void_p(16)  # never dereferenced: the checks come first
+    code, msg = _rejects(L.zeknox_lde_rows, 0, dummy, dummy, lg_n, rate, 4, 7, None)
+    assert code == 1 and "2^32" in msg, msg
+    code, msg = _rejects(L.zeknox_lde_rows_noalloc, 0, dummy, dummy, lg_n, rate, 4, 7, None)
+    assert code == 1 and "static limit" in msg, msg
+    cfg = zk.NTTConfig(batches=1, extension_rate_bits=rate, are_inputs_on_device=True, are_outputs_on_device=True)
+    code, msg = _rejects(L.compute_batched_lde, 0, dummy, dummy, lg_n, 0, cfg)
+    assert code == 1, msg
+    job = zk.CommitJob(lg_n=lg_n, rate_bits=rate, cols=4, cap_height=0, hash_type=0, input=16, leaves=16,
+                       digests=16, caps=16)
+    code, msg = _rejects(L.zeknox_commit, 0, ctypes.byref(job), None)
+    assert code == 1 and "2^32" in msg, msg
+
+
+def test_noalloc_refuses_beyond_its_static_limit():
+    L = zk.load()
+    dummy = ctypes.c_void_p(16)
+    for lg_n, rate in ((16, 3), (18, 1), (17, 2)):
+        code, msg = _rejects(L.zeknox_lde_rows_noalloc, 0, dummy, dummy, lg_n, rate, 4, 7, None)
+        assert code == 1 and "static limit" in msg, msg

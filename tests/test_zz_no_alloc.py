@@ -1,7 +1,9 @@
 """zeknox_lde_rows_noalloc: the fused LDE for callers that cannot allocate
-device memory (graph capture, foreign allocators).  It must give the same
-rows as zeknox_lde_rows, bit for bit, call after call, without changing the
-GPU's free memory once its first call has set it up.
+device memory (their device memory belongs to another allocator or a fixed
+arena, or their thread must not enter the driver's allocator).  Called through
+the C ABI, it must give the same rows as zeknox_lde_rows, bit for bit, call
+after call, without changing the GPU's free memory once its first call has set
+it up.
 
 Kept in its own file, collected last, so a stop-at-first-failure run has
 already run every other test if this one fails."""
@@ -36,6 +38,21 @@ def test_noalloc_matches_lde_rows_twice():
     assert torch.equal(ref, out)
     ref, out = _pair(11, 2, 24, 62)
     assert torch.equal(ref, out)
+
+
+def test_noalloc_shape_and_generator_changes():
+    # one shape, then another, then the first again, then the first with
+    # another coset generator: every call builds its own coset table, so none
+    # reads what the previous call left
+    for seed, (lg, rate, cols, gen) in enumerate(((12, 3, 20, 7), (9, 1, 16, 7), (12, 3, 20, 7), (12, 3, 20, 11),
+                                                   (12, 2, 17, 11), (12, 3, 20, 7))):
+        c = _dev(O.field_data(70 + seed, cols << lg))
+        ref = torch.zeros(cols << (lg + rate), dtype=torch.int64, device="cuda")
+        zk.lde_rows(0, ref, c, lg, rate, cols, coset_gen=gen)
+        out = torch.full_like(ref, -1)
+        zk.lde_rows_noalloc(0, out, c, lg, rate, cols, coset_gen=gen)
+        torch.cuda.synchronize()
+        assert torch.equal(ref, out), (lg, rate, cols, gen)
 
 
 def test_noalloc_allocates_nothing():

@@ -399,7 +399,9 @@ def lde_rows(device_id, rows, coeffs, lg_n, rate_bits, cols, coset_gen=7, stream
 
 def lde_rows_noalloc(device_id, rows, coeffs, lg_n, rate_bits, cols, coset_gen=7, stream=None):
     """zeknox_lde_rows_noalloc: the same result as lde_rows without allocating
-    device memory (static 32 MiB scratch; lg_n + rate_bits <= 18)."""
+    device memory (static 32 MiB scratch; lg_n + rate_bits <= 18), for callers
+    whose device memory belongs to another allocator or whose thread must not
+    enter the driver's allocator."""
     _check(load().zeknox_lde_rows_noalloc(device_id, _ptr(rows), _ptr(coeffs), lg_n, rate_bits, cols, coset_gen,
                                           ctypes.c_void_p(stream) if stream else None))
     return rows

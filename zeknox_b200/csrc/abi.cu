@@ -211,7 +211,8 @@ extern "C" RustError compute_batched_lde(size_t device_id, void *output, void *i
 {
     if (lg_domain_size == 0 || cfg.extension_rate_bits < 1) return fail((int)cudaErrorInvalidValue, "invalid args");
     return guarded([&] {
-        if (lg_domain_size + cfg.extension_rate_bits > 32) throw zk::arg_failure("extended size above 2^32");
+        if (cfg.extension_rate_bits > 32 || lg_domain_size > 32 - cfg.extension_rate_bits)
+            throw zk::arg_failure("extended size above 2^32");
         if ((!input && cfg.batches) || (!output && (cfg.batches + cfg.salt_size))) throw zk::arg_failure("null buffer");
         zk::DeviceCtx &c = zk::device(device_id);
         std::lock_guard<std::recursive_mutex> lk(c.mu);
@@ -228,7 +229,7 @@ extern "C" RustError compute_batched_lde_multi_gpu(void *output, void *input, ui
         return fail((int)cudaErrorInvalidValue, "invalid args");
     return guarded([&] {
         const uint32_t rate = cfg.extension_rate_bits;
-        if (lg_domain_size + rate > 32) throw zk::arg_failure("extended size above 2^32");
+        if (rate > 32 || lg_domain_size > 32 - rate) throw zk::arg_failure("extended size above 2^32");
         const uint64_t n = 1ULL << lg_domain_size, N = n << rate;
         if (total_num_input_elements < n * cfg.batches || total_num_output_elements < N * cfg.batches)
             throw zk::arg_failure("element counts smaller than batches x size");
@@ -305,7 +306,7 @@ extern "C" RustError zeknox_lde_rows_scatter(size_t device_id, uint64_t *const *
 {
     return guarded([&] {
         if (lg_n == 0 || rate_bits == 0 || cols == 0) throw zk::arg_failure("lg_n, rate_bits and cols must be >= 1");
-        if (lg_n + rate_bits > 32) throw zk::arg_failure("extended size above 2^32");
+        if (rate_bits > 32 || lg_n > 32 - rate_bits) throw zk::arg_failure("extended size above 2^32");
         if (!dst_ptrs || !coeffs) throw zk::arg_failure("null buffer");
         const uint32_t lg_dst = zk::ilog2_exact(n_dst);
         if (lg_dst == ~0u || lg_dst > lg_n + rate_bits)
@@ -608,7 +609,7 @@ extern "C" RustError zeknox_lde_rows(size_t device_id, uint64_t *rows, const uin
 {
     return guarded([&] {
         if (lg_n == 0 || rate_bits == 0 || cols == 0) throw zk::arg_failure("lg_n, rate_bits and cols must be >= 1");
-        if (lg_n + rate_bits > 32) throw zk::arg_failure("extended size above 2^32");
+        if (rate_bits > 32 || lg_n > 32 - rate_bits) throw zk::arg_failure("extended size above 2^32");
         if (!rows || !coeffs) throw zk::arg_failure("null buffer");
         zk::DeviceCtx &c = zk::device(device_id);
         std::lock_guard<std::recursive_mutex> lk(c.mu);

@@ -15,7 +15,7 @@ namespace zk {
 void check_job(const zk_commit_job &j)
 {
     if (j.lg_n == 0 || j.rate_bits == 0 || j.cols == 0) throw arg_failure("lg_n, rate_bits and cols must be >= 1");
-    if (j.lg_n + j.rate_bits > 32) throw arg_failure("extended size above 2^32");
+    if (j.rate_bits > 32 || j.lg_n > 32 - j.rate_bits) throw arg_failure("extended size above 2^32");
     if (j.cap_height > j.lg_n + j.rate_bits) throw arg_failure("cap_height above log2 of the leaf count");
     if (!j.input || !j.leaves || !j.caps || (!j.digests && j.cap_height < j.lg_n + j.rate_bits))
         throw arg_failure("null buffer");

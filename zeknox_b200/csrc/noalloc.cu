@@ -1,22 +1,27 @@
 // noalloc.cu -- zeknox_lde_rows_noalloc: the fused LDE for callers that
 // cannot allocate device memory.
 //
-// Some callers cannot call cudaMalloc at the point where they need the LDE:
-// code recording into a CUDA graph, code running under an allocator that owns
-// all device memory (a framework's caching allocator or a fixed arena), or a
-// host thread that must never block on the driver's allocator.  The regular
-// entry points take their temporaries and tables from the stream-ordered pool
-// and build tables on first use, which allocates.  This entry point instead
-// keeps everything it needs in file-scope device arrays that exist from the
-// moment the library's device code is loaded on a GPU until the process exits:
+// Some callers cannot call cudaMalloc where they need the LDE: code whose
+// device memory is all owned by another allocator (a framework's caching
+// allocator or an arena reserved at start-up, where a cudaMalloc fails or
+// fragments that arena), or a host thread on a latency-critical path that must
+// not enter the driver's allocator (cudaMalloc and cudaFree can synchronise
+// the device).  The regular entry points take their temporaries and tables
+// from the stream-ordered pool and build tables on first use, which allocates.
+// This entry point instead keeps everything it needs in file-scope device
+// arrays that exist from the moment the library's device code is loaded on a
+// GPU until the process exits:
 //   * scratch: NOALLOC_SCRATCH_WORDS words (32 MiB), the inter-pass buffer of
 //     one column chunk;
-//   * the twiddle tables w_{2^k}^t (k <= 18) and the coset table of the last
-//     shape used.
-// Limits: lg_n + rate_bits <= NOALLOC_MAX_LG (18).  The scratch is shared by
-// every call on a GPU and keeps the last call's contents (it needs no
-// clearing: each pass fully writes what the next pass reads); calls whose
-// work overlaps on the GPU race on it and on the coset table, so callers
+//   * the twiddle tables w_{2^k}^t for every k <= 18, filled once per device
+//     by the first call;
+//   * the coset table (g * w_N^c)^j, rebuilt by every call for its own shape
+//     and generator before its transform, so a call never depends on what an
+//     earlier call of another shape left there.
+// Limits: lg_n + rate_bits <= NOALLOC_MAX_LG (18).  The scratch and the coset
+// table are shared by every call on a GPU and keep the last call's contents
+// (the scratch needs no clearing: each pass fully writes what the next pass
+// reads); calls whose work overlaps on the GPU race on them, so callers
 // serialise them (one stream, or their own ordering).
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -46,13 +51,11 @@ static __device__ __align__(256) uint64_t g_noalloc_coset[1ULL << NOALLOC_MAX_LG
 const uint64_t H_OMEGA[33] = {ZK_OMEGA_LIST};
 
 // Per-device device addresses of the arrays above (host code may not use the
-// arrays' names as device pointers) and what the tables currently hold.
+// arrays' names as device pointers); set, with every twiddle table filled, by
+// the first call on the device.
 struct NoAllocState {
     bool ready = false;
     uint64_t *scratch = nullptr, *twiddles = nullptr, *coset = nullptr;
-    uint32_t tw_built = 0;  // bit k set: table of 2^k entries filled
-    uint32_t cos_lg = ~0u, cos_rate = ~0u;
-    uint64_t cos_gen = 0;
 };
 NoAllocState g_state[NOALLOC_MAX_DEVICES];
 std::mutex g_mu;
@@ -63,16 +66,27 @@ __global__ void noalloc_powers(uint64_t *tab, uint64_t count, uint64_t w)
         tab[t] = zk::gl_pow(w, t);
 }
 
+// tab[c * n + j] = (g * wN^c)^j: each thread fills a run of COSET_RUN
+// consecutive j with one exponentiation and then one multiply per entry.
+constexpr uint32_t COSET_RUN = 16;
 __global__ void noalloc_coset_powers(uint64_t *tab, uint64_t n, uint32_t cosets, uint64_t g, uint64_t wN)
 {
-    uint64_t total = n * cosets;
-    for (uint64_t k = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; k < total; k += (uint64_t)gridDim.x * blockDim.x) {
-        uint64_t c = k / n, j = k % n;
-        tab[k] = zk::gl_pow(zk::gl_mul(g, zk::gl_pow(wN, c)), j);
+    const uint64_t runs_per_coset = (n + COSET_RUN - 1) / COSET_RUN;
+    const uint64_t runs = runs_per_coset * cosets;
+    for (uint64_t k = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; k < runs; k += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t c = k / runs_per_coset, j0 = (k - c * runs_per_coset) * COSET_RUN;
+        const uint64_t base = zk::gl_mul(g, zk::gl_pow(wN, c));
+        uint64_t v = zk::gl_pow(base, j0);
+        for (uint32_t i = 0; i < COSET_RUN && j0 + i < n; i++) {
+            tab[c * n + j0 + i] = v;
+            v = zk::gl_mul(v, base);
+        }
     }
 }
 
 uint64_t *tw_table(NoAllocState &st, uint32_t k) { return st.twiddles + ((1ULL << k) - 1); }
+
+unsigned grid_for(uint64_t items) { return (unsigned)((items + 255) / 256 < 1024 ? (items + 255) / 256 : 1024); }
 
 void check(cudaError_t e, const char *what)
 {
@@ -90,15 +104,23 @@ extern "C" RustError zeknox_lde_rows_noalloc(size_t device_id, uint64_t *rows, c
     RustError r{0, nullptr};
     try {
         if (lg_n == 0 || rate_bits == 0 || cols == 0) throw zk::arg_failure("lg_n, rate_bits and cols must be >= 1");
-        if (lg_n + rate_bits > NOALLOC_MAX_LG)
-            throw zk::arg_failure("zeknox_lde_rows_noalloc: lg_n + rate_bits = " + std::to_string(lg_n + rate_bits) +
-                                  " exceeds the static limit of " + std::to_string(NOALLOC_MAX_LG));
+        // each term on its own first, so the sum below cannot wrap
+        if (rate_bits > NOALLOC_MAX_LG || lg_n > NOALLOC_MAX_LG - rate_bits)
+            throw zk::arg_failure("zeknox_lde_rows_noalloc: lg_n = " + std::to_string(lg_n) + " with rate_bits = " +
+                                  std::to_string(rate_bits) + " exceeds the static limit lg_n + rate_bits <= " +
+                                  std::to_string(NOALLOC_MAX_LG));
         if (!rows || !coeffs) throw zk::arg_failure("null buffer");
         if (device_id >= (size_t)NOALLOC_MAX_DEVICES) throw zk::arg_failure("device id out of range");
         int ndev = 0;
         check(cudaGetDeviceCount(&ndev), "cudaGetDeviceCount");
         if (device_id >= (size_t)ndev) throw zk::arg_failure("invalid device id");
         check(cudaSetDevice((int)device_id), "cudaSetDevice");
+        // an error left by earlier, unrelated work is reported as such (and
+        // left pending for its owner) rather than taken for one of ours
+        const cudaError_t pending = cudaPeekAtLastError();
+        if (pending != cudaSuccess)
+            throw zk::cuda_failure(-(int)pending, std::string("zeknox_lde_rows_noalloc: a CUDA error from earlier work "
+                                                              "is pending: ") + cudaGetErrorString(pending));
         cudaStream_t s = (cudaStream_t)stream;  // NULL: the legacy default stream
         const uint64_t gen = (coset_gen ? coset_gen : ZK_GENERATOR) % zk::GL_P;
 
@@ -106,35 +128,27 @@ extern "C" RustError zeknox_lde_rows_noalloc(size_t device_id, uint64_t *rows, c
         NoAllocState &st = g_state[device_id];
         if (!st.ready) {
             // one-time set-up on this device (with it current): device
-            // addresses of the file-scope arrays
-            check(cudaGetSymbolAddress((void **)&st.scratch, g_noalloc_scratch), "cudaGetSymbolAddress(scratch)");
-            check(cudaGetSymbolAddress((void **)&st.twiddles, g_noalloc_twiddles), "cudaGetSymbolAddress(twiddles)");
-            check(cudaGetSymbolAddress((void **)&st.coset, g_noalloc_coset), "cudaGetSymbolAddress(coset)");
-            st.ready = true;
-        }
-        // tables: filled by kernels into the static arrays, once per size
-        const uint64_t *tw[33] = {};
-        auto need = [&](uint32_t k) {
-            if (!(st.tw_built >> k & 1)) {
-                noalloc_powers<<<(unsigned)(((1ULL << k) + 255) / 256 < 1024 ? ((1ULL << k) + 255) / 256 : 1024), 256, 0,
-                                 s>>>(tw_table(st, k), 1ULL << k, H_OMEGA[k]);
+            // addresses of the file-scope arrays, then every twiddle table the
+            // size limit can use, finished before the call goes on
+            NoAllocState t;
+            check(cudaGetSymbolAddress((void **)&t.scratch, g_noalloc_scratch), "cudaGetSymbolAddress(scratch)");
+            check(cudaGetSymbolAddress((void **)&t.twiddles, g_noalloc_twiddles), "cudaGetSymbolAddress(twiddles)");
+            check(cudaGetSymbolAddress((void **)&t.coset, g_noalloc_coset), "cudaGetSymbolAddress(coset)");
+            for (uint32_t k = 0; k <= NOALLOC_MAX_LG; k++) {
+                noalloc_powers<<<grid_for(1ULL << k), 256, 0, s>>>(tw_table(t, k), 1ULL << k, H_OMEGA[k]);
                 check(cudaGetLastError(), "twiddle table");
-                st.tw_built |= 1u << k;
             }
-            tw[k] = tw_table(st, k);
-        };
-        need(12);
-        for (auto &p : zk::lde_rows_passes(lg_n))
-            if (p.first) need(p.first + p.second);
-        if (st.cos_lg != lg_n || st.cos_rate != rate_bits || st.cos_gen != gen) {
-            const uint64_t total = 1ULL << (lg_n + rate_bits);
-            noalloc_coset_powers<<<(unsigned)((total + 255) / 256 < 1024 ? (total + 255) / 256 : 1024), 256, 0, s>>>(
-                st.coset, 1ULL << lg_n, 1u << rate_bits, gen, H_OMEGA[lg_n + rate_bits]);
-            check(cudaGetLastError(), "coset table");
-            st.cos_lg = lg_n;
-            st.cos_rate = rate_bits;
-            st.cos_gen = gen;
+            check(cudaStreamSynchronize(s), "twiddle tables");
+            t.ready = true;
+            st = t;
         }
+        const uint64_t *tw[33] = {};
+        for (uint32_t k = 0; k <= NOALLOC_MAX_LG; k++) tw[k] = tw_table(st, k);
+        // this call's coset table, queued ahead of its transform
+        const uint64_t n = 1ULL << lg_n;
+        noalloc_coset_powers<<<grid_for(((n + COSET_RUN - 1) / COSET_RUN) << rate_bits), 256, 0, s>>>(
+            st.coset, n, 1u << rate_bits, gen, H_OMEGA[lg_n + rate_bits]);
+        check(cudaGetLastError(), "coset table");
         // column chunk so that the intermediate fits the static scratch
         const uint64_t N = 1ULL << (lg_n + rate_bits);
         uint64_t chunk = (NOALLOC_SCRATCH_WORDS / N) / 16 * 16;
