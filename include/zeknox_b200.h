@@ -170,6 +170,41 @@ uint64_t zeknox_tune_get(const char *name, uint32_t lg, uint64_t dflt);
 /* Load a table: one knob per line, "<name> <lg or *> <value>". */
 RustError zeknox_tune_load(const char *path);
 
+/* ---- Self-tests of the device arithmetic (no reference counterpart; the
+ * reference checks its primitives from a test binary, native/tests/tests.cu).
+ * The lazily reduced arithmetic of the hashes and the NTT takes its rare
+ * carry / borrow / wrap branches only near the field's edges (0, p - 1, 2^32
+ * neighbours, 2^64 - 2^32, the non-canonical range [p, 2^64)), which uniform
+ * data almost never reaches; these calls run the device primitives on chosen
+ * operands.  Device buffers; stream NULL: the device's stream, and the call
+ * waits.
+ *
+ * zeknox_field_selftest: for i < n, with x = a[i], y = b[i], z = c[i] (any
+ * 64-bit words; xc, yc = their canonical values), writes the canonical result
+ * of operation k to out[k * n + i], k < ZK_SELFTEST_OPS:
+ *   0 xc + yc            1 xc - yc           2 xc + yc (the NTT's butterfly sum)
+ *   3 x * y              4 x * y (lazy product, multiply-assisted reduction)
+ *   5 x * y (lazy product, ALU reduction)    6 x^2 (lazy, multiply-assisted)
+ *   7 x^2 (lazy, ALU)    8 x * y + z (lazy, multiply-assisted)   9 the same, ALU
+ *  10 x^7 (lazy S-box)  11 x^7 (lazy S-box with the squaring routine)
+ *  12 x * 2^(z mod 192) 13 x + yc (lazy sum)
+ *  14 4 (x y + y z + z x) through the 128-bit accumulator, multiply-assisted
+ *  15 the same, ALU     16 x + 5 y + 6 z (carry-counting sum)
+ *  17 4 (41 x + 39 y + 34 z) + yc (small-constant dot product)
+ *  18 p0 + 2^22 p1 + 2^44 p2 with p0, p1, p2 the low 28 bits of x, y, z
+ *  19 x + 2^64 y        20 x + 2^64 (y mod 2^32)      21 x * 2^(y mod 64) */
+#define ZK_SELFTEST_OPS 22
+RustError zeknox_field_selftest(size_t device_id, const uint64_t *a, const uint64_t *b, const uint64_t *c, uint64_t n,
+                                uint64_t *out, void *stream);
+
+/* One permutation of each of n states, in place: 12-word states for Poseidon
+ * (0), Poseidon-BN128 (2), Poseidon2 (3) and Monolith (4), lanes any 64-bit
+ * words in and canonical out; 25-word Keccak-f[1600] states for Keccak (1).
+ * cooperative != 0 runs the four-threads-per-state form the Merkle builder
+ * uses for narrow tree levels (Poseidon and Poseidon2 only). */
+RustError zeknox_permute(size_t device_id, uint64_t *states, uint64_t n, uint32_t hash_type, uint32_t cooperative,
+                         void *stream);
+
 /* Number of kernels this library has launched so far in the process. */
 uint64_t zeknox_launch_count(void);
 

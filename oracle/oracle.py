@@ -49,6 +49,7 @@ def lib():
         L.zko_hash_one.argtypes = [i, _u64p, u64, _u64p]
         L.zko_hash_two.argtypes = [i, _u64p, _u64p, _u64p]
         L.zko_permute.argtypes = [i, _u64p]
+        L.zko_keccak_f.argtypes = [_u64p]
         L.zko_merkle.argtypes = [_u64p, _u64p, _u64p, u64, u64, u64, u64, u64, i]
         L.zko_eval_poly.restype = u64
         L.zko_eval_poly.argtypes = [_u64p, u64, u64]
@@ -155,6 +156,14 @@ def permute(h, state):
     return s
 
 
+def keccak_f(state):
+    """Keccak-f[1600] of one 25-lane state; returns a new array."""
+    s = np.array(state, dtype=np.uint64, copy=True)
+    assert s.size == 25
+    lib().zko_keccak_f(_ptr(s))
+    return s
+
+
 def merkle_sizes(n_leaves, cap_height):
     n_caps = 1 << cap_height
     return 2 * (n_leaves - n_caps), n_caps
@@ -218,3 +227,39 @@ def field_data(seed, n):
         z = (z ^ (z >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
         z = z ^ (z >> np.uint64(31))
     return np.where(z >= np.uint64(P), z - np.uint64(P), z)
+
+
+# ----------------------------------------------------------- field corner cases
+
+# Operands at the edges of the lazily reduced arithmetic: 0 and small values,
+# the 2^32 neighbourhood (EPS = 2^32 - 1 = 2^64 mod p), 2^63, the top of the
+# canonical range (p - 2^32 and p - 1 = 2^64 - 2^32), and non-canonical words
+# in [p, 2^64).
+CORNERS = sorted({0, 1, 2, 3, 7, (1 << 31), (1 << 32) - 2, (1 << 32) - 1, 1 << 32, (1 << 32) + 1, (1 << 33) - 1,
+                  (1 << 63) - 1, 1 << 63, (1 << 63) + 1, P - (1 << 32) - 1, P - (1 << 32), P - (1 << 32) + 1, P - 3,
+                  P - 2, P - 1, P, P + 1, P + (1 << 31), (1 << 64) - (1 << 31), (1 << 64) - 3, (1 << 64) - 2,
+                  (1 << 64) - 1})
+CANONICAL_CORNERS = [v for v in CORNERS if v < P]
+
+
+def field_ops_expected(a, b, c):
+    """Exact values of the device self-test operations (ZK_SELFTEST_OPS rows,
+    include/zeknox_b200.h) for operand arrays a, b, c of any 64-bit words;
+    Python integers, so the arithmetic is the definition mod p."""
+    rows = [[] for _ in range(22)]
+    for x, y, z in zip((int(v) for v in a), (int(v) for v in b), (int(v) for v in c)):
+        xc, yc = x % P, y % P
+        lo28 = (1 << 28) - 1
+        vals = [
+            (xc + yc) % P, (xc - yc) % P, (xc + yc) % P,
+            x * y % P, x * y % P, x * y % P, x * x % P, x * x % P,
+            (x * y + z) % P, (x * y + z) % P, pow(x, 7, P), pow(x, 7, P),
+            x * pow(2, z % 192, P) % P, (x + yc) % P,
+            4 * (x * y + y * z + z * x) % P, 4 * (x * y + y * z + z * x) % P,
+            (x + 5 * y + 6 * z) % P, (4 * (41 * x + 39 * y + 34 * z) + yc) % P,
+            ((x & lo28) + ((y & lo28) << 22) + ((z & lo28) << 44)) % P,
+            (x + (y << 64)) % P, (x + ((y & 0xFFFFFFFF) << 64)) % P, x * (1 << (y % 64)) % P,
+        ]
+        for k, v in enumerate(vals):
+            rows[k].append(v)
+    return np.array(rows, dtype=np.uint64)

@@ -597,6 +597,9 @@ int zko_hash_two(int h, const u64 l[4], const u64 r[4], u64 out[4])
     return 0;
 }
 
+/* Keccak-f[1600] alone, 25 lanes in place (the permutation of keccak256 above). */
+void zko_keccak_f(u64 st[25]) { keccak_f(st); }
+
 int zko_permute(int h, u64 s[12])
 {
     if (h != H_POSEIDON && h != H_POSEIDON2 && h != H_MONOLITH && h != H_POSEIDON_BN128) return -1;

@@ -115,3 +115,23 @@ def test_init_entry_points():
     assert zk.get_number_of_gpus() >= 1
     zk.init_twiddle_factors(0, 16)
     zk.init_cuda_degree(20)
+
+
+def test_lde_multi_gpu_entry_matches_single():
+    """compute_batched_lde_multi_gpu on the GPUs present (one on this test's
+    machine) against compute_batched_lde, batches 1..9 at lg 17, rate 3, as the
+    reference's wrappers/rust/tests/ntt.rs:578-661 does: host input, output in
+    GPU 0's memory."""
+    lg, rate = 17, 3
+    ngpu = zk.get_number_of_gpus()
+    host = O.field_data(171, 9 << lg)
+    out = torch.zeros(9 << (lg + rate), dtype=torch.int64, device="cuda")
+    for batches in range(1, 10):
+        inp = torch.from_numpy(host[:batches << lg].view(np.int64).copy())
+        out.fill_(-1)
+        zk.lde_batch_multi_gpu(out, inp, ngpu, lg, batches, rate)
+        single = torch.zeros(batches << (lg + rate), dtype=torch.int64)
+        zk.lde_batch(0, single, inp, lg, batches, rate)
+        assert torch.equal(out[:batches << (lg + rate)].cpu(), single), batches
+    # and against the oracle on the last, largest call
+    assert np.array_equal(single.numpy().view(np.uint64), O.batched_lde(host, lg, rate, 9))

@@ -55,6 +55,15 @@ def median_ms(fn, flush, reps=3):
     return statistics.median(ts)
 
 
+def uniform_field(n, seed):
+    """n field elements uniform over all of [0, p), drawn on the device: 64-bit
+    words with the ones >= p (the int64 values in [-(2^32 - 1), -1]) folded by
+    subtracting p, which adds 2^32 - 1 modulo 2^64."""
+    g = torch.Generator(device="cuda").manual_seed(seed)
+    w = torch.randint(-(1 << 63), (1 << 63) - 1, (n,), dtype=torch.int64, device="cuda", generator=g)
+    return torch.where((w < 0) & (w >= -((1 << 32) - 1)), w + ((1 << 32) - 1), w)
+
+
 @pytest.mark.skipif(not os.path.exists(REF_GPU), reason="reference CUDA library not built (make -C oracle ref_gpu)")
 def test_headline_commit_matches_and_beats_reference_cuda_path():
     lg, rate, cols, cap, h = 15, 3, 256, 4, 3
@@ -62,8 +71,7 @@ def test_headline_commit_matches_and_beats_reference_cuda_path():
     R = ref_lib()
     assert R.init_twiddle_factors(0, lg + rate).code == 0
     assert R.init_coset(0, lg + rate, 7).code == 0
-    g = torch.Generator(device="cuda").manual_seed(11)
-    inp = torch.randint(0, 1 << 62, (cols * n,), dtype=torch.int64, device="cuda", generator=g)
+    inp = uniform_field(cols * n, 11)
     ev = torch.empty(cols * N, dtype=torch.int64, device="cuda")
     leaves = torch.empty(cols * N, dtype=torch.int64, device="cuda")
     n_dig, n_cap = zk.merkle_sizes(N, cap)
@@ -101,8 +109,7 @@ def test_forest_matches_and_beats_reference_cuda_path(h, n_leaves, leaf_size, ca
     fill_digests_buf_linear_gpu_with_gpu_ptr and this library's: identical
     digests and caps, and this library no slower."""
     R = ref_lib()
-    g = torch.Generator(device="cuda").manual_seed(100 + h)
-    leaves = torch.randint(0, 1 << 62, (n_leaves * leaf_size,), dtype=torch.int64, device="cuda", generator=g)
+    leaves = uniform_field(n_leaves * leaf_size, 100 + h)
     n_dig, n_cap = zk.merkle_sizes(n_leaves, cap)
     dig = torch.zeros(max(n_dig, 1) * 4, dtype=torch.int64, device="cuda")
     caps = torch.zeros(n_cap * 4, dtype=torch.int64, device="cuda")

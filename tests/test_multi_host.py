@@ -89,3 +89,35 @@ def test_partition_rules():
     sh = multi.split_subtrees(64, 8, 4)
     assert [s["caps"] for s in sh] == [(0, 2), (2, 2), (4, 2), (6, 2)]
     assert sh[1]["digests"] == (2 * 14, 2 * 14) and sh[1]["cap_height"] == 1
+
+
+def test_cxx_partition_matches_host_partition(tmp_path):
+    """The C++ partition the multi-GPU entry points use (multi_split.h), compiled
+    on its own, gives the same column runs and subtree GPU counts as the host
+    functions the process-group path uses, for 1..8 GPUs."""
+    import subprocess
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    src = tmp_path / "split.cpp"
+    src.write_text('#include <stdio.h>\n#include "multi_split.h"\n'
+                   'int main(){for(unsigned g=1;g<=8;g++)for(unsigned b=0;b<=40;b++){'
+                   'zk::ColumnSplit s=zk::split_columns(b,g);'
+                   'for(unsigned k=0;k<g;k++)printf("%u %u %u %llu %llu\\n",g,b,k,'
+                   '(unsigned long long)s.first[k],(unsigned long long)s.take[k]);}'
+                   'for(unsigned g=1;g<=8;g++)for(unsigned c=1;c<=256;c*=2)'
+                   'printf("m %u %u %llu\\n",g,c,(unsigned long long)zk::merkle_gpu_count(g,c));return 0;}\n')
+    exe = tmp_path / "split"
+    subprocess.run(["g++", "-std=c++17", "-I", os.path.join(root, "zeknox_b200", "csrc"), str(src), "-o", str(exe)],
+                   check=True)
+    lines = subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.splitlines()
+    n_cols = n_merkle = 0
+    for line in lines:
+        f = line.split()
+        if f[0] == "m":
+            g, c, count = map(int, f[1:])
+            assert count == multi.merkle_gpus(c, g), line
+            n_merkle += 1
+        else:
+            g, b, k, first, take = map(int, f)
+            assert (first, take) == multi.split_columns(b, g)[k], line
+            n_cols += 1
+    assert n_cols == sum(g * 41 for g in range(1, 9)) and n_merkle == 8 * 9

@@ -22,6 +22,7 @@ LIB_PATH = os.path.join(HERE, "libzeknox.so")
 P = 0xFFFFFFFF00000001
 HASH_POSEIDON, HASH_KECCAK, HASH_POSEIDON_BN128, HASH_POSEIDON2, HASH_MONOLITH = 0, 1, 2, 3, 4
 FORWARD, INVERSE = 0, 1
+SELFTEST_OPS = 22  # ZK_SELFTEST_OPS of include/zeknox_b200.h
 
 # Exported C symbols (include/lib.h, include/merkle/merkle.h, include/zeknox_b200.h).
 ABI_SYMBOLS = [
@@ -37,7 +38,7 @@ EXT_SYMBOLS = ["zeknox_last_error", "zeknox_commit", "zeknox_commit_batch", "zek
                "zeknox_lde_rows_noalloc", "zeknox_server_create", "zeknox_server_submit", "zeknox_server_wait",
                "zeknox_server_release", "zeknox_server_stats", "zeknox_server_destroy", "zeknox_tune_set",
                "zeknox_tune_get", "zeknox_tune_clear", "zeknox_tune_load", "zeknox_transpose_rev",
-               "zeknox_lde_rows_scatter"]
+               "zeknox_lde_rows_scatter", "zeknox_field_selftest", "zeknox_permute"]
 
 # Tuning table measured on B200 by ``python -m zeknox_b200.autotune``; loaded
 # by load() unless ZEKNOX_TUNE_FILE names another table ("" or "none": no table).
@@ -194,6 +195,10 @@ def load():
     L.zeknox_merkle_batch.restype = RustError
     L.zeknox_merkle_batch.argtypes = [sz, ctypes.POINTER(MerkleJob), u32]
     L.zeknox_lde_rows_scatter.restype = RustError
+    L.zeknox_field_selftest.restype = RustError
+    L.zeknox_field_selftest.argtypes = [sz, vp, vp, vp, u64, vp, vp]
+    L.zeknox_permute.restype = RustError
+    L.zeknox_permute.argtypes = [sz, vp, u64, u32, u32, vp]
     L.zeknox_lde_rows_scatter.argtypes = [sz, ctypes.POINTER(ctypes.c_void_p), u32, vp, u32, u32, u32, u32, u32, u64, vp]
     L.zeknox_transpose_rev.restype = RustError
     L.zeknox_transpose_rev.argtypes = [sz, vp, vp, u32, u32, vp]
@@ -416,6 +421,26 @@ def lde_rows_scatter(device_id, dst, coeffs, lg_n, rate_bits, cols, col_offset, 
     arr = (ctypes.c_void_p * len(ptrs))(*ptrs)
     _check(load().zeknox_lde_rows_scatter(device_id, arr, len(ptrs), _ptr(coeffs), lg_n, rate_bits, cols, col_offset,
                                           row_stride, coset_gen, ctypes.c_void_p(stream) if stream else None))
+
+
+def field_selftest(device_id, a, b, c, out, stream=None):
+    """zeknox_field_selftest: the device field primitives on operand arrays
+    a, b, c (n words each); out holds SELFTEST_OPS * n words, op-major."""
+    n = a.numel()
+    assert b.numel() == n and c.numel() == n and out.numel() >= SELFTEST_OPS * n
+    _check(load().zeknox_field_selftest(device_id, _ptr(a), _ptr(b), _ptr(c), n, _ptr(out),
+                                        ctypes.c_void_p(stream) if stream else None))
+    return out
+
+
+def permute(device_id, states, hash_type, cooperative=False, stream=None):
+    """zeknox_permute: one permutation of every state in place (12 words per
+    state; 25 for Keccak-f)."""
+    width = 25 if hash_type == HASH_KECCAK else 12
+    assert states.numel() % width == 0
+    _check(load().zeknox_permute(device_id, _ptr(states), states.numel() // width, hash_type, int(bool(cooperative)),
+                                 ctypes.c_void_p(stream) if stream else None))
+    return states
 
 
 def transpose_rev(device_id, output, inp, lg_n, cols, stream=None):

@@ -9,13 +9,17 @@
 #include <stdlib.h>
 #include <string.h>
 
+#include <exception>
 #include <string>
+#include <thread>
+#include <vector>
 
 #include "../../include/lib.h"
 #include "../../include/zeknox_b200.h"
 #include "batch.cuh"
 #include "geom.h"
 #include "gl64.cuh"
+#include "multi_split.h"
 #include "ntt_api.cuh"
 #include "runtime.cuh"
 #include "zk_constants.h"
@@ -83,6 +87,33 @@ struct Staged {
         }
     }
 };
+
+// fn(g) for g < gpus, each on its own host thread so that every GPU's copies
+// and kernels are issued at once (the reference issues all GPUs before it
+// waits, native/ntt/ntt.cu:339-447, and runs one OpenMP thread per GPU,
+// native/merkle/merkle.cu:392-451); the first failure is rethrown after all
+// threads have finished.
+template <class F>
+void on_each_gpu(uint32_t gpus, F &&fn)
+{
+    if (gpus == 1) {
+        fn(0u);
+        return;
+    }
+    std::vector<std::exception_ptr> errs(gpus);
+    std::vector<std::thread> threads;
+    for (uint32_t g = 0; g < gpus; g++)
+        threads.emplace_back([&, g] {
+            try {
+                fn(g);
+            } catch (...) {
+                errs[g] = std::current_exception();
+            }
+        });
+    for (auto &t : threads) t.join();
+    for (auto &e : errs)
+        if (e) std::rethrow_exception(e);
+}
 
 }  // namespace
 
@@ -236,34 +267,30 @@ extern "C" RustError compute_batched_lde_multi_gpu(void *output, void *input, ui
         int ngpu = zk::device_count();
         uint32_t G = num_gpu == 0 ? 1 : num_gpu;
         if ((int)G > ngpu) throw zk::arg_failure("num_gpu exceeds the GPUs present");
-        // columns split as in the reference: the first (batches % G) GPUs take one more
-        std::vector<uint64_t> take(G), first(G);
-        uint64_t acc = 0;
-        for (uint32_t g = 0; g < G; g++) {
-            take[g] = cfg.batches / G + (g < cfg.batches % G ? 1 : 0);
-            first[g] = acc;
-            acc += take[g];
-        }
-        NTT_Config sub = cfg;
-        sub.are_inputs_on_device = false;  // host input (ntt.cu:360-364)
-        sub.are_outputs_on_device = true;
-        sub.salt_size = 0;
-        for (uint32_t g = 0; g < G; g++) {
-            if (!take[g]) continue;
+        const zk::ColumnSplit sp = zk::split_columns(cfg.batches, G);
+        // input in host memory (ntt.cu:360-364), output on GPU 0; every GPU
+        // stages, transforms and copies its columns concurrently
+        on_each_gpu(G, [&](uint32_t g) {
+            if (!sp.take[g]) return;
             zk::DeviceCtx &c = zk::device(g);
             std::lock_guard<std::recursive_mutex> lk(c.mu);
-            sub.batches = (uint32_t)take[g];
-            uint64_t *dst = (uint64_t *)output + first[g] * N;
+            NTT_Config sub = cfg;
+            sub.are_inputs_on_device = false;
+            sub.are_outputs_on_device = true;
+            sub.salt_size = 0;
+            sub.batches = (uint32_t)sp.take[g];
+            uint64_t *dst = (uint64_t *)output + sp.first[g] * N;
+            uint64_t *src = (uint64_t *)input + sp.first[g] * n;
             if (g == 0) {
-                lde_on(c, dst, (uint64_t *)input + first[g] * n, lg_domain_size, ntt_direction, sub);
+                lde_on(c, dst, src, lg_domain_size, ntt_direction, sub);
             } else {
-                // compute on GPU g, then copy into GPU 0's output buffer
-                zk::DevBuf tmp(c, take[g] * N);
-                lde_on(c, tmp.p, (uint64_t *)input + first[g] * n, lg_domain_size, ntt_direction, sub);
-                ZK_CUDA(cudaMemcpyPeerAsync(dst, 0, tmp.p, g, take[g] * N * 8, c.stream));
+                // computed on GPU g, then copied into GPU 0's output buffer
+                zk::DevBuf tmp(c, sp.take[g] * N);
+                lde_on(c, tmp.p, src, lg_domain_size, ntt_direction, sub);
+                ZK_CUDA(cudaMemcpyPeerAsync(dst, 0, tmp.p, (int)g, sp.take[g] * N * 8, c.stream));
                 c.sync();
             }
-        }
+        });
     });
 }
 
@@ -383,38 +410,34 @@ extern "C" void fill_digests_buf_linear_multigpu_with_gpu_ptr(void *digests_buf_
         return;
     }
     RustError e = guarded([&] {
-        int ngpu = zk::device_count();
-        // largest power of two of GPUs that divides the caps: each GPU builds a
-        // contiguous run of whole subtrees (merkle.cu:381-438 does one per GPU)
-        uint64_t G = 1;
-        while (G * 2 <= (uint64_t)ngpu && G * 2 <= cap_buf_size) G *= 2;
+        const uint64_t G = zk::merkle_gpu_count((uint64_t)zk::device_count(), cap_buf_size);
         const uint64_t L = leaves_buf_size / cap_buf_size, D = 2 * L - 2;
         const uint64_t caps_g = cap_buf_size / G;
         uint32_t hg = 0;
         while ((1ULL << hg) < caps_g) hg++;
-        if (G == 1) {
-            zk::DeviceCtx &c = zk::device(0);
-            std::lock_guard<std::recursive_mutex> lk(c.mu);
-            std::string e2;
-            if (!zk::merkle_device((uint64_t *)digests_buf_gpu_ptr, (uint64_t *)cap_buf_gpu_ptr,
-                                   (const uint64_t *)leaves_buf_gpu_ptr, digests_buf_size, cap_buf_size,
-                                   leaves_buf_size, leaf_size, cap_height, hash_type, c.stream, e2))
-                throw zk::arg_failure(e2);
-            c.sync();
-            return;
-        }
-        for (uint64_t g = 0; g < G; g++) {
+        // GPU g builds subtrees [g * caps_g, (g + 1) * caps_g) from leaves
+        // copied into its own memory (remote data lands locally before any
+        // kernel reads it) and copies its digests and caps back to GPU 0; all
+        // GPUs at once
+        on_each_gpu((uint32_t)G, [&](uint32_t g) {
             zk::DeviceCtx &c = zk::device(g);
             std::lock_guard<std::recursive_mutex> lk(c.mu);
             const uint64_t leaves_g = caps_g * L, dig_g = caps_g * D;
             const uint64_t *src_leaves = (const uint64_t *)leaves_buf_gpu_ptr + g * leaves_g * leaf_size;
             uint64_t *dst_dig = (uint64_t *)digests_buf_gpu_ptr + g * dig_g * 4;
             uint64_t *dst_cap = (uint64_t *)cap_buf_gpu_ptr + g * caps_g * 4;
+            if (G == 1) {
+                std::string e2;
+                if (!zk::merkle_device(dst_dig, dst_cap, src_leaves, digests_buf_size, cap_buf_size, leaves_buf_size,
+                                       leaf_size, cap_height, hash_type, c.stream, e2))
+                    throw zk::arg_failure(e2);
+                c.sync();
+                return;
+            }
             zk::DevBuf lv(c, g ? leaves_g * leaf_size : 0), dg(c, g ? dig_g * 4 : 0), cp(c, g ? caps_g * 4 : 0);
             const uint64_t *use_leaves = src_leaves;
             uint64_t *use_dig = dst_dig, *use_cap = dst_cap;
             if (g) {
-                // remote data lands in this GPU's memory before any kernel reads it
                 ZK_CUDA(cudaMemcpyPeerAsync(lv.p, (int)g, src_leaves, 0, leaves_g * leaf_size * 8, c.stream));
                 use_leaves = lv.p;
                 use_dig = dg.p;
@@ -429,7 +452,7 @@ extern "C" void fill_digests_buf_linear_multigpu_with_gpu_ptr(void *digests_buf_
                 ZK_CUDA(cudaMemcpyPeerAsync(dst_cap, 0, cp.p, (int)g, caps_g * 32, c.stream));
             }
             c.sync();
-        }
+        });
     });
     if (e.code) {
         record_error("fill_digests_buf_linear_multigpu_with_gpu_ptr", e.message ? e.message : "error");

@@ -21,7 +21,7 @@ namespace zk {
 #ifdef __CUDACC__
 // the multiply is large (~130 multiply-adds): one out-of-line copy keeps the
 // permutation's code within the instruction cache
-#define ZK_FR_NOINLINE __host__ __device__ __noinline__
+#define ZK_FR_NOINLINE static __host__ __device__ __noinline__
 #define ZK_FR_HD __host__ __device__ __forceinline__
 #else
 #define ZK_FR_NOINLINE static
