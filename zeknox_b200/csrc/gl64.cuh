@@ -353,10 +353,11 @@ ZK_HD uint64_t gl_sqr(uint64_t a) { return gl_canon(gl_sqr_nc(a)); }
 // 2^(s mod 32) -- the multiply pipe, which the NTT passes leave mostly idle,
 // instead of 64-bit shifts on the integer ALU they are bound by -- and the
 // reduction knows which limbs are zero: for s < 32 the value is below 2^96
-// (lo + EPS * r2), for s >= 32 its low word is 0.
+// (lo + EPS * r2), for s >= 32 its low word is 0.  a may be any 64-bit word
+// (like gl_mul); the result is canonical.
 ZK_HD uint64_t gl_mul_pow2_lt64(uint64_t a, unsigned s)
 {
-    if (s == 0) return a;
+    if (s == 0) return gl_canon(a);
 #ifdef __CUDA_ARCH__
     const uint32_t m = 1u << (s & 31);
     uint32_t q0, q1, q2;  // a * m = q0 + 2^32 q1 + 2^64 q2
@@ -413,7 +414,8 @@ ZK_HD uint64_t gl_mul_pow2_lt64(uint64_t a, unsigned s)
 #endif
 }
 
-// a * 2^s for any s (taken mod 192, the order of 2).  2^96 = -1 turns
+// a * 2^s for any s (taken mod 192, the order of 2) and any 64-bit word a;
+// canonical result.  2^96 = -1 turns
 // s >= 96 into a negation; for 64 <= s < 96, 2^s = 2^(s-32) - 2^(s-64)
 // because 2^64 = 2^32 - 1.
 ZK_HD uint64_t gl_mul_pow2(uint64_t a, unsigned s)
