@@ -31,6 +31,7 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
+REPO_ROOT = ROOT
 sys.path.insert(0, ROOT)
 from oracle import oracle as O  # noqa: E402
 
@@ -70,7 +71,8 @@ def block_after(src, marker):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", default=os.environ.get("ZEKNOX_REFERENCE_DIR", os.path.join(REPO_ROOT, "..", "reference")),
+                    help="the reference tree (default: $ZEKNOX_REFERENCE_DIR, else ../reference beside this repository)")
     args = ap.parse_args()
     tests = open(os.path.join(args.ref, "native/tests/tests.cu")).read()
     params = open(os.path.join(args.ref, "native/ff/gl64_params.hpp")).read()

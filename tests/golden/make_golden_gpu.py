@@ -6,7 +6,7 @@ The reference has no CPU NTT, so the NTT family is pinned by running its CUDA
 path (native/lib.cu compute_batched_ntt / compute_batched_lde /
 compute_transpose_rev, rebuilt for sm_100a by ``make -C oracle ref_gpu`` into
 oracle/_ref/libzeknox_ref_gpu.so) on the same seeded inputs the tests use.
-Outputs go to <out> (default gpurun_out/golden_gpu.npz); small results are
+Outputs go to <out> (default golden_gpu_new.npz in the working directory); small results are
 stored whole, large ones as sha256 of their bytes.  The committed copy is
 tests/golden/golden_gpu.npz.
 
@@ -51,7 +51,7 @@ def store(out, key, arr):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--out", default=os.path.join(ROOT, "gpurun_out", "golden_gpu.npz"))
+    ap.add_argument("--out", default="golden_gpu_new.npz")
     args = ap.parse_args()
     R = ctypes.CDLL(os.path.join(ROOT, "oracle", "_ref", "libzeknox_ref_gpu.so"))
     R.init_twiddle_factors.restype = zk.RustError

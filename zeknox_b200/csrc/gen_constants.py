@@ -37,6 +37,7 @@ import re
 import sys
 
 P = 0xFFFFFFFF00000001
+REPO_ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
 ROOT_2_32 = 1753635133440165772  # primitive 2^32-th root of unity (Plonky2)
 GENERATOR = 7
 
@@ -296,7 +297,8 @@ def fmt_list(name, vals, per_line=4, hexw=16):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", default=os.environ.get("ZEKNOX_REFERENCE_DIR", os.path.join(REPO_ROOT, "..", "reference")),
+                    help="the reference tree (default: $ZEKNOX_REFERENCE_DIR, else ../reference beside this repository)")
     ap.add_argument("--out", default=os.path.join(os.path.dirname(os.path.abspath(__file__)), "zk_constants.h"))
     args = ap.parse_args()
 

@@ -16,11 +16,13 @@ subtrees need whole leaf rows):
 Exchange volume per rank: N * cols * 8 * (G - 1) / G bytes for G hashing
 ranks.
 
-``commit_distributed_p2p`` fuses steps 1 and 2: every hashing rank exposes its
-row shard as symmetric memory, and each rank's row-writing LDE kernel stores
-its columns of every row straight into the owning rank's shard
-(``zeknox_lde_rows_scatter``: plain P2P stores over NVLink, no staging buffer,
-no separate collective), so the exchange overlaps the transform tile by tile.
+``commit_distributed_p2p`` fuses steps 1 and 2: every hashing rank exports its
+row shard with a CUDA IPC handle, every other rank maps it, and each rank's
+row-writing LDE kernel stores its columns of every row straight into the
+owning rank's shard (``zeknox_lde_rows_scatter``: plain P2P stores over
+NVLink, no staging buffer, no separate collective), so the exchange overlaps
+the transform tile by tile.  The shards are ordinary device allocations: no
+NVLink multicast object is created or bound.
 
 zeknox itself has no multi-process commit: its multi-GPU entry points
 (native/ntt/ntt.cu:315-471, native/merkle/merkle.cu:283-499) drive several GPUs
@@ -124,16 +126,38 @@ def commit_distributed(coeffs, lg_n, rate_bits, cols, cap_height, hash_type, cos
     return commit_sharded(coeffs, lg_n, rate_bits, cols, cap_height, lde, merkle, group=group)
 
 
+def _mapped_shards(buf, G, group):
+    """Device addresses, in this process, of the G hashing ranks' row shards.
+    Each owner exports its shard (``buf`` on ranks < G) as a CUDA IPC handle
+    (cudaIpcGetMemHandle, through torch's CUDA tensor sharing); every rank
+    maps the others' shards (cudaIpcOpenMemHandle).  Returns the addresses and
+    the mapped tensors, which must stay alive while the addresses are used."""
+    from torch.multiprocessing.reductions import reduce_tensor
+
+    world = dist.get_world_size(group)
+    rank = dist.get_rank(group)
+    handles = [None] * world
+    dist.all_gather_object(handles, reduce_tensor(buf) if rank < G else None, group=group)
+    ptrs, keep = [], []
+    for r in range(G):
+        if r == rank:
+            ptrs.append(buf.data_ptr())
+        else:
+            rebuild, args = handles[r]
+            t = rebuild(*args)
+            keep.append(t)
+            ptrs.append(t.data_ptr())
+    return ptrs, keep
+
+
 def commit_distributed_p2p(coeffs, lg_n, rate_bits, cols, cap_height, hash_type, coset_gen=7, group=None,
                            device_id=None):
     """The distributed commit with the row exchange fused into the LDE: the
-    hashing ranks' row shards are symmetric memory (torch.distributed
-    symmetric memory, mapped into every rank's address space), every rank's
-    ``zeknox_lde_rows_scatter`` writes its columns of each row directly into
-    the owner's shard, then a host barrier and the local forests as in
-    ``commit_distributed``.  Same arguments and results."""
-    import torch.distributed._symmetric_memory as symm_mem
-
+    hashing ranks' row shards are mapped into every rank's address space by
+    CUDA IPC handles, every rank's ``zeknox_lde_rows_scatter`` writes its
+    columns of each row directly into the owner's shard, then a host barrier
+    and the local forests as in ``commit_distributed``.  Same arguments and
+    results."""
     from . import fill_digests_buf_linear_gpu, lde_rows_scatter, merkle_sizes
 
     if not coeffs.is_cuda:
@@ -147,9 +171,8 @@ def commit_distributed_p2p(coeffs, lg_n, rate_bits, cols, cap_height, hash_type,
     c0, k = shards[rank]
     G = merkle_gpus(n_caps, world)
     rows_per = N // G
-    buf = symm_mem.empty(rows_per * cols, dtype=torch.int64, device=coeffs.device)
-    hdl = symm_mem.rendezvous(buf, group if group is not None else dist.group.WORLD)
-    ptrs = [int(p) for p in hdl.buffer_ptrs][:G]
+    buf = torch.empty(rows_per * cols if rank < G else 0, dtype=torch.int64, device=coeffs.device)
+    ptrs, mapped = _mapped_shards(buf, G, group)
     if k:
         lde_rows_scatter(dev, ptrs, coeffs, lg_n, rate_bits, k, c0, cols, coset_gen)  # waits for its kernels
     torch.cuda.synchronize(coeffs.device)
@@ -169,6 +192,8 @@ def commit_distributed_p2p(coeffs, lg_n, rate_bits, cols, cap_height, hash_type,
         my_caps = torch.zeros(caps_g * 4, dtype=torch.int64, device=coeffs.device)
     gathered = [torch.empty(caps_g * 4, dtype=torch.int64, device=coeffs.device) for _ in range(world)]
     dist.all_gather(gathered, my_caps, group=group)
-    # no rank may reuse or free its shard while another rank could still be writing it
+    # no rank may reuse or free its shard while another rank could still be
+    # writing it or still holds its mapping
+    del mapped
     dist.barrier(group=group)
     return torch.cat(gathered[:G]), digests, leaves
