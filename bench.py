@@ -11,6 +11,13 @@ Synthetic seeded field data (splitmix64, values in [0, p)).
 
 For N > 1 run under torchrun; every rank commits its own job (weak scaling,
 no data-path collective).  Rank 0 prints one JSON line.
+
+At N = 1 the same line also carries the uneven batch (64 jobs, one CUDA graph
+per memory wave vs one plain C-ABI call per stage per job: batched_over_plain,
+batched_elems_per_s, plain_elems_per_s, and the batch's Poseidon permutation
+floor) and the serving stream (Poisson requests at 0.7 of the serial capacity:
+serve_p50_ms, serve_p99_ms, delivered and offered elements/s); --no-extras
+skips them.
 """
 import argparse
 import json
@@ -303,7 +310,6 @@ def run_ours(args, rank, world):
         torch.cuda.synchronize()
         if s:
             tr_ms.append(a.elapsed_time(b))
-    del ev_cols
     tr_t = statistics.median(tr_ms) * 1e-3
     tr_bytes = 16 * N * COLS
     roofline_transpose = {"bound": "hbm", "kernel": "transpose_rev_kernel (compute_transpose_rev, 256 x 2^18)",
@@ -326,6 +332,22 @@ def run_ours(args, rank, world):
                "sample": "one commit of %d cols x 2^%d coeffs (rate 3, Poseidon2 cap 4): LDE by the CPU restatement, "
                          "Merkle by %s" % (COLS, args.cpu_lg, "the reference's fill_digests_buf_linear_cpu"
                                            if kind == "reference" else "the oracle port")}
+    # the uneven batch (batched graph vs plain per-call) and the serving
+    # stream, on this GPU after the headline (one GPU only: they are
+    # single-GPU workloads)
+    extras = {}
+    if rank == 0 and world == 1 and not args.no_extras:
+        del ev_cols
+        torch.cuda.empty_cache()
+        batch = measure_batch(args.batch_steps, args.budget_gb)
+        serve = measure_serve(args.requests)
+        extras = {"batched_over_plain": batch["batched_over_plain"],
+                  "batched_elems_per_s": batch["batched_elems_per_s"],
+                  "plain_elems_per_s": batch["plain_elems_per_s"],
+                  "serve_p50_ms": serve["p50_ms"], "serve_p99_ms": serve["p99_ms"],
+                  "serve_delivered_elems_per_s": serve["delivered_elems_per_s"],
+                  "serve_offered_elems_per_s": serve["offered_elems_per_s"],
+                  "uneven_batch": batch, "serving": serve}
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": "elems/s", "n_gpus": world, "steps": args.steps,
@@ -337,6 +359,7 @@ def run_ours(args, rank, world):
                     "d2h_bytes_per_step": n_cap * 32},
             "gpu_launches": launches, "clocks": clocks,
             "stage_ms": {"lde_rows": lde_t * 1e3, "merkle": mk_t * 1e3},
+            **extras,
         }
         print(json.dumps(line), flush=True)
 
@@ -389,15 +412,49 @@ def uneven_jobs(count=64, seed=3):
     return jobs
 
 
-def run_batch(args):
-    """Uneven batch: one graph per memory wave (batched) vs one synchronous C-ABI
-    call per stage per job (plain: compute_batched_lde -> compute_transpose_rev ->
-    fill_digests_buf_linear_gpu_with_gpu_ptr)."""
+def perms_of(n_leaves, leaf_size, cap_height):
+    """Permutations of a width-12 sponge forest: ceil(leaf_size / 8) per leaf
+    (none for leaves of <= 4 elements), one per internal node."""
+    leaf = n_leaves * ((leaf_size + 7) // 8) if leaf_size > 4 else 0
+    return leaf + n_leaves - (1 << cap_height)
+
+
+def poseidon_perm_rate(steps=3):
+    """Poseidon permutations/s of one 2^20 x 135 forest, cap height 4 (CUDA
+    events, L2 flushed): the throughput the uneven batch's floor is taken at."""
     import torch
     import zeknox_b200 as zk
-    torch.cuda.set_device(0)
+    nl, ls, ch = 1 << 20, 135, 4
+    leaves = dev_field(nl * ls, 77)
+    n_dig, n_cap = zk.merkle_sizes(nl, ch)
+    dig = torch.empty(n_dig * 4, dtype=torch.int64, device="cuda")
+    caps = torch.empty(n_cap * 4, dtype=torch.int64, device="cuda")
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    zk.fill_digests_buf_linear_gpu(dig, caps, leaves, nl, ls, ch, 0)
+    ts = []
+    for s in range(steps):
+        flush.fill_(s & 0xFF)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        zk.fill_digests_buf_linear_gpu(dig, caps, leaves, nl, ls, ch, 0)
+        b.record()
+        torch.cuda.synchronize()
+        ts.append(a.elapsed_time(b))
+    del leaves, dig, caps, flush
+    torch.cuda.empty_cache()
+    return perms_of(nl, ls, ch) / (statistics.median(ts) * 1e-3)
+
+
+def measure_batch(steps, budget_gb):
+    """Uneven batch: one graph per memory wave (batched) vs one synchronous C-ABI
+    call per stage per job (plain: compute_batched_lde -> compute_transpose_rev ->
+    fill_digests_buf_linear_gpu_with_gpu_ptr), same jobs, same buffers, caps
+    compared.  Also the batch's Poseidon permutation count at the measured
+    forest rate: no schedule of these jobs on these kernels beats that time."""
+    import torch
+    import zeknox_b200 as zk
     jobs = uneven_jobs()
-    budget = int(args.budget_gb * (1 << 30))
+    budget = int(budget_gb * (1 << 30))
     waves, cur, used = [], [], 0
     for jb in jobs:
         n, N = 1 << jb["lg_n"], 1 << (jb["lg_n"] + jb["rate"])
@@ -409,7 +466,8 @@ def run_batch(args):
         used += need
     waves.append(cur)
     total_elems = sum((1 << (j["lg_n"] + j["rate"])) * j["cols"] for j in jobs)
-    t_batch, t_plain, max_job = 0.0, 0.0, 0
+    total_perms = sum(perms_of(1 << (j["lg_n"] + j["rate"]), j["cols"], j["cap"]) for j in jobs)
+    t_batch, t_plain = 0.0, 0.0
     for wave in waves:
         bufs, cjobs = [], []
         for jb in wave:
@@ -421,19 +479,18 @@ def run_batch(args):
             caps = torch.empty(n_cap * 4, dtype=torch.int64, device="cuda")
             bufs.append((inp, leaves, dig, caps, n_dig, n_cap))
             cjobs.append(zk.commit_job(jb["lg_n"], jb["rate"], jb["cols"], jb["cap"], jb["hash"], inp, leaves, dig, caps))
-            max_job = max(max_job, N * jb["cols"])
         zk.commit_batch(0, cjobs)  # capture
         torch.cuda.synchronize()
         caps_b = [b[3].clone() for b in bufs]
         a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        for _ in range(args.steps):
+        for _ in range(steps):
             a.record()
             zk.commit_batch(0, cjobs)
             b.record()
             torch.cuda.synchronize()
-            t_batch += a.elapsed_time(b) / args.steps
+            t_batch += a.elapsed_time(b) / steps
         # plain path, same jobs and buffers
-        for _ in range(args.steps):
+        for _ in range(steps):
             a.record()
             for jb, (inp, leaves, dig, caps, n_dig, n_cap) in zip(wave, bufs):
                 N = 1 << (jb["lg_n"] + jb["rate"])
@@ -445,17 +502,28 @@ def run_batch(args):
                 torch.cuda.synchronize()
             b.record()
             torch.cuda.synchronize()
-            t_plain += a.elapsed_time(b) / args.steps
+            t_plain += a.elapsed_time(b) / steps
         for cb, bb in zip(caps_b, bufs):
             assert torch.equal(cb, bb[3]), "batched and plain commitments differ"
         del bufs, cjobs, caps_b
         torch.cuda.empty_cache()
-    line = {"metric": "uneven batch LDE+Merkle commit elems/s (batched graph vs plain per-call)",
-            "unit": "elems/s", "batched": total_elems / (t_batch * 1e-3), "plain": total_elems / (t_plain * 1e-3),
-            "batched_over_plain": t_plain / t_batch, "batched_ms": t_batch, "plain_ms": t_plain, "jobs": len(jobs),
-            "waves": len(waves), "elements": total_elems, "steps": args.steps, "dtype": "u64",
-            "config": {"workload": "64 jobs: lg_n U{10..20}, cols U{8..400}, rate_bits U{1,2,3}, Poseidon, "
-                                   "cap_height min(4, lg N), seed 3", "budget_gb": args.budget_gb}}
+    rate = poseidon_perm_rate()
+    floor_ms = total_perms / rate * 1e3
+    return {"batched_elems_per_s": total_elems / (t_batch * 1e-3), "plain_elems_per_s": total_elems / (t_plain * 1e-3),
+            "batched_over_plain": t_plain / t_batch, "batched_ms": t_batch, "plain_ms": t_plain,
+            "poseidon_perms": total_perms, "poseidon_perms_per_s": rate, "perm_floor_ms": floor_ms,
+            "batched_frac_of_perm_floor": floor_ms / t_batch, "plain_bound_over_floor": t_plain / floor_ms,
+            "jobs": len(jobs), "waves": len(waves), "elements": total_elems, "steps": steps,
+            "workload": "64 jobs: lg_n U{10..20}, cols U{8..400}, rate_bits U{1,2,3}, Poseidon, cap_height min(4, lg N), "
+                        "seed 3; waves of <= %g GiB" % budget_gb}
+
+
+def run_batch(args):
+    import torch
+    torch.cuda.set_device(0)
+    d = measure_batch(args.steps, args.budget_gb)
+    line = {"metric": "uneven batch LDE+Merkle commit elems/s (batched graph vs plain per-call)", "unit": "elems/s",
+            "dtype": "u64", **d}
     print(json.dumps(line), flush=True)
 
 
@@ -500,20 +568,20 @@ def run_hashes(args):
     print(json.dumps(line), flush=True)
 
 
-def run_serve(args):
+def measure_serve(requests):
     """Serving: a Poisson stream of LDE + Poseidon commit requests (log2 size
     U{12..22}, columns U{16..256}, rate_bits 3, cap height 4) admitted by
     zeknox_server against a 120 GB budget; arrival rate 0.7x the capacity
-    measured with serial plain calls.  Reports p50/p99 latency (submit -> caps
-    on host) and throughput vs the serial plain calls."""
+    measured with serial plain calls.  p50/p99 latency (submit -> caps on
+    host), delivered throughput (elements / first arrival -> last completion)
+    and offered throughput (elements / arrival span)."""
     import threading as th
 
     import torch
     import zeknox_b200 as zk
-    torch.cuda.set_device(0)
     rng = np.random.default_rng(5)
     reqs = []
-    for k in range(args.requests):
+    for k in range(requests):
         lg, cols = int(rng.integers(12, 23)), int(rng.integers(16, 257))
         reqs.append((lg, 3, cols, 4, 0, dev_field(cols << lg, 5000 + k)))
     elems = [(1 << (lg + r)) * c for lg, r, c, _, _, _ in reqs]
@@ -542,6 +610,8 @@ def run_serve(args):
     lat, queue = [None] * len(reqs), [None] * len(reqs)
     done_t = [None] * len(reqs)
     with zk.Server(0, 120 << 30, 8) as srv:
+        # twiddles and coset tables of the stream's sizes resident before it starts
+        srv.prepare(12, 22, 3)
         tickets = [None] * len(reqs)
         submitted = []  # indices, in submission order
         lock = th.Lock()
@@ -582,14 +652,24 @@ def run_serve(args):
         rt.join()
         st = srv.stats()
     span = max(done_t) - t0
-    line = {"metric": "serving LDE+Poseidon commit: p50/p99 latency and throughput", "unit": "ms",
-            "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
-            "mean_queue_ms": float(np.mean(queue)), "throughput_elems_per_s": sum(elems) / span,
-            "serial_plain_elems_per_s": capacity, "offered_load": 0.7, "requests": len(reqs),
-            "arrival_rate_per_s": rate, "peak_budget_bytes": st["peak"], "budget_bytes": 120 << 30,
-            "slots": 8, "dtype": "u64",
-            "config": {"workload": "Poisson stream: lg_n U{12..22}, cols U{16..256}, rate_bits 3, Poseidon, cap 4, "
-                                   "120 GB budget, 8 slots, seed 5"}}
+    arrivals = float(np.sum(gaps))
+    del reqs
+    torch.cuda.empty_cache()
+    return {"p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+            "mean_queue_ms": float(np.mean(queue)), "delivered_elems_per_s": sum(elems) / span,
+            "offered_elems_per_s": sum(elems) / arrivals, "serial_plain_elems_per_s": capacity,
+            "offered_load": 0.7, "requests": len(elems), "arrival_rate_per_s": rate, "arrival_span_s": arrivals,
+            "completion_span_s": span, "peak_budget_bytes": st["peak"], "budget_bytes": 120 << 30, "slots": 8,
+            "workload": "Poisson stream: lg_n U{12..22}, cols U{16..256}, rate_bits 3, Poseidon, cap 4, 120 GB budget, "
+                        "8 slots, seed 5; latency = submit -> caps on host"}
+
+
+def run_serve(args):
+    import torch
+    torch.cuda.set_device(0)
+    d = measure_serve(args.requests)
+    line = {"metric": "serving LDE+Poseidon commit: p50/p99 latency and throughput", "unit": "ms", "dtype": "u64",
+            **d}
     print(json.dumps(line), flush=True)
 
 
@@ -604,7 +684,10 @@ def main():
     ap.add_argument("--lg-n", type=int, default=LG_N, help="log2 coefficients per column (profiling cases)")
     ap.add_argument("--only", default=None, choices=["lde", "merkle", "transpose"],
                     help="profiling: run only this stage for warmup+steps iterations and exit")
-    ap.add_argument("--requests", type=int, default=16, help="serve workload: number of requests")
+    ap.add_argument("--requests", type=int, default=32, help="serve workload: number of requests")
+    ap.add_argument("--batch-steps", type=int, default=1, help="uneven batch: timed passes per wave")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="headline only: skip the uneven-batch and serving measurements of the default run")
     ap.add_argument("--workload", default="commit", choices=["commit", "batch", "hashes", "serve"],
                     help="commit: the headline line; batch: uneven 64-job batch vs plain calls; hashes: 2^20 x 135 "
                          "forests with Poseidon2, Monolith and Keccak")

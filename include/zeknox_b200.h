@@ -135,17 +135,43 @@ typedef struct {
     uint64_t *caps_host;      /* host buffer of 2^cap_height x 4 words, filled on completion (may be NULL) */
 } zk_serve_request;
 
+/* zk_serve_result.status of a request cancelled while queued */
+#define ZK_SERVE_CANCELLED (-10000)
+
 typedef struct {
-    int status;               /* 0 queued, 1 running, 2 done, < 0 failed (negated cudaError or -1) */
+    int status;               /* 0 queued, 1 running, 2 done, < 0 failed (negated cudaError, or -1 for a shape
+                                 rejected when it started) or ZK_SERVE_CANCELLED */
     double latency_ms;        /* submit -> caps on host (done only) */
     double queue_ms;          /* submit -> admitted */
     const uint64_t *leaves, *digests, *caps;  /* device results (done, until released) */
 } zk_serve_result;
 
 RustError zeknox_server_create(size_t device_id, uint64_t budget_bytes, uint32_t slots, void **server);
+/* Build and keep resident every table a request of lg_n in [lg_n_min,
+ * lg_n_max] with this rate and coset generator (0 means 7) reads -- twiddles
+ * of every pass, inverse twiddles, the LDE coset tables -- so no request waits
+ * for a table build.  Synchronous; call before submitting (optional: a request
+ * whose tables are missing has them built on the device context's stream, and
+ * its slot stream waits for them on the device). */
+RustError zeknox_server_prepare(void *server, uint32_t lg_n_min, uint32_t lg_n_max, uint32_t rate_bits,
+                                uint64_t coset_gen);
 RustError zeknox_server_submit(void *server, const zk_serve_request *req, uint64_t *ticket);
 /* Wait up to timeout_ms (< 0: forever) for the ticket; fills *result. */
 RustError zeknox_server_wait(void *server, uint64_t ticket, double timeout_ms, zk_serve_result *result);
+/* Take a queued request out of the queue: its status becomes
+ * ZK_SERVE_CANCELLED.  A request that has started cannot be cancelled. */
+RustError zeknox_server_cancel(void *server, uint64_t ticket);
+/* Test hook (failure injection on the host, no GPU fault): the next request
+ * the server starts fails at `stage` -- ZK_SERVE_FAIL_ALLOC: its device
+ * allocation is refused (status -cudaErrorMemoryAllocation);
+ * ZK_SERVE_FAIL_SHAPE: its shape is rejected when it starts (status -1);
+ * ZK_SERVE_FAIL_LAUNCH: queuing its kernels fails after its buffers were
+ * allocated (status -cudaErrorLaunchFailure).  The failed request's memory
+ * and slot are freed at once; later requests are unaffected.  0 clears. */
+#define ZK_SERVE_FAIL_ALLOC 1
+#define ZK_SERVE_FAIL_SHAPE 2
+#define ZK_SERVE_FAIL_LAUNCH 3
+RustError zeknox_server_inject_failure(void *server, int stage);
 /* Free the ticket's device results (returns their bytes to the budget). */
 RustError zeknox_server_release(void *server, uint64_t ticket);
 /* Bytes currently admitted against the budget, and the peak so far. */

@@ -87,3 +87,68 @@ def test_small_request_passes_a_head_that_waits_for_memory():
     # the small request, submitted last, started before the second big one
     # (which waited for the first one's memory)
     assert res[2][0] < res[1][0], res
+
+
+@pytest.mark.parametrize("stage,status", [(zk.SERVE_FAIL_ALLOC, -2), (zk.SERVE_FAIL_SHAPE, -1),
+                                          (zk.SERVE_FAIL_LAUNCH, -719)])
+def test_injected_start_failure_leaves_later_requests_exact(stage, status):
+    """A request whose start fails on the host (device allocation refused, a
+    shape rejected when it starts, kernel queuing refused after its buffers
+    were allocated) reports a negative status, gives its memory and slot back,
+    and the requests after it still come out bit-exact."""
+    shapes = [(11, 3, 40, 4, 0), (10, 2, 64, 3, 3), (12, 1, 24, 4, 4)]
+    inputs = [to_dev(O.field_data(1200 + i, s[2] << s[0])) for i, s in enumerate(shapes)]
+    solo = [alone(*s, inp)[0] for s, inp in zip(shapes, inputs)]
+    caps_host = [torch.zeros((1 << s[3]) * 4, dtype=torch.int64).pin_memory() for s in shapes]
+    with zk.Server(0, 2 << 30, 2) as srv:
+        srv.prepare(10, 12, 3)
+        srv.prepare(10, 12, 2)
+        srv.prepare(10, 12, 1)
+        srv.inject_failure(stage)  # the next request the server starts: the first one
+        tickets = [srv.submit(*s, inp, caps_host=ch) for s, inp, ch in zip(shapes, inputs, caps_host)]
+        r = srv.wait(tickets[0])
+        assert r.status == status, r.status
+        assert not r.leaves and not r.caps
+        srv.release(tickets[0])
+        for t, ch, caps in zip(tickets[1:], caps_host[1:], solo[1:]):
+            r = srv.wait(t)
+            assert r.status == 2, r.status
+            assert np.array_equal(ch.numpy().view(np.uint64), caps)
+            srv.release(t)
+        st = srv.stats()
+        assert st["in_use"] == 0 and st["completed"] == len(shapes) - 1
+        # the server keeps serving: the failed shape again, now without injection
+        t = srv.submit(*shapes[0], inputs[0], caps_host=caps_host[0])
+        assert srv.wait(t).status == 2
+        assert np.array_equal(caps_host[0].numpy().view(np.uint64), solo[0])
+        srv.release(t)
+
+
+def test_cancel_a_queued_request():
+    """One slot busy with large jobs: a small request behind them is cancelled
+    while queued (status ZK_SERVE_CANCELLED, nothing counted against the
+    budget), cancelling a started or finished one is refused, and the rest
+    still come out bit-exact."""
+    big = (16, 3, 128, 4, 0)
+    small = (10, 2, 16, 2, 3)
+    shapes = [big, big, small, small]
+    inputs = [to_dev(O.field_data(1300 + i, s[2] << s[0])) for i, s in enumerate(shapes)]
+    solo = [alone(*s, inp)[0] for s, inp in zip(shapes, inputs)]
+    caps_host = [torch.zeros((1 << s[3]) * 4, dtype=torch.int64).pin_memory() for s in shapes]
+    with zk.Server(0, 8 << 30, 1) as srv:
+        tickets = [srv.submit(*s, inp, caps_host=ch) for s, inp, ch in zip(shapes, inputs, caps_host)]
+        srv.cancel(tickets[2])  # two large commits are ahead of it on the one slot
+        r = srv.wait(tickets[2], 0.0)
+        assert r.status == zk.SERVE_CANCELLED
+        with pytest.raises(zk.ZeknoxError):
+            srv.cancel(tickets[2])
+        srv.release(tickets[2])
+        for i in (0, 1, 3):
+            r = srv.wait(tickets[i])
+            assert r.status == 2, (i, r.status)
+            assert np.array_equal(caps_host[i].numpy().view(np.uint64), solo[i])
+            with pytest.raises(zk.ZeknoxError):
+                srv.cancel(tickets[i])
+            srv.release(tickets[i])
+        st = srv.stats()
+        assert st["in_use"] == 0 and st["completed"] == 3

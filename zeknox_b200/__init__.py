@@ -23,6 +23,8 @@ P = 0xFFFFFFFF00000001
 HASH_POSEIDON, HASH_KECCAK, HASH_POSEIDON_BN128, HASH_POSEIDON2, HASH_MONOLITH = 0, 1, 2, 3, 4
 FORWARD, INVERSE = 0, 1
 SELFTEST_OPS = 22  # ZK_SELFTEST_OPS of include/zeknox_b200.h
+SERVE_CANCELLED = -10000  # ZK_SERVE_CANCELLED
+SERVE_FAIL_ALLOC, SERVE_FAIL_SHAPE, SERVE_FAIL_LAUNCH = 1, 2, 3  # ZK_SERVE_FAIL_*
 
 # Exported C symbols (include/lib.h, include/merkle/merkle.h, include/zeknox_b200.h).
 ABI_SYMBOLS = [
@@ -36,7 +38,8 @@ ABI_SYMBOLS = [
 EXT_SYMBOLS = ["zeknox_last_error", "zeknox_commit", "zeknox_commit_batch", "zeknox_commit_scratch_words",
                "zeknox_lde_rows", "zeknox_launch_count", "zeknox_measure_mul_rate", "zeknox_merkle_batch",
                "zeknox_lde_rows_noalloc", "zeknox_server_create", "zeknox_server_submit", "zeknox_server_wait",
-               "zeknox_server_release", "zeknox_server_stats", "zeknox_server_destroy", "zeknox_tune_set",
+               "zeknox_server_release", "zeknox_server_stats", "zeknox_server_destroy", "zeknox_server_prepare",
+               "zeknox_server_cancel", "zeknox_server_inject_failure", "zeknox_tune_set",
                "zeknox_tune_get", "zeknox_tune_clear", "zeknox_tune_load", "zeknox_transpose_rev",
                "zeknox_lde_rows_scatter", "zeknox_field_selftest", "zeknox_permute"]
 
@@ -192,6 +195,12 @@ def load():
     L.zeknox_server_stats.argtypes = [vp, ctypes.POINTER(u64), ctypes.POINTER(u64), ctypes.POINTER(u64)]
     L.zeknox_server_destroy.restype = RustError
     L.zeknox_server_destroy.argtypes = [vp]
+    L.zeknox_server_prepare.restype = RustError
+    L.zeknox_server_prepare.argtypes = [vp, u32, u32, u32, u64]
+    L.zeknox_server_cancel.restype = RustError
+    L.zeknox_server_cancel.argtypes = [vp, u64]
+    L.zeknox_server_inject_failure.restype = RustError
+    L.zeknox_server_inject_failure.argtypes = [vp, ctypes.c_int]
     L.zeknox_merkle_batch.restype = RustError
     L.zeknox_merkle_batch.argtypes = [sz, ctypes.POINTER(MerkleJob), u32]
     L.zeknox_lde_rows_scatter.restype = RustError
@@ -525,6 +534,17 @@ class Server:
 
     def release(self, ticket):
         _check(load().zeknox_server_release(self._h, ticket))
+
+    def prepare(self, lg_n_min, lg_n_max, rate_bits, coset_gen=7):
+        """Build every table requests of these sizes read, ahead of them."""
+        _check(load().zeknox_server_prepare(self._h, lg_n_min, lg_n_max, rate_bits, coset_gen))
+
+    def cancel(self, ticket):
+        _check(load().zeknox_server_cancel(self._h, ticket))
+
+    def inject_failure(self, stage):
+        """Test hook: the next request started fails at `stage` (SERVE_FAIL_*)."""
+        _check(load().zeknox_server_inject_failure(self._h, stage))
 
     def stats(self):
         a, b, c = ctypes.c_uint64(), ctypes.c_uint64(), ctypes.c_uint64()

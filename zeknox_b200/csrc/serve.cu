@@ -36,7 +36,7 @@ using Clock = std::chrono::steady_clock;
 struct Ticket {
     zk_serve_request req;
     Clock::time_point t_submit, t_admit, t_done;
-    int status = 0;  // 0 queued, 1 running, 2 done, < 0 failed
+    int status = 0;  // 0 queued, 1 running, 2 done, < 0 failed or cancelled
     int slot = -1;
     uint64_t bytes = 0;
     uint64_t *leaves = nullptr, *digests = nullptr, *caps = nullptr, *scratch = nullptr;
@@ -48,6 +48,7 @@ struct Server {
     uint64_t budget = 0, in_use = 0, peak = 0, completed = 0;
     std::vector<cudaStream_t> slot_stream;
     std::vector<uint64_t> slot_ticket;  // 0 = idle
+    cudaEvent_t tables_ready = nullptr; // recorded on the context stream after a start's table builds
     std::mutex mu;
     std::condition_variable cv;  // signalled on submit, completion, release, stop
     std::deque<uint64_t> queue;
@@ -55,6 +56,7 @@ struct Server {
     uint64_t next_id = 1;
     uint64_t blocked_head = 0;  // head of the queue that waits for memory
     uint32_t bypassed = 0;      // small requests started ahead of it
+    int inject_next = 0;        // test hook: the next start fails at this stage (ZK_SERVE_FAIL_*)
     bool stop = false;
     std::thread worker;
 
@@ -66,21 +68,20 @@ struct Server {
                     commit_scratch_words(r.lg_n, r.rate_bits, r.cols, r.input_is_values != 0));
     }
 
-    void run_one(uint64_t id, int slot)
+    // Allocate an admitted job's buffers and queue its whole commit on the
+    // slot stream.  Runs on the server thread without `mu` (client threads
+    // keep submitting, waiting and releasing meanwhile): a starting ticket can
+    // be neither released nor cancelled, and only this thread starts jobs.
+    // Returns 1 when the work is queued, else a negative status, with anything
+    // allocated already returned on the stream.
+    int start(Ticket &t, int slot, int inject)
     {
-        Ticket &t = tickets[id];
         const zk_serve_request &r = t.req;
         cudaStream_t s = slot_stream[slot];
         const uint64_t N = 1ULL << (r.lg_n + r.rate_bits);
         const uint64_t n_caps = 1ULL << r.cap_height;
+        std::lock_guard<std::recursive_mutex> lk(ctx->mu);
         try {
-            std::lock_guard<std::recursive_mutex> lk(ctx->mu);
-            ZK_CUDA(cudaSetDevice(ctx->id));
-            ZK_CUDA(cudaMallocAsync((void **)&t.leaves, N * r.cols * 8, s));
-            if (N > n_caps) ZK_CUDA(cudaMallocAsync((void **)&t.digests, (N - n_caps) * 64, s));
-            ZK_CUDA(cudaMallocAsync((void **)&t.caps, n_caps * 32, s));
-            const uint64_t sw = commit_scratch_words(r.lg_n, r.rate_bits, r.cols, r.input_is_values != 0);
-            if (sw) ZK_CUDA(cudaMallocAsync((void **)&t.scratch, sw * 8, s));
             zk_commit_job j{};
             j.lg_n = r.lg_n;
             j.rate_bits = r.rate_bits;
@@ -90,11 +91,26 @@ struct Server {
             j.input_is_values = r.input_is_values;
             j.coset_gen = r.coset_gen;
             j.input = r.input;
+            if (inject == ZK_SERVE_FAIL_SHAPE) j.cap_height = j.lg_n + j.rate_bits + 1;  // a shape that cannot commit
+            if (inject == ZK_SERVE_FAIL_ALLOC)
+                throw cuda_failure(-(int)cudaErrorMemoryAllocation, "device allocation refused (injected)");
+            ZK_CUDA(cudaMallocAsync((void **)&t.leaves, N * r.cols * 8, s));
+            if (N > n_caps) ZK_CUDA(cudaMallocAsync((void **)&t.digests, (N - n_caps) * 64, s));
+            ZK_CUDA(cudaMallocAsync((void **)&t.caps, n_caps * 32, s));
+            const uint64_t sw = commit_scratch_words(r.lg_n, r.rate_bits, r.cols, r.input_is_values != 0);
+            if (sw) ZK_CUDA(cudaMallocAsync((void **)&t.scratch, sw * 8, s));
             j.leaves = t.leaves;
             j.digests = t.digests;
             j.caps = t.caps;
+            check_job(j);
+            // tables this shape reads that are not resident yet are built on
+            // the context stream; the slot stream waits for them on the
+            // device, not the server thread on the host
             prepare_job(*ctx, j);
-            ZK_CUDA(cudaStreamSynchronize(ctx->stream));  // tables built on the context stream
+            ZK_CUDA(cudaEventRecord(tables_ready, ctx->stream));
+            ZK_CUDA(cudaStreamWaitEvent(s, tables_ready, 0));
+            if (inject == ZK_SERVE_FAIL_LAUNCH)
+                throw cuda_failure(-(int)cudaErrorLaunchFailure, "kernel launch refused (injected)");
             commit_enqueue(*ctx, j, s, t.scratch);
             if (t.scratch) {
                 ZK_CUDA(cudaFreeAsync(t.scratch, s));
@@ -103,11 +119,21 @@ struct Server {
             if (r.caps_host) ZK_CUDA(cudaMemcpyAsync(r.caps_host, t.caps, n_caps * 32, cudaMemcpyDeviceToHost, s));
             ZK_CUDA(cudaEventCreateWithFlags(&t.done_ev, cudaEventDisableTiming));
             ZK_CUDA(cudaEventRecord(t.done_ev, s));
-            t.status = 1;
-        } catch (const cuda_failure &e) {
-            t.status = e.code < 0 ? e.code : -1;
-        } catch (const std::exception &) {
-            t.status = -1;
+            return 1;
+        } catch (const std::exception &e) {
+            const cuda_failure *cf = dynamic_cast<const cuda_failure *>(&e);
+            const arg_failure *af = dynamic_cast<const arg_failure *>(&e);
+            for (uint64_t **p : {&t.leaves, &t.digests, &t.caps, &t.scratch})
+                if (*p) {
+                    (void)cudaFreeAsync(*p, s);
+                    *p = nullptr;
+                }
+            if (t.done_ev) {
+                cudaEventDestroy(t.done_ev);
+                t.done_ev = nullptr;
+            }
+            (void)cudaGetLastError();
+            return cf ? (cf->code < 0 ? cf->code : -1) : af ? -af->code : -1;
         }
     }
 
@@ -121,11 +147,6 @@ struct Server {
                 uint64_t id = slot_ticket[k];
                 if (!id) continue;
                 Ticket &t = tickets[id];
-                if (t.status < 0) {
-                    slot_ticket[k] = 0;
-                    progressed = true;
-                    continue;
-                }
                 cudaError_t q = cudaEventQuery(t.done_ev);
                 if (q == cudaErrorNotReady) continue;
                 t.t_done = Clock::now();
@@ -168,12 +189,20 @@ struct Server {
                 peak = in_use > peak ? in_use : peak;
                 t.slot = slot;
                 t.t_admit = Clock::now();
+                t.status = 1;
                 slot_ticket[slot] = id;
-                run_one(id, slot);
-                if (t.status < 0) {
-                    // could not start: give the memory back now
+                const int inject = inject_next;
+                inject_next = 0;
+                lk.unlock();
+                const int st = start(t, slot, inject);
+                lk.lock();
+                if (st < 0) {
+                    // could not start: the slot and the memory are free again
+                    t.status = st;
+                    t.t_done = Clock::now();
                     in_use -= t.bytes;
                     t.bytes = 0;
+                    slot_ticket[slot] = 0;
                 }
                 cv.notify_all();
             }
@@ -237,6 +266,7 @@ extern "C" RustError zeknox_server_create(size_t device_id, uint64_t budget_byte
         s->slot_stream.resize(slots);
         s->slot_ticket.assign(slots, 0);
         for (auto &st : s->slot_stream) ZK_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+        ZK_CUDA(cudaEventCreateWithFlags(&s->tables_ready, cudaEventDisableTiming));
         s->worker = std::thread([s] {
             cudaSetDevice(s->ctx->id);
             s->loop();
@@ -333,6 +363,59 @@ extern "C" RustError zeknox_server_stats(void *server, uint64_t *in_use_bytes, u
     });
 }
 
+extern "C" RustError zeknox_server_prepare(void *server, uint32_t lg_n_min, uint32_t lg_n_max, uint32_t rate_bits,
+                                           uint64_t coset_gen)
+{
+    return zk::guard([&] {
+        Server *s = zk::as_server(server);
+        if (lg_n_min == 0 || lg_n_min > lg_n_max || rate_bits == 0 || rate_bits > 32 || lg_n_max > 32 - rate_bits)
+            throw zk::arg_failure("need 1 <= lg_n_min <= lg_n_max and lg_n_max + rate_bits <= 32");
+        std::lock_guard<std::recursive_mutex> dl(s->ctx->mu);
+        ZK_CUDA(cudaSetDevice(s->ctx->id));
+        for (uint32_t lg = lg_n_min; lg <= lg_n_max; lg++) {
+            zk_commit_job j{};
+            j.lg_n = lg;
+            j.rate_bits = rate_bits;
+            j.coset_gen = coset_gen;
+            j.input_is_values = 1;  // the inverse tables too
+            zk::prepare_job(*s->ctx, j);
+        }
+        s->ctx->sync();
+    });
+}
+
+extern "C" RustError zeknox_server_cancel(void *server, uint64_t ticket)
+{
+    return zk::guard([&] {
+        Server *s = zk::as_server(server);
+        std::lock_guard<std::mutex> lk(s->mu);
+        auto it = s->tickets.find(ticket);
+        if (it == s->tickets.end()) throw zk::arg_failure("unknown ticket");
+        zk::Ticket &t = it->second;
+        if (t.status != 0) throw zk::arg_failure("only a queued request can be cancelled");
+        for (auto q = s->queue.begin(); q != s->queue.end(); ++q)
+            if (*q == ticket) {
+                s->queue.erase(q);
+                break;
+            }
+        if (s->blocked_head == ticket) s->blocked_head = 0;
+        t.status = ZK_SERVE_CANCELLED;
+        t.bytes = 0;  // never admitted: nothing was counted against the budget
+        t.t_done = t.t_admit = zk::Clock::now();
+        s->cv.notify_all();
+    });
+}
+
+extern "C" RustError zeknox_server_inject_failure(void *server, int stage)
+{
+    return zk::guard([&] {
+        Server *s = zk::as_server(server);
+        if (stage < 0 || stage > ZK_SERVE_FAIL_LAUNCH) throw zk::arg_failure("unknown failure stage");
+        std::lock_guard<std::mutex> lk(s->mu);
+        s->inject_next = stage;
+    });
+}
+
 extern "C" RustError zeknox_server_destroy(void *server)
 {
     return zk::guard([&] {
@@ -352,6 +435,7 @@ extern "C" RustError zeknox_server_destroy(void *server)
             cudaStreamSynchronize(st);
             cudaStreamDestroy(st);
         }
+        cudaEventDestroy(s->tables_ready);
         delete s;
     });
 }
