@@ -430,14 +430,18 @@ def poseidon_perm_rate(steps=3):
     dig = torch.empty(n_dig * 4, dtype=torch.int64, device="cuda")
     caps = torch.empty(n_cap * 4, dtype=torch.int64, device="cuda")
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    # the Merkle entry point queues on the legacy default stream: time it there
+    legacy = torch.cuda.default_stream()
     zk.fill_digests_buf_linear_gpu(dig, caps, leaves, nl, ls, ch, 0)
+    torch.cuda.synchronize()
     ts = []
     for s in range(steps):
-        flush.fill_(s & 0xFF)
+        with torch.cuda.stream(legacy):
+            flush.fill_(s & 0xFF)
         a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        a.record()
+        a.record(legacy)
         zk.fill_digests_buf_linear_gpu(dig, caps, leaves, nl, ls, ch, 0)
-        b.record()
+        b.record(legacy)
         torch.cuda.synchronize()
         ts.append(a.elapsed_time(b))
     del leaves, dig, caps, flush
@@ -568,27 +572,73 @@ def run_hashes(args):
     print(json.dumps(line), flush=True)
 
 
-def measure_serve(requests):
+def serve_stream(srv, reqs, gaps, caps_host):
+    """Submit reqs[i] at the cumulative times gaps[:i+1] (all at once when gaps
+    is None) while a client thread takes every result as soon as it is ready,
+    in completion order, and releases it.  Returns per-request latency and
+    queue time (ms), the completion times and the start time (perf_counter)."""
+    import threading as th
+    n = len(reqs)
+    tickets, submitted, lock = [None] * n, [], th.Lock()
+    lat, queue, done_t = [None] * n, [None] * n, [None] * n
+
+    def reaper():
+        outstanding, seen, n_done = set(), 0, 0
+        while n_done < n:
+            with lock:
+                outstanding.update(submitted[seen:])
+                seen = len(submitted)
+            finished = []
+            for i in outstanding:
+                r = srv.wait(tickets[i], 0.0)
+                if r.status == 2 or r.status < 0:
+                    assert r.status == 2, r.status
+                    lat[i], queue[i], done_t[i] = r.latency_ms, r.queue_ms, time.perf_counter()
+                    srv.release(tickets[i])
+                    finished.append(i)
+            outstanding.difference_update(finished)
+            n_done += len(finished)
+            if not finished:
+                time.sleep(0.0002)
+
+    rt = th.Thread(target=reaper)
+    rt.start()
+    t0 = time.perf_counter()
+    when = t0
+    for i, (lg, r, c, cap, h, inp) in enumerate(reqs):
+        if gaps is not None:
+            when += gaps[i]
+            delay = when - time.perf_counter()
+            if delay > 0:
+                time.sleep(delay)
+        tickets[i] = srv.submit(lg, r, c, cap, h, inp, caps_host=caps_host[i])
+        with lock:
+            submitted.append(i)
+    rt.join()
+    return lat, queue, done_t, t0
+
+
+def measure_serve(requests, serial_sample=24):
     """Serving: a Poisson stream of LDE + Poseidon commit requests (log2 size
     U{12..22}, columns U{16..256}, rate_bits 3, cap height 4) admitted by
-    zeknox_server against a 120 GB budget; arrival rate 0.7x the capacity
-    measured with serial plain calls.  p50/p99 latency (submit -> caps on
-    host), delivered throughput (elements / first arrival -> last completion)
-    and offered throughput (elements / arrival span)."""
-    import threading as th
-
+    zeknox_server against a 120 GB budget with 8 slots; arrival rate 0.7x the
+    capacity of serial plain calls (one synchronous zeknox_commit per request,
+    timed on the first `serial_sample` requests).  Reports p50/p99 latency
+    (submit -> caps on host), delivered throughput (elements / first arrival
+    -> last completion), offered throughput (elements / arrival span), and
+    the server's capacity with every request submitted at once.  Requests read
+    their coefficients from one shared seeded pool (the stream can then be
+    long without holding every input)."""
     import torch
     import zeknox_b200 as zk
     rng = np.random.default_rng(5)
-    reqs = []
-    for k in range(requests):
-        lg, cols = int(rng.integers(12, 23)), int(rng.integers(16, 257))
-        reqs.append((lg, 3, cols, 4, 0, dev_field(cols << lg, 5000 + k)))
-    elems = [(1 << (lg + r)) * c for lg, r, c, _, _, _ in reqs]
-    # serial plain calls: one synchronous zeknox_commit per request
+    shapes = [(int(rng.integers(12, 23)), 3, int(rng.integers(16, 257)), 4, 0) for _ in range(requests)]
+    pool = dev_field(256 << 22, 5000)
+    reqs = [(lg, r, c, cap, h, pool[:c << lg]) for lg, r, c, cap, h in shapes]
+    elems = [(1 << (lg + r)) * c for lg, r, c, _, _ in shapes]
     serial = []
     a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    for lg, r, c, cap, h, inp in reqs:
+    for lg, r, c, cap, h, inp in reqs[:serial_sample]:
         N = 1 << (lg + r)
         leaves = torch.empty(N * c, dtype=torch.int64, device="cuda")
         n_dig, n_cap = zk.merkle_sizes(N, cap)
@@ -603,63 +653,28 @@ def measure_serve(requests):
         serial.append(a.elapsed_time(b))
         del leaves, dig, caps
         torch.cuda.empty_cache()
-    capacity = sum(elems) / (sum(serial) * 1e-3)
+    capacity = sum(elems[:serial_sample]) / (sum(serial) * 1e-3)
     rate = 0.7 / (np.mean(serial) * 1e-3)  # requests per second
     gaps = rng.exponential(1.0 / rate, size=len(reqs))
-    caps_host = [torch.zeros((1 << cap) * 4, dtype=torch.int64).pin_memory() for _, _, _, cap, _, _ in reqs]
-    lat, queue = [None] * len(reqs), [None] * len(reqs)
-    done_t = [None] * len(reqs)
+    caps_host = [torch.zeros((1 << cap) * 4, dtype=torch.int64).pin_memory() for _, _, _, cap, _ in shapes]
     with zk.Server(0, 120 << 30, 8) as srv:
         # twiddles and coset tables of the stream's sizes resident before it starts
         srv.prepare(12, 22, 3)
-        tickets = [None] * len(reqs)
-        submitted = []  # indices, in submission order
-        lock = th.Lock()
-
-        def reaper():
-            # a client that takes each result as soon as it is ready, in
-            # completion order, and releases its memory back to the budget
-            outstanding, seen, n_done = set(), 0, 0
-            while n_done < len(reqs):
-                with lock:
-                    outstanding.update(submitted[seen:])
-                    seen = len(submitted)
-                finished = []
-                for i in outstanding:
-                    r = srv.wait(tickets[i], 0.0)
-                    if r.status == 2 or r.status < 0:
-                        assert r.status == 2, r.status
-                        lat[i], queue[i], done_t[i] = r.latency_ms, r.queue_ms, time.perf_counter()
-                        srv.release(tickets[i])
-                        finished.append(i)
-                outstanding.difference_update(finished)
-                n_done += len(finished)
-                if not finished:
-                    time.sleep(0.0002)
-
-        rt = th.Thread(target=reaper)
-        rt.start()
-        t0 = time.perf_counter()
-        when = t0
-        for i, (lg, r, c, cap, h, inp) in enumerate(reqs):
-            when += gaps[i]
-            delay = when - time.perf_counter()
-            if delay > 0:
-                time.sleep(delay)
-            tickets[i] = srv.submit(lg, r, c, cap, h, inp, caps_host=caps_host[i])
-            with lock:
-                submitted.append(i)
-        rt.join()
-        st = srv.stats()
+        lat, queue, done_t, t0 = serve_stream(srv, reqs, gaps, caps_host)
+        peak = srv.stats()["peak"]
+        _, _, done_s, t0s = serve_stream(srv, reqs, None, caps_host)
     span = max(done_t) - t0
     arrivals = float(np.sum(gaps))
-    del reqs
+    saturated = sum(elems) / (max(done_s) - t0s)
+    del reqs, pool
     torch.cuda.empty_cache()
     return {"p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
             "mean_queue_ms": float(np.mean(queue)), "delivered_elems_per_s": sum(elems) / span,
-            "offered_elems_per_s": sum(elems) / arrivals, "serial_plain_elems_per_s": capacity,
-            "offered_load": 0.7, "requests": len(elems), "arrival_rate_per_s": rate, "arrival_span_s": arrivals,
-            "completion_span_s": span, "peak_budget_bytes": st["peak"], "budget_bytes": 120 << 30, "slots": 8,
+            "offered_elems_per_s": sum(elems) / arrivals, "delivered_over_offered": arrivals / span,
+            "saturated_elems_per_s": saturated, "serial_plain_elems_per_s": capacity,
+            "saturated_over_serial": saturated / capacity, "offered_load": 0.7, "requests": len(elems),
+            "arrival_rate_per_s": rate, "arrival_span_s": arrivals, "completion_span_s": span,
+            "peak_budget_bytes": peak, "budget_bytes": 120 << 30, "slots": 8, "serial_sample": serial_sample,
             "workload": "Poisson stream: lg_n U{12..22}, cols U{16..256}, rate_bits 3, Poseidon, cap 4, 120 GB budget, "
                         "8 slots, seed 5; latency = submit -> caps on host"}
 
@@ -684,7 +699,7 @@ def main():
     ap.add_argument("--lg-n", type=int, default=LG_N, help="log2 coefficients per column (profiling cases)")
     ap.add_argument("--only", default=None, choices=["lde", "merkle", "transpose"],
                     help="profiling: run only this stage for warmup+steps iterations and exit")
-    ap.add_argument("--requests", type=int, default=32, help="serve workload: number of requests")
+    ap.add_argument("--requests", type=int, default=96, help="serve workload: number of requests")
     ap.add_argument("--batch-steps", type=int, default=1, help="uneven batch: timed passes per wave")
     ap.add_argument("--no-extras", action="store_true",
                     help="headline only: skip the uneven-batch and serving measurements of the default run")
