@@ -579,7 +579,7 @@ def serve_stream(srv, reqs, gaps, caps_host):
     queue time (ms), the completion times and the start time (perf_counter)."""
     import threading as th
     n = len(reqs)
-    tickets, submitted, lock = [None] * n, [], th.Lock()
+    tickets, submitted, lock, failed = [None] * n, [], th.Lock(), []
     lat, queue, done_t = [None] * n, [None] * n, [None] * n
 
     def reaper():
@@ -592,7 +592,8 @@ def serve_stream(srv, reqs, gaps, caps_host):
             for i in outstanding:
                 r = srv.wait(tickets[i], 0.0)
                 if r.status == 2 or r.status < 0:
-                    assert r.status == 2, r.status
+                    if r.status < 0:
+                        failed.append((i, r.status))  # reported after the stream (the thread must not stop early)
                     lat[i], queue[i], done_t[i] = r.latency_ms, r.queue_ms, time.perf_counter()
                     srv.release(tickets[i])
                     finished.append(i)
@@ -615,6 +616,8 @@ def serve_stream(srv, reqs, gaps, caps_host):
         with lock:
             submitted.append(i)
     rt.join()
+    if failed:
+        raise RuntimeError("serving requests failed (index, status): %s" % failed[:8])
     return lat, queue, done_t, t0
 
 

@@ -218,8 +218,11 @@ RustError zeknox_tune_load(const char *path);
  *  15 the same, ALU     16 x + 5 y + 6 z (carry-counting sum)
  *  17 4 (41 x + 39 y + 34 z) + yc (small-constant dot product)
  *  18 p0 + 2^22 p1 + 2^44 p2 with p0, p1, p2 the low 28 bits of x, y, z
- *  19 x + 2^64 y        20 x + 2^64 (y mod 2^32)      21 x * 2^(y mod 64) */
-#define ZK_SELFTEST_OPS 22
+ *  19 x + 2^64 y        20 x + 2^64 (y mod 2^32)      21 x * 2^(y mod 64)
+ *  22 x + y (the NTT's lazy sum)            23 x - y (the NTT's lazy difference)
+ *  24..33 x * 2^e (the NTT's lazy power-of-two twiddle), e = 1, 24, 31, 32,
+ *         60, 63, 64, 72, 84, 95 */
+#define ZK_SELFTEST_OPS 34
 RustError zeknox_field_selftest(size_t device_id, const uint64_t *a, const uint64_t *b, const uint64_t *c, uint64_t n,
                                 uint64_t *out, void *stream);
 

@@ -246,7 +246,7 @@ def field_ops_expected(a, b, c):
     """Exact values of the device self-test operations (ZK_SELFTEST_OPS rows,
     include/zeknox_b200.h) for operand arrays a, b, c of any 64-bit words;
     Python integers, so the arithmetic is the definition mod p."""
-    rows = [[] for _ in range(22)]
+    rows = [[] for _ in range(34)]
     for x, y, z in zip((int(v) for v in a), (int(v) for v in b), (int(v) for v in c)):
         xc, yc = x % P, y % P
         lo28 = (1 << 28) - 1
@@ -259,7 +259,8 @@ def field_ops_expected(a, b, c):
             (x + 5 * y + 6 * z) % P, (4 * (41 * x + 39 * y + 34 * z) + yc) % P,
             ((x & lo28) + ((y & lo28) << 22) + ((z & lo28) << 44)) % P,
             (x + (y << 64)) % P, (x + ((y & 0xFFFFFFFF) << 64)) % P, x * (1 << (y % 64)) % P,
-        ]
+            (x + y) % P, (x - y) % P,
+        ] + [x * (1 << e) % P for e in (1, 24, 31, 32, 60, 63, 64, 72, 84, 95)]
         for k, v in enumerate(vals):
             rows[k].append(v)
     return np.array(rows, dtype=np.uint64)

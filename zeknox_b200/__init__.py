@@ -22,7 +22,7 @@ LIB_PATH = os.path.join(HERE, "libzeknox.so")
 P = 0xFFFFFFFF00000001
 HASH_POSEIDON, HASH_KECCAK, HASH_POSEIDON_BN128, HASH_POSEIDON2, HASH_MONOLITH = 0, 1, 2, 3, 4
 FORWARD, INVERSE = 0, 1
-SELFTEST_OPS = 22  # ZK_SELFTEST_OPS of include/zeknox_b200.h
+SELFTEST_OPS = 34  # ZK_SELFTEST_OPS of include/zeknox_b200.h
 SERVE_CANCELLED = -10000  # ZK_SERVE_CANCELLED
 SERVE_FAIL_ALLOC, SERVE_FAIL_SHAPE, SERVE_FAIL_LAUNCH = 1, 2, 3  # ZK_SERVE_FAIL_*
 

@@ -59,16 +59,150 @@ __device__ __forceinline__ uint64_t ntt_add(uint64_t a, uint64_t b)
     return c ? (((uint64_t)t1 << 32) | t0) : (((uint64_t)r1 << 32) | r0);  // gl_add's selection
 }
 
-// In-register DIF on E = 2^LOGE values: natural input, bit-reversed output.
-// Stages and butterflies are expanded at compile time so every index and every
-// shift amount is a constant (the values stay in registers).
+// ---- lazily reduced butterfly arithmetic.  Inside a pass the values are any
+// 64-bit representatives ("nc"), as in the hash permutations: sums and
+// differences fold their carry or borrow back in (2^64 = EPS mod p) with no
+// comparison and no canonicalisation, twiddle products stay unreduced, and a
+// value is canonicalised once, when the pass stores it to global memory.
+
+// a + b for any 64-bit a, b: lo + 2^64 c = lo + c * EPS, which can carry once
+// more (only when both operands are >= p); the carries enter as multiply-adds
+// c * EPS + lo, so they run on the multiply pipe the passes leave idle.
+__device__ __forceinline__ uint64_t ntt_add_nc(uint64_t a, uint64_t b)
+{
+    uint32_t r0, r1, c;
+    asm("{\n\t"
+        "mad.lo.cc.u32   %0, %3, %7, %5;\n\t"   // r = a + b
+        "madc.lo.cc.u32  %1, %4, %7, %6;\n\t"
+        "madc.lo.u32     %2, %8, %8, %8;\n\t"   // c = carry
+        "mad.lo.cc.u32   %0, %2, 0xffffffff, %0;\n\t"  // r += c * EPS
+        "madc.lo.cc.u32  %1, %8, %8, %1;\n\t"
+        "madc.lo.u32     %2, %8, %8, %8;\n\t"
+        "mad.lo.cc.u32   %0, %2, 0xffffffff, %0;\n\t"  // second carry: r + EPS < 2 EPS
+        "madc.lo.u32     %1, %8, %8, %1;\n\t"
+        "}"
+        : "=&r"(r0), "=&r"(r1), "=&r"(c)
+        : "r"((uint32_t)a), "r"((uint32_t)(a >> 32)), "r"((uint32_t)b), "r"((uint32_t)(b >> 32)), "r"(d_ntt_one),
+          "r"(d_ntt_zero));
+    return ((uint64_t)r1 << 32) | r0;
+}
+
+// a - b for any 64-bit a, b: the wrapped difference d stands for d - 2^64 =
+// d - EPS on a borrow, which can borrow once more (d < EPS).
+__device__ __forceinline__ uint64_t ntt_sub_nc(uint64_t a, uint64_t b)
+{
+    uint32_t r0, r1, m;
+    asm("{\n\t"
+        "sub.cc.u32      %0, %3, %5;\n\t"
+        "subc.cc.u32     %1, %4, %6;\n\t"
+        "subc.u32        %2, 0, 0;\n\t"       // m = borrow ? EPS : 0
+        "sub.cc.u32      %0, %0, %2;\n\t"
+        "subc.cc.u32     %1, %1, 0;\n\t"
+        "subc.u32        %2, 0, 0;\n\t"
+        "sub.cc.u32      %0, %0, %2;\n\t"
+        "subc.u32        %1, %1, 0;\n\t"
+        "}"
+        : "=&r"(r0), "=&r"(r1), "=&r"(m)
+        : "r"((uint32_t)a), "r"((uint32_t)(a >> 32)), "r"((uint32_t)b), "r"((uint32_t)(b >> 32)));
+    return ((uint64_t)r1 << 32) | r0;
+}
+
+// a * 2^E for 0 < E < 96 and any 64-bit a, unreduced.  With t = E mod 32 and
+// a * 2^t = q0 + 2^32 q1 + 2^64 q2 (two wide multiplies of a's halves):
+//   E <  32:  q0 + 2^32 q1 + EPS q2
+//   E <  64:  2^32 q0 + EPS q1 - q2          (2^96 = -1)
+//   E <  96:  EPS q0 - q1 - 2^32 q2          (2^128 = -2^32)
+// each folded to 64 bits with at most two carry / borrow corrections.
+template <unsigned E>
+__device__ __forceinline__ uint64_t ntt_mul_pow2_nc(uint64_t a)
+{
+    static_assert(E > 0 && E < 96, "exponent");
+    const uint32_t m = 1u << (E & 31);
+    uint32_t q0, q1, q2;
+    asm("{\n\t"
+        ".reg .u64 p0, p1;\n\t"
+        ".reg .u32 h0, l1, h1;\n\t"
+        "mul.wide.u32    p0, %3, %5;\n\t"
+        "mul.wide.u32    p1, %4, %5;\n\t"
+        "mov.b64         {%0, h0}, p0;\n\t"
+        "mov.b64         {l1, h1}, p1;\n\t"
+        "add.cc.u32      %1, h0, l1;\n\t"
+        "addc.u32        %2, h1, 0;\n\t"
+        "}"
+        : "=r"(q0), "=r"(q1), "=r"(q2)
+        : "r"((uint32_t)a), "r"((uint32_t)(a >> 32)), "r"(m));
+    uint32_t t0, t1;
+    if constexpr (E < 32) {
+        // (q1:q0) + q2 * EPS < 2^65 - 2^33: one correction
+        uint64_t e;
+        asm("mul.wide.u32 %0, %1, 0xffffffff;" : "=l"(e) : "r"(q2));
+        asm("{\n\t"
+            ".reg .u32 c;\n\t"
+            "add.cc.u32      %0, %2, %4;\n\t"
+            "addc.cc.u32     %1, %3, %5;\n\t"
+            "addc.u32        c, 0, 0;\n\t"
+            "mad.lo.cc.u32   %0, c, 0xffffffff, %0;\n\t"
+            "addc.u32        %1, %1, 0;\n\t"
+            "}"
+            : "=&r"(t0), "=&r"(t1)
+            : "r"(q0), "r"(q1), "r"((uint32_t)e), "r"((uint32_t)(e >> 32)));
+    } else if constexpr (E < 64) {
+        // 2^32 q0 + q1 * EPS - q2 with a signed top limb in {-1, 0, 1}
+        uint64_t e;
+        asm("mul.wide.u32 %0, %1, 0xffffffff;" : "=l"(e) : "r"(q1));
+        asm("{\n\t"
+            ".reg .u32 top, cl, ch;\n\t"
+            "add.cc.u32      %1, %2, %4;\n\t"
+            "addc.u32        top, 0, 0;\n\t"
+            "sub.cc.u32      %0, %3, %5;\n\t"
+            "subc.cc.u32     %1, %1, 0;\n\t"
+            "subc.u32        top, top, 0;\n\t"
+            "neg.s32         cl, top;\n\t"
+            "shr.s32         ch, top, 31;\n\t"
+            "add.cc.u32      %0, %0, cl;\n\t"
+            "addc.u32        %1, %1, ch;\n\t"
+            "}"
+            : "=&r"(t0), "=&r"(t1)
+            : "r"(q0), "r"((uint32_t)e), "r"((uint32_t)(e >> 32)), "r"(q2));
+    } else {
+        // (q0 - q2) * 2^32 - q0 - q1, in (-2^64, 2^64): a borrow stands for
+        // -2^64 = -EPS, which can borrow once more
+        asm("{\n\t"
+            ".reg .u32 b;\n\t"
+            "sub.cc.u32      %0, 0, %2;\n\t"
+            "subc.cc.u32     %1, %2, %4;\n\t"
+            "subc.u32        b, 0, 0;\n\t"
+            "sub.cc.u32      %0, %0, %3;\n\t"
+            "subc.cc.u32     %1, %1, 0;\n\t"
+            "subc.u32        b, b, 0;\n\t"       // 0 or -1 (the value is above -2^64)
+            "sub.cc.u32      %0, %0, b;\n\t"     // b = -1 = EPS as a u32: subtract EPS
+            "subc.cc.u32     %1, %1, 0;\n\t"
+            "subc.u32        b, 0, 0;\n\t"
+            "sub.cc.u32      %0, %0, b;\n\t"
+            "subc.u32        %1, %1, 0;\n\t"
+            "}"
+            : "=&r"(t0), "=&r"(t1)
+            : "r"(q0), "r"(q1), "r"(q2));
+    }
+    return ((uint64_t)t1 << 32) | t0;
+}
+
+// In-register DIF on E = 2^LOGE values: natural input, bit-reversed output,
+// values lazily reduced.  Stages and butterflies are expanded at compile time
+// so every index and every shift amount is a constant (the values stay in
+// registers).  A twiddle w_{2^H}^I = 2^k with 96 <= k is -2^(k-96): the
+// difference is taken the other way round instead of negated.
 template <int INV, int H, int SPAN, int BLK, int I>
 __device__ __forceinline__ void dif_bfly(uint64_t *x)
 {
+    constexpr unsigned K = (root_exp(H, INV) * (unsigned)I) % 192u;
+    constexpr bool NEG = K >= 96;
+    constexpr unsigned E = NEG ? K - 96 : K;
     const uint64_t u = x[BLK + I], v = x[BLK + I + SPAN];
-    x[BLK + I] = ntt_add(u, v);
-    const uint64_t d = gl_sub(u, v);
-    x[BLK + I + SPAN] = I == 0 ? d : gl_mul_pow2(d, (root_exp(H, INV) * (unsigned)I) % 192u);
+    x[BLK + I] = ntt_add_nc(u, v);
+    const uint64_t d = NEG ? ntt_sub_nc(v, u) : ntt_sub_nc(u, v);
+    if constexpr (E == 0) x[BLK + I + SPAN] = d;
+    else x[BLK + I + SPAN] = ntt_mul_pow2_nc<E>(d);
     if constexpr (I + 1 < SPAN) dif_bfly<INV, H, SPAN, BLK, I + 1>(x);
 }
 
@@ -159,7 +293,7 @@ __device__ __forceinline__ void dif_substep(uint64_t *sm, uint32_t tile_elems, c
 #pragma unroll
             for (int p = 1; p < E; p++) {
                 const uint32_t f = bitrev32((uint32_t)p, LOGE);
-                x[p] = gl_mul(x[p], __ldg(tw_small + ((step * f) & 4095u)));
+                x[p] = gl_mul_nc(x[p], __ldg(tw_small + ((step * f) & 4095u)));
             }
         }
 #pragma unroll
@@ -204,7 +338,7 @@ __device__ __forceinline__ void first_substep_twiddles(uint64_t *x, uint32_t m_l
 #pragma unroll
         for (int p = 1; p < E; p++) {
             const uint32_t f = bitrev32((uint32_t)p, LOGE);
-            x[p] = gl_mul(x[p], __ldg(tw_small + ((step * f) & 4095u)));
+            x[p] = gl_mul_nc(x[p], __ldg(tw_small + ((step * f) & 4095u)));
         }
     }
 }
@@ -278,9 +412,9 @@ __global__ void __launch_bounds__(NT, 1024 / NT) ntt_pass_kernel(NttPassArgs a)
     // group member run m -> m + q are `step` positions apart
     auto load_elem = [&](uint64_t vcol, uint64_t pos) -> uint64_t {
         if (LOADM == LOAD_PLAIN) return a.src[vcol * a.src_stride + pos];
-        if (LOADM == LOAD_SCALE) return gl_mul(a.src[vcol * a.src_stride + pos], __ldg(a.tab + pos));
+        if (LOADM == LOAD_SCALE) return gl_mul_nc(a.src[vcol * a.src_stride + pos], __ldg(a.tab + pos));
         if (LOADM == LOAD_COSETS)
-            return gl_mul(a.src[(vcol >> a.rate) * a.src_stride + pos], __ldg(a.tab + ((vcol & rmask) << a.L) + pos));
+            return gl_mul_nc(a.src[(vcol >> a.rate) * a.src_stride + pos], __ldg(a.tab + ((vcol & rmask) << a.L) + pos));
         return pos < a.n_src ? a.src[vcol * a.src_stride + pos] : 0;  // LOAD_EXTEND
     };
     // pass twiddle (S > 1) and the store of one element
@@ -288,8 +422,9 @@ __global__ void __launch_bounds__(NT, 1024 / NT) ntt_pass_kernel(NttPassArgs a)
         if (S > 1) {
             const uint64_t o = pos & (S - 1);
             const uint64_t f = bitrev32(m, LOGR);
-            val = gl_mul(val, __ldg(a.tw_pass + o * f));
+            val = gl_mul_nc(val, __ldg(a.tw_pass + o * f));
         }
+        val = gl_canon(val);  // global memory holds canonical values
         if (STOREM == STORE_ROWS) {
             const uint64_t b = vcol >> a.rate;
             if (b < a.cols) {
@@ -395,6 +530,31 @@ __global__ void __launch_bounds__(NT, 1024 / NT) ntt_pass_kernel(NttPassArgs a)
         }
     }
 
+    if constexpr (STOREM == STORE_ROWS && NT == 256 && LOGR >= 4) {
+        // Row tile of 16 virtual columns (one coset, consecutive real columns)
+        // x 2^LOGR consecutive positions, the groups being whole rows of the
+        // tile (log_w == LOGR): thread (c, w0) writes column c of rows w0,
+        // w0 + 16, ...; a warp stores two 128-byte row segments per step.
+        // The destination advances by 16 rows per step and the shared-memory
+        // index by a compile-time constant (swz is linear over XOR, and c,
+        // w0 and the step occupy disjoint bits).
+        if (log_w == (uint32_t)LOGR && !a.dst_tab) {
+            const uint32_t c = threadIdx.x & 15u, w0 = threadIdx.x >> 4;
+            const uint64_t b = (v0 >> a.rate) + c;
+            if (b < a.cols) {
+                const uint64_t row0 = ((uint64_t)bitrev32((uint32_t)(v0 & rmask), a.rate) << a.L) + pos0 + w0;
+                uint64_t *d = a.dst + row0 * a.row_stride + b;
+                const uint64_t dstep = 16 * a.row_stride;
+                const uint32_t sb = swz((c << LOGR) + w0);
+#pragma unroll
+                for (uint32_t k = 0; k < R / 16; k++) {
+                    *d = gl_canon(sm[sb ^ swz_c(16 * k)]);
+                    d += dstep;
+                }
+            }
+            return;
+        }
+    }
     // ---- pass twiddle + store through shared memory
     for (uint32_t e = threadIdx.x; e < tile; e += NT) {
         uint32_t g, m;

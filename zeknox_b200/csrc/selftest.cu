@@ -90,6 +90,19 @@ __global__ void field_selftest_kernel(const uint64_t *__restrict__ a, const uint
         r[19] = gl_reduce128(x, y);
         r[20] = gl_reduce96(x, y & 0xFFFFFFFFULL);
         r[21] = gl_mul_pow2_lt64(x, (unsigned)(y % 64));
+        // the NTT passes' lazily reduced butterfly arithmetic
+        r[22] = gl_canon(ntt_add_nc(x, y));
+        r[23] = gl_canon(ntt_sub_nc(x, y));
+        r[24] = gl_canon(ntt_mul_pow2_nc<1>(x));
+        r[25] = gl_canon(ntt_mul_pow2_nc<24>(x));
+        r[26] = gl_canon(ntt_mul_pow2_nc<31>(x));
+        r[27] = gl_canon(ntt_mul_pow2_nc<32>(x));
+        r[28] = gl_canon(ntt_mul_pow2_nc<60>(x));
+        r[29] = gl_canon(ntt_mul_pow2_nc<63>(x));
+        r[30] = gl_canon(ntt_mul_pow2_nc<64>(x));
+        r[31] = gl_canon(ntt_mul_pow2_nc<72>(x));
+        r[32] = gl_canon(ntt_mul_pow2_nc<84>(x));
+        r[33] = gl_canon(ntt_mul_pow2_nc<95>(x));
 #pragma unroll
         for (int k = 0; k < ZK_SELFTEST_OPS; k++) out[k * n + i] = r[k];
     }

@@ -57,6 +57,7 @@ struct Server {
     uint64_t blocked_head = 0;  // head of the queue that waits for memory
     uint32_t bypassed = 0;      // small requests started ahead of it
     int inject_next = 0;        // test hook: the next start fails at this stage (ZK_SERVE_FAIL_*)
+    bool mem_wait = false;      // a start found the device full: admit nothing until a job finishes
     bool stop = false;
     std::thread worker;
 
@@ -68,12 +69,26 @@ struct Server {
                     commit_scratch_words(r.lg_n, r.rate_bits, r.cols, r.input_is_values != 0));
     }
 
+    static void release_buffers(Ticket &t, cudaStream_t s)
+    {
+        for (uint64_t **p : {&t.leaves, &t.digests, &t.caps, &t.scratch})
+            if (*p) {
+                (void)cudaFreeAsync(*p, s);
+                *p = nullptr;
+            }
+    }
+
+    // start() result: the device had no room for the job although the budget
+    // did (the request goes back to the head of the queue)
+    static constexpr int START_LATER = 0;
+
     // Allocate an admitted job's buffers and queue its whole commit on the
     // slot stream.  Runs on the server thread without `mu` (client threads
     // keep submitting, waiting and releasing meanwhile): a starting ticket can
     // be neither released nor cancelled, and only this thread starts jobs.
-    // Returns 1 when the work is queued, else a negative status, with anything
-    // allocated already returned on the stream.
+    // Returns 1 when the work is queued, START_LATER when the device is out of
+    // memory, else a negative status; on anything but 1, what it allocated is
+    // already returned on the stream.
     int start(Ticket &t, int slot, int inject)
     {
         const zk_serve_request &r = t.req;
@@ -94,11 +109,29 @@ struct Server {
             if (inject == ZK_SERVE_FAIL_SHAPE) j.cap_height = j.lg_n + j.rate_bits + 1;  // a shape that cannot commit
             if (inject == ZK_SERVE_FAIL_ALLOC)
                 throw cuda_failure(-(int)cudaErrorMemoryAllocation, "device allocation refused (injected)");
-            ZK_CUDA(cudaMallocAsync((void **)&t.leaves, N * r.cols * 8, s));
-            if (N > n_caps) ZK_CUDA(cudaMallocAsync((void **)&t.digests, (N - n_caps) * 64, s));
-            ZK_CUDA(cudaMallocAsync((void **)&t.caps, n_caps * 32, s));
             const uint64_t sw = commit_scratch_words(r.lg_n, r.rate_bits, r.cols, r.input_is_values != 0);
-            if (sw) ZK_CUDA(cudaMallocAsync((void **)&t.scratch, sw * 8, s));
+            auto allocate = [&]() -> cudaError_t {
+                cudaError_t e = cudaMallocAsync((void **)&t.leaves, N * r.cols * 8, s);
+                if (e == cudaSuccess && N > n_caps) e = cudaMallocAsync((void **)&t.digests, (N - n_caps) * 64, s);
+                if (e == cudaSuccess) e = cudaMallocAsync((void **)&t.caps, n_caps * 32, s);
+                if (e == cudaSuccess && sw) e = cudaMallocAsync((void **)&t.scratch, sw * 8, s);
+                if (e != cudaSuccess) {
+                    (void)cudaGetLastError();
+                    release_buffers(t, s);
+                }
+                return e;
+            };
+            cudaError_t ae = allocate();
+            if (ae == cudaErrorMemoryAllocation) {
+                // the budget fits but the device does not (memory held by the
+                // stream-ordered pool, or by other users of the GPU): give the
+                // pool's unused memory back to the driver and try once more
+                cudaMemPool_t pool;
+                if (cudaDeviceGetDefaultMemPool(&pool, ctx->id) == cudaSuccess) (void)cudaMemPoolTrimTo(pool, 0);
+                ae = allocate();
+            }
+            if (ae == cudaErrorMemoryAllocation) return START_LATER;
+            if (ae != cudaSuccess) throw cuda_failure(-(int)ae, "device allocation");
             j.leaves = t.leaves;
             j.digests = t.digests;
             j.caps = t.caps;
@@ -123,11 +156,7 @@ struct Server {
         } catch (const std::exception &e) {
             const cuda_failure *cf = dynamic_cast<const cuda_failure *>(&e);
             const arg_failure *af = dynamic_cast<const arg_failure *>(&e);
-            for (uint64_t **p : {&t.leaves, &t.digests, &t.caps, &t.scratch})
-                if (*p) {
-                    (void)cudaFreeAsync(*p, s);
-                    *p = nullptr;
-                }
+            release_buffers(t, s);
             if (t.done_ev) {
                 cudaEventDestroy(t.done_ev);
                 t.done_ev = nullptr;
@@ -158,9 +187,12 @@ struct Server {
                 completed++;
                 progressed = true;
             }
-            if (progressed) cv.notify_all();
+            if (progressed) {
+                mem_wait = false;
+                cv.notify_all();
+            }
             // admit in arrival order, small requests past a head that waits for memory
-            while (!queue.empty()) {
+            while (!queue.empty() && !mem_wait) {
                 int slot = -1;
                 for (size_t k = 0; k < slot_ticket.size(); k++)
                     if (!slot_ticket[k]) {
@@ -196,7 +228,23 @@ struct Server {
                 lk.unlock();
                 const int st = start(t, slot, inject);
                 lk.lock();
-                if (st < 0) {
+                if (st == START_LATER) {
+                    // device out of memory: back to the head of the queue until
+                    // a running job finishes; with none running it never fits
+                    in_use -= t.bytes;
+                    slot_ticket[slot] = 0;
+                    bool running = false;
+                    for (uint64_t other : slot_ticket) running |= other != 0;
+                    if (running) {
+                        t.status = 0;
+                        queue.push_front(id);
+                        mem_wait = true;
+                        break;
+                    }
+                    t.status = -(int)cudaErrorMemoryAllocation;
+                    t.t_done = Clock::now();
+                    t.bytes = 0;
+                } else if (st < 0) {
                     // could not start: the slot and the memory are free again
                     t.status = st;
                     t.t_done = Clock::now();
