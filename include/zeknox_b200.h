@@ -118,10 +118,12 @@ RustError zeknox_lde_rows_noalloc(size_t device_id, uint64_t *rows, const uint64
 
 /* ---- Serving: continuous batching of commit requests on one GPU ----
  *
- * A server owns a device-memory budget and `slots` streams.  Requests
- * (zk_serve_request) are queued by any host thread; a server thread admits
- * them in arrival order whenever a slot is free and the job's memory (its
- * leaves, digests, caps and scratch) fits the budget -- while the head waits
+ * A server owns a device-memory budget, reserved as one allocation when it is
+ * created (jobs then never call the driver's allocator), and `slots` streams.
+ * Requests (zk_serve_request) are queued by any host thread; a server thread
+ * admits them in arrival order whenever a slot is free and the job's memory
+ * (its leaves, digests, caps and scratch, one contiguous range of the
+ * reservation) fits -- while the head waits
  * for memory, up to `slots` small requests (<= budget / 8) behind it that fit
  * may start first -- runs the commit on the slot's stream -- so admitted jobs
  * overlap on the device -- copies the caps to the request's host buffer, and
@@ -162,12 +164,13 @@ RustError zeknox_server_wait(void *server, uint64_t ticket, double timeout_ms, z
  * ZK_SERVE_CANCELLED.  A request that has started cannot be cancelled. */
 RustError zeknox_server_cancel(void *server, uint64_t ticket);
 /* Test hook (failure injection on the host, no GPU fault): the next request
- * the server starts fails at `stage` -- ZK_SERVE_FAIL_ALLOC: its device
- * allocation is refused (status -cudaErrorMemoryAllocation);
+ * the server starts fails at `stage` -- ZK_SERVE_FAIL_ALLOC: as if its device
+ * memory were refused (status -cudaErrorMemoryAllocation);
  * ZK_SERVE_FAIL_SHAPE: its shape is rejected when it starts (status -1);
  * ZK_SERVE_FAIL_LAUNCH: queuing its kernels fails after its buffers were
- * allocated (status -cudaErrorLaunchFailure).  The failed request's memory
- * and slot are freed at once; later requests are unaffected.  0 clears. */
+ * placed in the budget (status -cudaErrorLaunchFailure).  The failed
+ * request's memory and slot are freed at once; later requests are
+ * unaffected.  0 clears. */
 #define ZK_SERVE_FAIL_ALLOC 1
 #define ZK_SERVE_FAIL_SHAPE 2
 #define ZK_SERVE_FAIL_LAUNCH 3

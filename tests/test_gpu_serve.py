@@ -58,11 +58,13 @@ def test_rejects_request_larger_than_budget():
 
 
 def job_bytes(lg, rate, cols, cap):
-    """The server's accounting of one request's device memory."""
+    """The server's accounting of one request's device memory: leaves,
+    digests, caps and LDE scratch, each rounded up to 256 bytes."""
     N, caps = 1 << (lg + rate), 1 << cap
     t = torch.zeros(1, dtype=torch.int64)
     words = zk.commit_scratch_words(zk.commit_job(lg, rate, cols, cap, 0, t, t, t, t))
-    return 8 * (N * cols + 8 * (N - caps) + 4 * caps + words)
+    up = lambda b: (b + 255) // 256 * 256
+    return up(8 * N * cols) + up(64 * (N - caps)) + up(32 * caps) + up(8 * words)
 
 
 def test_small_request_passes_a_head_that_waits_for_memory():

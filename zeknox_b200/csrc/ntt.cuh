@@ -273,6 +273,14 @@ struct NttPassArgs {
 // second term a compile-time constant.
 __host__ __device__ constexpr uint32_t swz_c(uint32_t w) { return w ^ (((w >> 4) ^ (w >> 8) ^ (w >> 12)) & 15u); }
 
+// bits-bit reversal of a compile-time value
+__host__ __device__ constexpr uint32_t bitrev_c(uint32_t x, int bits)
+{
+    uint32_t r = 0;
+    for (int i = 0; i < bits; i++) r |= ((x >> i) & 1u) << (bits - 1 - i);
+    return r;
+}
+
 template <int LOGE, int INV, int NT, int LOG_RCUR>
 __device__ __forceinline__ void dif_substep(uint64_t *sm, uint32_t tile_elems, const uint64_t *__restrict__ tw_small)
 {
@@ -523,8 +531,20 @@ __global__ void __launch_bounds__(NT, 1024 / NT) ntt_pass_kernel(NttPassArgs a)
                 dif_regs<LAST, INV>(x);
                 uint64_t vcol, pos;
                 gpos(g, mb, vcol, pos);
+                if (vcol >= a.vcols) continue;
+                if (S > 1) {
+                    // member mb + e sits at pos + e * S, all at offset o = pos mod S,
+                    // and rev(mb + e) = rev(mb) + rev(e): one table row per task,
+                    // compile-time strides along it
+                    const uint64_t o = pos & (S - 1);
+                    const uint64_t *twb = a.tw_pass + o * bitrev32(mb, LOGR);
 #pragma unroll
-                for (int e = 0; e < (int)EL; e++) store_elem(vcol, pos + ((uint64_t)e << s_lo), mb + e, x[e]);
+                    for (int e = 1; e < (int)EL; e++) x[e] = gl_mul_nc(x[e], __ldg(twb + o * bitrev_c((uint32_t)e, LOGR)));
+                    x[0] = gl_mul_nc(x[0], __ldg(twb));
+                }
+                uint64_t *d = a.dst + vcol * a.dst_stride + pos;
+#pragma unroll
+                for (int e = 0; e < (int)EL; e++) d[(uint64_t)e << s_lo] = gl_canon(x[e]);
             }
             return;
         }

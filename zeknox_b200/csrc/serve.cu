@@ -2,16 +2,23 @@
 //
 // Host side: any thread submits requests into a FIFO; one server thread per
 // server admits the head of the queue whenever a slot stream is idle and the
-// job's device memory fits the budget, enqueues the whole commit (allocation,
-// LDE, Merkle, caps copy-out) on that slot's stream, and polls the slot
-// events to retire finished jobs.  While the head waits for memory (not for a
-// slot), small requests behind it (at most 1/8 of the budget each) that fit
-// now may start ahead of it, at most `slots` of them per waiting head: a large
-// request then holds up no small one, and waits for at most `slots` small
-// ones itself.  Device side: jobs on different slots overlap; twiddle, coset
-// and round-constant tables stay resident in the device context across
-// requests (small requests on high-priority streams measured lower delivered
-// throughput and a 8x higher p50 on the 16-request stream).
+// job's device memory fits, enqueues the whole commit (LDE, Merkle, caps
+// copy-out) on that slot's stream, and polls the slot events to retire
+// finished jobs.  While the head waits for memory (not for a slot), small
+// requests behind it (at most 1/8 of the budget each) that fit now may start
+// ahead of it, at most `slots` of them per waiting head: a large request then
+// holds up no small one, and waits for at most `slots` small ones itself.
+//
+// Memory: the budget is one device allocation made when the server is
+// created (an arena), and every job takes one contiguous range of it
+// (first fit, freed ranges merged with their neighbours).  Jobs therefore
+// never call the driver's allocator, and a job the budget admits always has
+// the memory: per-job stream-ordered allocations of multi-GB buffers measured
+// out-of-memory failures and long allocation stalls at this size mix.
+//
+// Device side: jobs on different slots overlap; twiddle, coset and
+// round-constant tables stay resident in the device context across requests
+// (zeknox_server_prepare builds them ahead of the stream).
 #include <cuda_runtime.h>
 #include <string.h>
 
@@ -33,12 +40,61 @@ namespace {
 
 using Clock = std::chrono::steady_clock;
 
+constexpr uint64_t ARENA_ALIGN = 256;
+constexpr uint64_t NO_RANGE = ~0ULL;
+
+uint64_t align_up(uint64_t x) { return (x + ARENA_ALIGN - 1) / ARENA_ALIGN * ARENA_ALIGN; }
+
+// First-fit allocator over the byte offsets of the arena.
+struct RangeAlloc {
+    std::map<uint64_t, uint64_t> free_;  // offset -> size
+    void init(uint64_t size)
+    {
+        free_.clear();
+        if (size) free_[0] = size;
+    }
+    uint64_t take(uint64_t size)
+    {
+        for (auto it = free_.begin(); it != free_.end(); ++it) {
+            if (it->second < size) continue;
+            const uint64_t off = it->first, rest = it->second - size;
+            free_.erase(it);
+            if (rest) free_[off + size] = rest;
+            return off;
+        }
+        return NO_RANGE;
+    }
+    bool fits(uint64_t size) const
+    {
+        for (const auto &kv : free_)
+            if (kv.second >= size) return true;
+        return false;
+    }
+    void give(uint64_t off, uint64_t size)
+    {
+        auto it = free_.emplace(off, size).first;
+        auto nx = std::next(it);
+        if (nx != free_.end() && it->first + it->second == nx->first) {
+            it->second += nx->second;
+            free_.erase(nx);
+        }
+        if (it != free_.begin()) {
+            auto pv = std::prev(it);
+            if (pv->first + pv->second == it->first) {
+                pv->second += it->second;
+                free_.erase(it);
+            }
+        }
+    }
+};
+
 struct Ticket {
     zk_serve_request req;
     Clock::time_point t_submit, t_admit, t_done;
     int status = 0;  // 0 queued, 1 running, 2 done, < 0 failed or cancelled
     int slot = -1;
-    uint64_t bytes = 0;
+    uint64_t bytes = 0;        // arena bytes of the job (aligned pieces)
+    uint64_t off = NO_RANGE;   // its range in the arena while admitted
     uint64_t *leaves = nullptr, *digests = nullptr, *caps = nullptr, *scratch = nullptr;
     cudaEvent_t done_ev = nullptr;
 };
@@ -46,6 +102,8 @@ struct Ticket {
 struct Server {
     DeviceCtx *ctx = nullptr;
     uint64_t budget = 0, in_use = 0, peak = 0, completed = 0;
+    uint8_t *arena = nullptr;
+    RangeAlloc ranges;
     std::vector<cudaStream_t> slot_stream;
     std::vector<uint64_t> slot_ticket;  // 0 = idle
     cudaEvent_t tables_ready = nullptr; // recorded on the context stream after a start's table builds
@@ -57,43 +115,57 @@ struct Server {
     uint64_t blocked_head = 0;  // head of the queue that waits for memory
     uint32_t bypassed = 0;      // small requests started ahead of it
     int inject_next = 0;        // test hook: the next start fails at this stage (ZK_SERVE_FAIL_*)
-    bool mem_wait = false;      // a start found the device full: admit nothing until a job finishes
     bool stop = false;
     std::thread worker;
 
+    // Arena bytes of a job: leaves, digests, caps and LDE scratch, each
+    // starting on an ARENA_ALIGN boundary.
     static uint64_t job_bytes(const zk_serve_request &r)
     {
         const uint64_t N = 1ULL << (r.lg_n + r.rate_bits);
         const uint64_t caps = 1ULL << r.cap_height;
-        return 8 * (N * r.cols + 8 * (N - caps) + 4 * caps +
-                    commit_scratch_words(r.lg_n, r.rate_bits, r.cols, r.input_is_values != 0));
+        return align_up(8 * N * r.cols) + align_up(64 * (N - caps)) + align_up(32 * caps) +
+               align_up(8 * commit_scratch_words(r.lg_n, r.rate_bits, r.cols, r.input_is_values != 0));
     }
 
-    static void release_buffers(Ticket &t, cudaStream_t s)
+    void place(Ticket &t)
     {
-        for (uint64_t **p : {&t.leaves, &t.digests, &t.caps, &t.scratch})
-            if (*p) {
-                (void)cudaFreeAsync(*p, s);
-                *p = nullptr;
-            }
+        const zk_serve_request &r = t.req;
+        const uint64_t N = 1ULL << (r.lg_n + r.rate_bits);
+        const uint64_t n_caps = 1ULL << r.cap_height;
+        const uint64_t sw = commit_scratch_words(r.lg_n, r.rate_bits, r.cols, r.input_is_values != 0);
+        uint8_t *p = arena + t.off;
+        t.leaves = (uint64_t *)p;
+        p += align_up(8 * N * r.cols);
+        t.digests = N > n_caps ? (uint64_t *)p : nullptr;
+        p += align_up(64 * (N - n_caps));
+        t.caps = (uint64_t *)p;
+        p += align_up(32 * n_caps);
+        t.scratch = sw ? (uint64_t *)p : nullptr;
     }
 
-    // start() result: the device had no room for the job although the budget
-    // did (the request goes back to the head of the queue)
-    static constexpr int START_LATER = 0;
+    // Give an admitted job's range back (caller holds mu; nothing on the GPU
+    // may still use it).
+    void unadmit(Ticket &t)
+    {
+        if (t.off != NO_RANGE) {
+            ranges.give(t.off, t.bytes);
+            in_use -= t.bytes;
+            t.off = NO_RANGE;
+        }
+        t.leaves = t.digests = t.caps = t.scratch = nullptr;
+    }
 
-    // Allocate an admitted job's buffers and queue its whole commit on the
-    // slot stream.  Runs on the server thread without `mu` (client threads
-    // keep submitting, waiting and releasing meanwhile): a starting ticket can
-    // be neither released nor cancelled, and only this thread starts jobs.
-    // Returns 1 when the work is queued, START_LATER when the device is out of
-    // memory, else a negative status; on anything but 1, what it allocated is
-    // already returned on the stream.
+    // Queue an admitted job's whole commit on its slot stream.  Runs on the
+    // server thread without `mu` (client threads keep submitting, waiting and
+    // releasing meanwhile): a starting ticket can be neither released nor
+    // cancelled, and only this thread starts jobs.  Returns 1 when the work is
+    // queued, else a negative status (the slot stream has then finished
+    // whatever this start queued, so the range may be reused at once).
     int start(Ticket &t, int slot, int inject)
     {
         const zk_serve_request &r = t.req;
         cudaStream_t s = slot_stream[slot];
-        const uint64_t N = 1ULL << (r.lg_n + r.rate_bits);
         const uint64_t n_caps = 1ULL << r.cap_height;
         std::lock_guard<std::recursive_mutex> lk(ctx->mu);
         try {
@@ -106,35 +178,12 @@ struct Server {
             j.input_is_values = r.input_is_values;
             j.coset_gen = r.coset_gen;
             j.input = r.input;
-            if (inject == ZK_SERVE_FAIL_SHAPE) j.cap_height = j.lg_n + j.rate_bits + 1;  // a shape that cannot commit
-            if (inject == ZK_SERVE_FAIL_ALLOC)
-                throw cuda_failure(-(int)cudaErrorMemoryAllocation, "device allocation refused (injected)");
-            const uint64_t sw = commit_scratch_words(r.lg_n, r.rate_bits, r.cols, r.input_is_values != 0);
-            auto allocate = [&]() -> cudaError_t {
-                cudaError_t e = cudaMallocAsync((void **)&t.leaves, N * r.cols * 8, s);
-                if (e == cudaSuccess && N > n_caps) e = cudaMallocAsync((void **)&t.digests, (N - n_caps) * 64, s);
-                if (e == cudaSuccess) e = cudaMallocAsync((void **)&t.caps, n_caps * 32, s);
-                if (e == cudaSuccess && sw) e = cudaMallocAsync((void **)&t.scratch, sw * 8, s);
-                if (e != cudaSuccess) {
-                    (void)cudaGetLastError();
-                    release_buffers(t, s);
-                }
-                return e;
-            };
-            cudaError_t ae = allocate();
-            if (ae == cudaErrorMemoryAllocation) {
-                // the budget fits but the device does not (memory held by the
-                // stream-ordered pool, or by other users of the GPU): give the
-                // pool's unused memory back to the driver and try once more
-                cudaMemPool_t pool;
-                if (cudaDeviceGetDefaultMemPool(&pool, ctx->id) == cudaSuccess) (void)cudaMemPoolTrimTo(pool, 0);
-                ae = allocate();
-            }
-            if (ae == cudaErrorMemoryAllocation) return START_LATER;
-            if (ae != cudaSuccess) throw cuda_failure(-(int)ae, "device allocation");
             j.leaves = t.leaves;
             j.digests = t.digests;
             j.caps = t.caps;
+            if (inject == ZK_SERVE_FAIL_SHAPE) j.cap_height = j.lg_n + j.rate_bits + 1;  // a shape that cannot commit
+            if (inject == ZK_SERVE_FAIL_ALLOC)
+                throw cuda_failure(-(int)cudaErrorMemoryAllocation, "device allocation refused (injected)");
             check_job(j);
             // tables this shape reads that are not resident yet are built on
             // the context stream; the slot stream waits for them on the
@@ -145,10 +194,6 @@ struct Server {
             if (inject == ZK_SERVE_FAIL_LAUNCH)
                 throw cuda_failure(-(int)cudaErrorLaunchFailure, "kernel launch refused (injected)");
             commit_enqueue(*ctx, j, s, t.scratch);
-            if (t.scratch) {
-                ZK_CUDA(cudaFreeAsync(t.scratch, s));
-                t.scratch = nullptr;
-            }
             if (r.caps_host) ZK_CUDA(cudaMemcpyAsync(r.caps_host, t.caps, n_caps * 32, cudaMemcpyDeviceToHost, s));
             ZK_CUDA(cudaEventCreateWithFlags(&t.done_ev, cudaEventDisableTiming));
             ZK_CUDA(cudaEventRecord(t.done_ev, s));
@@ -156,12 +201,12 @@ struct Server {
         } catch (const std::exception &e) {
             const cuda_failure *cf = dynamic_cast<const cuda_failure *>(&e);
             const arg_failure *af = dynamic_cast<const arg_failure *>(&e);
-            release_buffers(t, s);
+            (void)cudaStreamSynchronize(s);  // whatever was queued finishes before the range is reused
+            (void)cudaGetLastError();
             if (t.done_ev) {
                 cudaEventDestroy(t.done_ev);
                 t.done_ev = nullptr;
             }
-            (void)cudaGetLastError();
             return cf ? (cf->code < 0 ? cf->code : -1) : af ? -af->code : -1;
         }
     }
@@ -187,12 +232,9 @@ struct Server {
                 completed++;
                 progressed = true;
             }
-            if (progressed) {
-                mem_wait = false;
-                cv.notify_all();
-            }
+            if (progressed) cv.notify_all();
             // admit in arrival order, small requests past a head that waits for memory
-            while (!queue.empty() && !mem_wait) {
+            while (!queue.empty()) {
                 int slot = -1;
                 for (size_t k = 0; k < slot_ticket.size(); k++)
                     if (!slot_ticket[k]) {
@@ -201,7 +243,7 @@ struct Server {
                     }
                 if (slot < 0) break;
                 auto pick = queue.begin();
-                if (in_use + tickets[*pick].bytes > budget) {
+                if (!ranges.fits(tickets[*pick].bytes)) {
                     if (blocked_head != *pick) {
                         blocked_head = *pick;
                         bypassed = 0;
@@ -209,7 +251,7 @@ struct Server {
                     if (bypassed >= slot_ticket.size()) break;
                     for (++pick; pick != queue.end(); ++pick) {
                         const uint64_t b = tickets[*pick].bytes;
-                        if (b <= budget / 8 && in_use + b <= budget) break;
+                        if (b <= budget / 8 && ranges.fits(b)) break;
                     }
                     if (pick == queue.end()) break;
                     bypassed++;
@@ -217,8 +259,10 @@ struct Server {
                 const uint64_t id = *pick;
                 Ticket &t = tickets[id];
                 queue.erase(pick);
+                t.off = ranges.take(t.bytes);
                 in_use += t.bytes;
                 peak = in_use > peak ? in_use : peak;
+                place(t);
                 t.slot = slot;
                 t.t_admit = Clock::now();
                 t.status = 1;
@@ -228,28 +272,11 @@ struct Server {
                 lk.unlock();
                 const int st = start(t, slot, inject);
                 lk.lock();
-                if (st == START_LATER) {
-                    // device out of memory: back to the head of the queue until
-                    // a running job finishes; with none running it never fits
-                    in_use -= t.bytes;
-                    slot_ticket[slot] = 0;
-                    bool running = false;
-                    for (uint64_t other : slot_ticket) running |= other != 0;
-                    if (running) {
-                        t.status = 0;
-                        queue.push_front(id);
-                        mem_wait = true;
-                        break;
-                    }
-                    t.status = -(int)cudaErrorMemoryAllocation;
-                    t.t_done = Clock::now();
-                    t.bytes = 0;
-                } else if (st < 0) {
-                    // could not start: the slot and the memory are free again
+                if (st < 0) {
+                    // could not start: the slot and the range are free again
                     t.status = st;
                     t.t_done = Clock::now();
-                    in_use -= t.bytes;
-                    t.bytes = 0;
+                    unadmit(t);
                     slot_ticket[slot] = 0;
                 }
                 cv.notify_all();
@@ -307,14 +334,33 @@ extern "C" RustError zeknox_server_create(size_t device_id, uint64_t budget_byte
     return zk::guard([&] {
         if (!server) throw zk::arg_failure("null out pointer");
         if (slots == 0 || slots > 64) throw zk::arg_failure("slots must be 1..64");
+        if (budget_bytes < zk::ARENA_ALIGN) throw zk::arg_failure("budget below one allocation unit");
         zk::DeviceCtx &c = zk::device(device_id);
         Server *s = new Server();
-        s->ctx = &c;
-        s->budget = budget_bytes;
-        s->slot_stream.resize(slots);
-        s->slot_ticket.assign(slots, 0);
-        for (auto &st : s->slot_stream) ZK_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
-        ZK_CUDA(cudaEventCreateWithFlags(&s->tables_ready, cudaEventDisableTiming));
+        try {
+            s->ctx = &c;
+            s->budget = budget_bytes / zk::ARENA_ALIGN * zk::ARENA_ALIGN;
+            {
+                std::lock_guard<std::recursive_mutex> dl(c.mu);
+                // the pool's cached temporaries go back to the driver first, so
+                // the reservation sees the device's free memory
+                cudaMemPool_t pool;
+                if (cudaDeviceGetDefaultMemPool(&pool, c.id) == cudaSuccess) (void)cudaMemPoolTrimTo(pool, 0);
+                ZK_CUDA(cudaMalloc((void **)&s->arena, s->budget));
+            }
+            s->ranges.init(s->budget);
+            s->slot_stream.assign(slots, nullptr);
+            s->slot_ticket.assign(slots, 0);
+            for (auto &st : s->slot_stream) ZK_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+            ZK_CUDA(cudaEventCreateWithFlags(&s->tables_ready, cudaEventDisableTiming));
+        } catch (...) {
+            for (auto &st : s->slot_stream)
+                if (st) cudaStreamDestroy(st);
+            if (s->tables_ready) cudaEventDestroy(s->tables_ready);
+            if (s->arena) cudaFree(s->arena);
+            delete s;
+            throw;
+        }
         s->worker = std::thread([s] {
             cudaSetDevice(s->ctx->id);
             s->loop();
@@ -386,14 +432,7 @@ extern "C" RustError zeknox_server_release(void *server, uint64_t ticket)
         if (it == s->tickets.end()) throw zk::arg_failure("unknown ticket");
         zk::Ticket &t = it->second;
         if (t.status == 0 || t.status == 1) throw zk::arg_failure("ticket still queued or running");
-        {
-            std::lock_guard<std::recursive_mutex> dl(s->ctx->mu);
-            ZK_CUDA(cudaSetDevice(s->ctx->id));
-            cudaStream_t st = t.slot >= 0 ? s->slot_stream[t.slot] : s->ctx->stream;
-            for (uint64_t *p : {t.leaves, t.digests, t.caps, t.scratch})
-                if (p) (void)cudaFreeAsync(p, st);
-        }
-        s->in_use -= t.bytes;
+        s->unadmit(t);  // its work has finished: the range is free at once
         s->tickets.erase(it);
         s->cv.notify_all();
     });
@@ -447,8 +486,7 @@ extern "C" RustError zeknox_server_cancel(void *server, uint64_t ticket)
                 break;
             }
         if (s->blocked_head == ticket) s->blocked_head = 0;
-        t.status = ZK_SERVE_CANCELLED;
-        t.bytes = 0;  // never admitted: nothing was counted against the budget
+        t.status = ZK_SERVE_CANCELLED;  // never admitted: it holds no range
         t.t_done = t.t_admit = zk::Clock::now();
         s->cv.notify_all();
     });
@@ -476,14 +514,12 @@ extern "C" RustError zeknox_server_destroy(void *server)
         s->worker.join();
         std::lock_guard<std::recursive_mutex> dl(s->ctx->mu);
         ZK_CUDA(cudaSetDevice(s->ctx->id));
-        for (auto &kv : s->tickets)
-            for (uint64_t *p : {kv.second.leaves, kv.second.digests, kv.second.caps, kv.second.scratch})
-                if (p) (void)cudaFreeAsync(p, s->slot_stream[kv.second.slot >= 0 ? kv.second.slot : 0]);
         for (auto &st : s->slot_stream) {
             cudaStreamSynchronize(st);
             cudaStreamDestroy(st);
         }
         cudaEventDestroy(s->tables_ready);
+        cudaFree(s->arena);
         delete s;
     });
 }
