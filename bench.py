@@ -493,15 +493,18 @@ def measure_batch(steps, budget_gb):
             b.record()
             torch.cuda.synchronize()
             t_batch += a.elapsed_time(b) / steps
-        # plain path, same jobs and buffers
+        # plain path, same jobs and buffers; the caller's evaluation buffer
+        # (the LDE output the transpose reads) is allocated once, outside the
+        # timed region, at the wave's largest job
+        ev_all = torch.empty(max((1 << (jb["lg_n"] + jb["rate"])) * jb["cols"] for jb in wave), dtype=torch.int64,
+                             device="cuda")
         for _ in range(steps):
             a.record()
             for jb, (inp, leaves, dig, caps, n_dig, n_cap) in zip(wave, bufs):
                 N = 1 << (jb["lg_n"] + jb["rate"])
-                ev = torch.empty(N * jb["cols"], dtype=torch.int64, device="cuda")
+                ev = ev_all[:N * jb["cols"]]
                 zk.lde_batch(0, ev, inp, jb["lg_n"], jb["cols"], jb["rate"], with_coset=True)
                 zk.transpose_rev_batch(0, leaves, ev, jb["lg_n"] + jb["rate"], jb["cols"])
-                del ev
                 zk.fill_digests_buf_linear_gpu(dig, caps, leaves, N, jb["cols"], jb["cap"], jb["hash"])
                 torch.cuda.synchronize()
             b.record()
@@ -509,7 +512,7 @@ def measure_batch(steps, budget_gb):
             t_plain += a.elapsed_time(b) / steps
         for cb, bb in zip(caps_b, bufs):
             assert torch.equal(cb, bb[3]), "batched and plain commitments differ"
-        del bufs, cjobs, caps_b
+        del bufs, cjobs, caps_b, ev_all
         torch.cuda.empty_cache()
     rate = poseidon_perm_rate()
     floor_ms = total_perms / rate * 1e3

@@ -531,20 +531,8 @@ __global__ void __launch_bounds__(NT, 1024 / NT) ntt_pass_kernel(NttPassArgs a)
                 dif_regs<LAST, INV>(x);
                 uint64_t vcol, pos;
                 gpos(g, mb, vcol, pos);
-                if (vcol >= a.vcols) continue;
-                if (S > 1) {
-                    // member mb + e sits at pos + e * S, all at offset o = pos mod S,
-                    // and rev(mb + e) = rev(mb) + rev(e): one table row per task,
-                    // compile-time strides along it
-                    const uint64_t o = pos & (S - 1);
-                    const uint64_t *twb = a.tw_pass + o * bitrev32(mb, LOGR);
 #pragma unroll
-                    for (int e = 1; e < (int)EL; e++) x[e] = gl_mul_nc(x[e], __ldg(twb + o * bitrev_c((uint32_t)e, LOGR)));
-                    x[0] = gl_mul_nc(x[0], __ldg(twb));
-                }
-                uint64_t *d = a.dst + vcol * a.dst_stride + pos;
-#pragma unroll
-                for (int e = 0; e < (int)EL; e++) d[(uint64_t)e << s_lo] = gl_canon(x[e]);
+                for (int e = 0; e < (int)EL; e++) store_elem(vcol, pos + ((uint64_t)e << s_lo), mb + e, x[e]);
             }
             return;
         }
