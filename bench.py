@@ -498,7 +498,7 @@ def measure_batch(steps, budget_gb):
         # timed region, at the wave's largest job
         ev_all = torch.empty(max((1 << (jb["lg_n"] + jb["rate"])) * jb["cols"] for jb in wave), dtype=torch.int64,
                              device="cuda")
-        for _ in range(steps):
+        for it in range(steps + 1):  # the first pass is untimed: tables, pool growth
             a.record()
             for jb, (inp, leaves, dig, caps, n_dig, n_cap) in zip(wave, bufs):
                 N = 1 << (jb["lg_n"] + jb["rate"])
@@ -509,7 +509,8 @@ def measure_batch(steps, budget_gb):
                 torch.cuda.synchronize()
             b.record()
             torch.cuda.synchronize()
-            t_plain += a.elapsed_time(b) / steps
+            if it:
+                t_plain += a.elapsed_time(b) / steps
         for cb, bb in zip(caps_b, bufs):
             assert torch.equal(cb, bb[3]), "batched and plain commitments differ"
         del bufs, cjobs, caps_b, ev_all
