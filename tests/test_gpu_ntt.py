@@ -79,7 +79,8 @@ def test_custom_coset_generator():
         zk.init_coset(0, 20, 7)
 
 
-@pytest.mark.parametrize("lg,b", [(0, 3), (1, 1), (5, 3), (6, 31), (10, 33), (12, 256), (17, 7), (20, 2)])
+@pytest.mark.parametrize("lg,b", [(0, 3), (1, 1), (1, 2), (5, 3), (6, 30), (6, 31), (10, 33), (12, 256), (17, 7),
+                                  (20, 2)])
 def test_transpose_rev(lg, b):
     x = O.field_data(lg + b, b << lg)
     out = torch.zeros(b << lg, dtype=torch.int64, device="cuda")
@@ -96,6 +97,21 @@ def test_transpose_rev(lg, b):
     zk.transpose_rev(0, out3, src, lg, b, stream=s.cuda_stream)
     s.synchronize()
     assert torch.equal(out, out3)
+
+
+@pytest.mark.parametrize("lg,b", [(9, 64), (12, 6)])
+def test_transpose_rev_unaligned_buffers(lg, b):
+    """Buffers that start 8 bytes past a 16-byte boundary take the 8-byte
+    form; both forms give the oracle's matrix."""
+    x = O.field_data(77 + lg, b << lg)
+    src = torch.zeros((b << lg) + 1, dtype=torch.int64, device="cuda")
+    src[1:] = to_dev(x)
+    out = torch.zeros((b << lg) + 1, dtype=torch.int64, device="cuda")
+    zk.transpose_rev_batch(0, out[1:], src[1:], lg, b)
+    assert np.array_equal(to_np(out[1:]), O.transpose_rev(x, lg, b))
+    aligned = torch.zeros(b << lg, dtype=torch.int64, device="cuda")
+    zk.transpose_rev_batch(0, aligned, src[1:], lg, b)
+    assert torch.equal(aligned, out[1:])
 
 
 def test_argument_errors():

@@ -476,7 +476,9 @@ void transpose_rev_device(DeviceCtx &c, uint64_t *out, const uint64_t *in, uint3
     if (cols == 0) return;
     dim3 grid((unsigned)((n + 63) / 64), (unsigned)((cols + 31) / 32));
     if (grid.y > 65535) throw arg_failure("too many columns for transpose");
-    transpose_rev_kernel<<<grid, 256, 0, c.stream>>>(in, out, lg, cols);
+    const bool vec16 = lg >= 1 && cols % 2 == 0 && ((uintptr_t)in % 16) == 0 && ((uintptr_t)out % 16) == 0;
+    if (vec16) transpose_rev_v2_kernel<<<grid, 256, 0, c.stream>>>(in, out, lg, cols);
+    else transpose_rev_kernel<<<grid, 256, 0, c.stream>>>(in, out, lg, cols);
     note_launch();
     ZK_CUDA(cudaGetLastError());
 }
