@@ -287,16 +287,28 @@ def run_ours(args, rank, world):
     mk_t = statistics.median(mk_ms) * 1e-3
     hbm, hbm_src = peaks()
     lde_bytes = 8 * (n + N) * COLS
-    traffic = None
+    traffic, prof = None, {}
     try:
         with open(os.path.join(ROOT, "profiles", "ncu_traffic.json")) as f:
-            traffic = json.load(f).get("lde_rows_config2_bytes_per_call")
+            prof = json.load(f)
+        traffic = prof.get("lde_rows_config2_bytes_per_call")
     except Exception:
         pass
     roofline = {"bound": "hbm", "kernel": "ntt_pass_kernel x2 (fused coset LDE -> leaf rows)",
                 "achieved": lde_bytes / lde_t / 1e9, "peak": hbm, "unit": "GB/s",
                 "frac": lde_bytes / lde_t / 1e9 / hbm, "traffic": traffic, "peak_source": hbm_src + " hbm_gbs",
                 "algorithmic_bytes": lde_bytes, "ms": lde_t * 1e3}
+    # the fused LDE's integer roofline: its executed instructions per output
+    # element (ncu, profiles/) against the instruction floor of its
+    # arithmetic (the primitives' measured costs times their counts per
+    # element), and the ALU pipe's utilisation in that capture
+    roofline_lde_int = None
+    if prof.get("lde_rows_config2_inst_per_elem"):
+        inst, floor = prof["lde_rows_config2_inst_per_elem"], prof["lde_rows_inst_floor_per_elem"]
+        roofline_lde_int = {"bound": "int issue (ALU pipe)", "achieved_inst_per_elem": inst,
+                            "floor_inst_per_elem": floor, "frac": floor / inst,
+                            "alu_pipe_pct": prof.get("lde_rows_config2_alu_pipe_pct"),
+                            "source": "ncu capture of one call (profiles/lde_rows_lg15_rate3.md)"}
     # compute_transpose_rev of the workload's evaluations (column-major 256 x
     # 2^18 -> bit-reversed leaf-major), the HBM-bound kernel of the unfused path
     ev_cols = torch.empty(N * COLS, dtype=torch.int64, device="cuda")
@@ -312,7 +324,7 @@ def run_ours(args, rank, world):
             tr_ms.append(a.elapsed_time(b))
     tr_t = statistics.median(tr_ms) * 1e-3
     tr_bytes = 16 * N * COLS
-    roofline_transpose = {"bound": "hbm", "kernel": "transpose_rev_kernel (compute_transpose_rev, 256 x 2^18)",
+    roofline_transpose = {"bound": "hbm", "kernel": "transpose_rev_v2_kernel (compute_transpose_rev, 256 x 2^18)",
                           "achieved": tr_bytes / tr_t / 1e9, "peak": hbm, "unit": "GB/s",
                           "frac": tr_bytes / tr_t / 1e9 / hbm, "algorithmic_bytes": tr_bytes, "ms": tr_t * 1e3,
                           "peak_source": hbm_src + " hbm_gbs"}
@@ -353,7 +365,8 @@ def run_ours(args, rank, world):
             "metric": METRIC, "value": value, "unit": "elems/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "u64", "data": "synthetic (seeded splitmix64 field elements)",
-            "config": config_dict(), "roofline": roofline, "roofline_hash": roofline_hash,
+            "config": config_dict(), "roofline": roofline, "roofline_lde_int": roofline_lde_int,
+            "roofline_hash": roofline_hash,
             "roofline_transpose": roofline_transpose, "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": "elems/s", "h2d_bytes_per_step": COLS * n * 8,
                     "d2h_bytes_per_step": n_cap * 32},
