@@ -1,9 +1,9 @@
 """The headline commit (256 columns x 2^15, rate 3, Poseidon2, cap height 4)
 through the reference's own CUDA library and through this one on the same
 GPU: the caps must be identical bit for bit (a full-size parity check against
-the reference itself), and this library's fused commit must not be slower
-than the reference's compute_batched_lde -> compute_transpose_rev ->
-fill_digests_buf_linear_gpu_with_gpu_ptr sequence.
+the reference itself), and this library's fused commit must be at least 1.3x
+faster than the reference's compute_batched_lde -> compute_transpose_rev ->
+fill_digests_buf_linear_gpu_with_gpu_ptr sequence (the forests likewise).
 
 The reference library is oracle/_ref/libzeknox_ref_gpu.so, compiled from the
 reference sources for sm_100a by `make -C oracle ref_gpu`; the test is skipped
@@ -97,7 +97,8 @@ def test_headline_commit_matches_and_beats_reference_cuda_path():
     assert torch.equal(caps, ref_caps)
     assert torch.equal(dig, ref_dig)
     print("headline commit: reference CUDA path %.2f ms, this library %.2f ms (%.2fx)" % (t_ref, t_ours, t_ref / t_ours))
-    assert t_ours <= t_ref
+    # measured 1.6-7.9x on B200; 1.3x leaves room for a noisy shared GPU
+    assert t_ours * 1.3 <= t_ref, (t_ref, t_ours)
 
 
 @pytest.mark.skipif(not os.path.exists(REF_GPU), reason="reference CUDA library not built (make -C oracle ref_gpu)")
@@ -107,7 +108,7 @@ def test_forest_matches_and_beats_reference_cuda_path(h, n_leaves, leaf_size, ca
     """The alternative-hash forests (2^20 leaves x 135, cap height 4) and the
     8192 x 84 Poseidon tree through the reference's
     fill_digests_buf_linear_gpu_with_gpu_ptr and this library's: identical
-    digests and caps, and this library no slower."""
+    digests and caps, and this library at least 1.3x faster."""
     R = ref_lib()
     leaves = uniform_field(n_leaves * leaf_size, 100 + h)
     n_dig, n_cap = zk.merkle_sizes(n_leaves, cap)
@@ -129,4 +130,5 @@ def test_forest_matches_and_beats_reference_cuda_path(h, n_leaves, leaf_size, ca
     assert torch.equal(dig, ref_dig)
     print("forest hash %d, %d x %d: reference %.2f ms, this library %.2f ms (%.2fx)" %
           (h, n_leaves, leaf_size, t_ref, t_ours, t_ref / t_ours))
-    assert t_ours <= t_ref
+    # measured 1.6-7.9x on B200; 1.3x leaves room for a noisy shared GPU
+    assert t_ours * 1.3 <= t_ref, (t_ref, t_ours)

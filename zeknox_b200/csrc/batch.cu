@@ -49,6 +49,7 @@ void prepare_job(DeviceCtx &c, const zk_commit_job &j)
 
 void commit_enqueue(DeviceCtx &c, const zk_commit_job &j, cudaStream_t s, uint64_t *scratch, bool host_input)
 {
+    NvtxRange range("zeknox commit");
     const uint64_t n = 1ULL << j.lg_n;
     const uint64_t N = n << j.rate_bits;
     cudaStream_t keep = c.stream;
@@ -215,6 +216,7 @@ static void run_graph(DeviceCtx &c, std::vector<uint64_t> key, uint32_t njobs, c
 
 void commit_batch_graph(DeviceCtx &c, const zk_commit_job *jobs, uint32_t njobs)
 {
+    NvtxRange range("zeknox commit_batch");
     if (njobs == 0) return;
     std::vector<double> cost(njobs);
     std::vector<uint64_t> words(njobs);
@@ -232,6 +234,7 @@ void commit_batch_graph(DeviceCtx &c, const zk_commit_job *jobs, uint32_t njobs)
 
 void merkle_batch_graph(DeviceCtx &c, const zk_merkle_job *jobs, uint32_t njobs)
 {
+    NvtxRange range("zeknox merkle_batch");
     if (njobs == 0) return;
     std::vector<double> cost(njobs);
     std::vector<uint64_t> words(njobs, 0);

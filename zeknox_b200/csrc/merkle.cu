@@ -112,6 +112,7 @@ bool merkle_device(uint64_t *digests, uint64_t *caps, const uint64_t *leaves, ui
                    uint64_t n_leaves, uint64_t leaf_size, uint64_t cap_height, uint64_t hash_type, cudaStream_t stream,
                    std::string &err)
 {
+    NvtxRange range("zeknox merkle");
     if (!merkle_geometry_ok(n_digests, n_caps, n_leaves, cap_height, err)) return false;
     if (n_caps > 0xFFFFFFFFULL) {
         err = "too many caps";

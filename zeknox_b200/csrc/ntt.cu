@@ -231,6 +231,7 @@ static void reorder(DeviceCtx &c, const uint64_t *src, uint64_t src_stride, uint
 void ntt_batch_device(DeviceCtx &c, uint64_t *inout, uint32_t lg, uint64_t batches, bool inverse, bool with_coset,
                       uint64_t *scratch)
 {
+    NvtxRange range("zeknox ntt");
     const uint64_t n = 1ULL << lg;
     if (batches == 0) return;
     DevBuf tmp;
@@ -272,6 +273,7 @@ void ntt_batch_device(DeviceCtx &c, uint64_t *inout, uint32_t lg, uint64_t batch
 void lde_batch_device(DeviceCtx &c, uint64_t *out, const uint64_t *in, uint32_t lg_n, uint32_t rate, uint64_t batches,
                       bool inverse, bool with_coset)
 {
+    NvtxRange range("zeknox lde");
     const uint64_t n = 1ULL << lg_n;
     const uint32_t lgN = lg_n + rate;
     const uint64_t N = 1ULL << lgN;
@@ -401,6 +403,7 @@ uint64_t lde_rows_scratch_elems(uint32_t lg_n, uint32_t rate, uint64_t cols)
 void lde_rows_device(DeviceCtx &c, uint64_t *rows, const uint64_t *coeffs, uint32_t lg_n, uint32_t rate, uint64_t cols,
                      uint64_t coset_gen, uint64_t *scratch, const uint64_t *host_coeffs, const RowScatter *scatter)
 {
+    NvtxRange range("zeknox lde_rows");
     const uint64_t n = 1ULL << lg_n;
     if (cols == 0) return;
     const bool multi = plan_passes(lg_n, true).size() > 1;
@@ -472,6 +475,7 @@ void prepare_tables(DeviceCtx &c, uint32_t lg_n, uint32_t rate, uint64_t coset_g
 
 void transpose_rev_device(DeviceCtx &c, uint64_t *out, const uint64_t *in, uint32_t lg, uint64_t cols)
 {
+    NvtxRange range("zeknox transpose_rev");
     const uint64_t n = 1ULL << lg;
     if (cols == 0) return;
     dim3 grid((unsigned)((n + 63) / 64), (unsigned)((cols + 31) / 32));

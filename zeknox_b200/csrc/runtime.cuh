@@ -11,6 +11,7 @@
 //     stream and are returned on the same stream.
 #pragma once
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 #include <stdint.h>
 
 #include <map>
@@ -102,6 +103,16 @@ void tune_load_file(const char *path);
 // key, so a graph captured under other knob values is not replayed.
 uint64_t tune_generation();
 constexpr uint32_t TUNE_ANY = 0xFFFFFFFFu;
+
+// NVTX range over a host-side stage (queuing an LDE, a forest, a commit, a
+// batch): a profiler that records NVTX (nsys, ncu's NVTX filters) shows the
+// stages by name; without one attached a range costs a few nanoseconds.
+struct NvtxRange {
+    explicit NvtxRange(const char *name) { nvtxRangePushA(name); }
+    ~NvtxRange() { nvtxRangePop(); }
+    NvtxRange(const NvtxRange &) = delete;
+    NvtxRange &operator=(const NvtxRange &) = delete;
+};
 
 // Count of kernels this library has launched (diagnostics: zeknox_launch_count).
 void note_launch(uint64_t n = 1);

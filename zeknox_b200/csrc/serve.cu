@@ -167,6 +167,7 @@ struct Server {
         const zk_serve_request &r = t.req;
         cudaStream_t s = slot_stream[slot];
         const uint64_t n_caps = 1ULL << r.cap_height;
+        NvtxRange range("zeknox serve start");
         std::lock_guard<std::recursive_mutex> lk(ctx->mu);
         try {
             zk_commit_job j{};
