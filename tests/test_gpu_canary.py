@@ -14,7 +14,7 @@ from tests.helpers import HASHES, to_dev, to_np
 pytestmark = pytest.mark.gpu
 
 GUARD = 512  # words on each side
-PATTERN = 0x5A5A5A5AA5A5A5A5 - (1 << 64)  # int64 view of the guard word
+PATTERN = 0x5A5A5A5AA5A5A5A5  # the guard word (a valid int64)
 
 
 def guarded(n):
