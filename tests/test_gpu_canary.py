@@ -18,8 +18,11 @@ PATTERN = 0x5A5A5A5AA5A5A5A5  # the guard word (a valid int64)
 
 
 def guarded(n):
-    """(whole buffer, interior view of n words)."""
+    """(whole buffer, interior view of n words): guards of PATTERN, interior
+    zero (Keccak leaves of < 4 words leave the rest of their digest as the
+    buffer held it, zero in the oracle's)."""
     t = torch.full((n + 2 * GUARD,), PATTERN, dtype=torch.int64, device="cuda")
+    t[GUARD:GUARD + n] = 0
     return t, t[GUARD:GUARD + n]
 
 
