@@ -368,21 +368,21 @@ __device__ __forceinline__ void first_substep_twiddles(uint64_t *x, uint32_t m_l
 // for STORE_SAME, the last sub-step stores straight from registers, instead of
 // separate load / store loops through shared memory.
 // Threads per SM the register budget aims at: 1280 (five 256-thread CTAs, 48
-// registers) for column-output passes of up to 2^9 points, 1024 (64
-// registers) for the row-output pass and the larger radices, which spill at
-// 48.  Measured on B200: fused LDE 1.065 against 1.101 ms at 256 x 2^15, rate 3
-// (4% fewer stalls on the first pass's loads); five CTAs for every pass (the
-// row pass then spills): 1.068 ms; six for column passes (40 registers,
-// spilling): 1.091 ms; 8-point register sub-steps at 40 or 64 registers:
-// 1.18-1.23 ms.
-template <int LOGR, int STOREM>
+// registers) for the LDE's coset-expanding column pass of up to 2^9 points,
+// whose first sub-step waits on its global loads; 1024 (64 registers)
+// otherwise.  Measured on B200: fused LDE 1.065 against 1.101 ms at 256 x
+// 2^15, rate 3; five CTAs for every pass (the row pass then spills): 1.068 ms,
+// and for every column pass the plain NTT's passes measured 1-4% slower; six
+// (40 registers, spilling): 1.091 ms; 8-point register sub-steps at 40 or 64
+// registers: 1.18-1.23 ms.  Radices of 2^10 and above spill at 48 registers.
+template <int LOGR, int LOADM, int STOREM>
 __host__ __device__ constexpr int pass_threads_per_sm()
 {
-    return (STOREM == STORE_ROWS || LOGR >= 10) ? 1024 : 1280;
+    return (LOADM == LOAD_COSETS && STOREM == STORE_SAME && LOGR < 10) ? 1280 : 1024;
 }
 
 template <int LOGR, int INV, int NT, int TILE, int LOADM, int STOREM, int DIRECT>
-__global__ void __launch_bounds__(NT, pass_threads_per_sm<LOGR, STOREM>() / NT) ntt_pass_kernel(NttPassArgs a)
+__global__ void __launch_bounds__(NT, pass_threads_per_sm<LOGR, LOADM, STOREM>() / NT) ntt_pass_kernel(NttPassArgs a)
 {
     extern __shared__ uint64_t sm[];
     constexpr uint32_t R = 1u << LOGR;
