@@ -237,6 +237,17 @@ RustError zeknox_field_selftest(size_t device_id, const uint64_t *a, const uint6
 RustError zeknox_permute(size_t device_id, uint64_t *states, uint64_t n, uint32_t hash_type, uint32_t cooperative,
                          void *stream);
 
+/* The checked build (make -C zeknox_b200 checked -> libzeknox_checked.so)
+ * tests every global-memory index of the NTT, reorder, transpose and Merkle
+ * kernels against the extent of its buffer and skips an access out of range
+ * (no trap: the context stays usable).  This call waits for the device and
+ * returns the accesses skipped since the last call: record[0] = count,
+ * record[1] = the first one's site (OobSite in csrc/bounds.cuh), record[2]
+ * its index, record[3] the extent; and clears them.  In the normal build it
+ * returns +cudaErrorNotSupported with a zero record.  No reference
+ * counterpart (a sanitizer stand-in). */
+RustError zeknox_bounds_report(size_t device_id, uint64_t *record);
+
 /* Number of kernels this library has launched so far in the process. */
 uint64_t zeknox_launch_count(void);
 

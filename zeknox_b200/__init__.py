@@ -17,7 +17,9 @@ import ctypes
 import os
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "libzeknox.so")
+# ZEKNOX_LIB selects another build of the library, e.g. libzeknox_checked.so
+# (range checks on every kernel's global accesses, zeknox_bounds_report)
+LIB_PATH = os.environ.get("ZEKNOX_LIB") or os.path.join(HERE, "libzeknox.so")
 
 P = 0xFFFFFFFF00000001
 HASH_POSEIDON, HASH_KECCAK, HASH_POSEIDON_BN128, HASH_POSEIDON2, HASH_MONOLITH = 0, 1, 2, 3, 4
@@ -41,7 +43,7 @@ EXT_SYMBOLS = ["zeknox_last_error", "zeknox_commit", "zeknox_commit_batch", "zek
                "zeknox_server_release", "zeknox_server_stats", "zeknox_server_destroy", "zeknox_server_prepare",
                "zeknox_server_cancel", "zeknox_server_inject_failure", "zeknox_tune_set",
                "zeknox_tune_get", "zeknox_tune_clear", "zeknox_tune_load", "zeknox_transpose_rev",
-               "zeknox_lde_rows_scatter", "zeknox_field_selftest", "zeknox_permute"]
+               "zeknox_lde_rows_scatter", "zeknox_field_selftest", "zeknox_permute", "zeknox_bounds_report"]
 
 # Tuning table measured on B200 by ``python -m zeknox_b200.autotune``; loaded
 # by load() unless ZEKNOX_TUNE_FILE names another table ("" or "none": no table).
@@ -206,6 +208,8 @@ def load():
     L.zeknox_lde_rows_scatter.restype = RustError
     L.zeknox_field_selftest.restype = RustError
     L.zeknox_field_selftest.argtypes = [sz, vp, vp, vp, u64, vp, vp]
+    L.zeknox_bounds_report.restype = RustError
+    L.zeknox_bounds_report.argtypes = [sz, ctypes.POINTER(ctypes.c_uint64)]
     L.zeknox_permute.restype = RustError
     L.zeknox_permute.argtypes = [sz, vp, u64, u32, u32, vp]
     L.zeknox_lde_rows_scatter.argtypes = [sz, ctypes.POINTER(ctypes.c_void_p), u32, vp, u32, u32, u32, u32, u32, u64, vp]
@@ -440,6 +444,19 @@ def field_selftest(device_id, a, b, c, out, stream=None):
     _check(load().zeknox_field_selftest(device_id, _ptr(a), _ptr(b), _ptr(c), n, _ptr(out),
                                         ctypes.c_void_p(stream) if stream else None))
     return out
+
+
+def bounds_report(device_id=0):
+    """zeknox_bounds_report: (checked, [count, site, index, extent]) -- the
+    out-of-range accesses the checked build's kernels skipped since the last
+    report (checked is False for the normal build, whose record is zero)."""
+    rec = (ctypes.c_uint64 * 4)()
+    err = load().zeknox_bounds_report(device_id, rec)
+    if err.message:
+        _libc.free(err.message)
+    if err.code not in (0, 801):  # 801: cudaErrorNotSupported, the normal build
+        raise ZeknoxError(err.code, "zeknox_bounds_report")
+    return err.code == 0, [int(v) for v in rec]
 
 
 def permute(device_id, states, hash_type, cooperative=False, stream=None):

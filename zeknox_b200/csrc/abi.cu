@@ -17,6 +17,7 @@
 #include "../../include/lib.h"
 #include "../../include/zeknox_b200.h"
 #include "batch.cuh"
+#include "bounds.cuh"
 #include "geom.h"
 #include "gl64.cuh"
 #include "multi_split.h"
@@ -646,6 +647,34 @@ extern "C" RustError zeknox_lde_rows(size_t device_id, uint64_t *rows, const uin
         }
         c.stream = keep;
         if (!stream) c.sync();
+    });
+}
+
+// Out-of-range accesses the checked build's kernels skipped on this device
+// since the last report: record = {count, first site, its index, its extent}.
+extern "C" RustError zeknox_bounds_report(size_t device_id, uint64_t *record)
+{
+    if (!zk::BOUNDS_CHECKED) {
+        if (record) record[0] = record[1] = record[2] = record[3] = 0;
+        return fail((int)cudaErrorNotSupported, "range checks are compiled only into libzeknox_checked.so");
+    }
+    return guarded([&] {
+        if (!record) throw zk::arg_failure("null record");
+        zk::DeviceCtx &c = zk::device(device_id);
+        std::lock_guard<std::recursive_mutex> lk(c.mu);
+        ZK_CUDA(cudaDeviceSynchronize());  // every queued kernel has recorded what it skipped
+        uint64_t total[4] = {0, 0, 0, 0};
+        for (auto take : {zk::oob_take_ntt, zk::oob_take_merkle, zk::oob_take_noalloc}) {
+            uint64_t r[4];
+            ZK_CUDA(take(r));
+            if (r[0] && !total[0]) {
+                total[1] = r[1];
+                total[2] = r[2];
+                total[3] = r[3];
+            }
+            total[0] += r[0];
+        }
+        for (int k = 0; k < 4; k++) record[k] = total[k];
     });
 }
 

@@ -143,4 +143,6 @@ bool merkle_device(uint64_t *digests, uint64_t *caps, const uint64_t *leaves, ui
     return true;
 }
 
+cudaError_t oob_take_merkle(uint64_t r[4]) { return oob_take_local(r); }
+
 }  // namespace zk

@@ -19,6 +19,7 @@
 #pragma once
 #include <stdint.h>
 
+#include "bounds.cuh"
 #include "coop.cuh"
 #include "hash.cuh"
 
@@ -42,6 +43,11 @@ __device__ __forceinline__ uint64_t merkle_node_index(const MerkleGeom &g, uint6
     return k * g.sub_digests + (level_nodes - 2) + (in_sub >> level_u);
 }
 
+// Words of the digest buffer and of the leaves (the extents the checked build
+// tests accesses against).
+__device__ __forceinline__ uint64_t merkle_digest_words(const MerkleGeom &g) { return 4 * (uint64_t)g.n_caps * g.sub_digests; }
+__device__ __forceinline__ uint64_t merkle_leaf_words(const MerkleGeom &g) { return g.n_leaves * g.leaf_size; }
+
 template <int H>
 __device__ __forceinline__ void leaf_hash(const uint64_t *__restrict__ row, uint64_t len, uint64_t out[4])
 {
@@ -58,6 +64,10 @@ __device__ __forceinline__ void merkle_leaf_body(const uint64_t *__restrict__ le
     if (i >= g.n_leaves) return;
     // caps == leaves: the leaf hashes are the caps, digests untouched
     uint64_t *dst = g.sub_leaves == 1 ? caps + 4 * i : digests + 4 * merkle_node_index(g, i, 0);
+    if (g.sub_leaves == 1 ? !ZK_IN_BOUNDS(4 * i + 3, 4 * (uint64_t)g.n_caps, OOB_MERKLE_CAP)
+                          : !ZK_IN_BOUNDS(4 * merkle_node_index(g, i, 0) + 3, merkle_digest_words(g), OOB_MERKLE_DIGEST))
+        return;
+    if (g.leaf_size && !ZK_IN_BOUNDS((i + 1) * g.leaf_size - 1, merkle_leaf_words(g), OOB_MERKLE_LEAF)) return;
     uint64_t d[4];
     if (H == HASH_KECCAK && g.leaf_size < 4) {
         // Keccak copies a < 4-word leaf and leaves the other digest words as
@@ -107,10 +117,14 @@ __global__ void __launch_bounds__(T, 1024 / T)
         uint64_t h[4];
         if (t < nodes) {
             const uint64_t *src = v == 0 ? leaves + (i0 + t) * g.leaf_size : &nd[2 * t][0];
-            sponge_hash_one<H>(src, v == 0 ? g.leaf_size : 8, h);
+            const bool row_ok =
+                v != 0 || ZK_IN_BOUNDS((i0 + t + 1) * g.leaf_size - 1, merkle_leaf_words(g), OOB_MERKLE_LEAF);
+            if (row_ok) sponge_hash_one<H>(src, v == 0 ? g.leaf_size : 8, h);
             const uint64_t di = merkle_node_index(g, i0 + ((uint64_t)t << v), (uint32_t)v);
+            if (row_ok && ZK_IN_BOUNDS(4 * di + 3, merkle_digest_words(g), OOB_MERKLE_DIGEST)) {
 #pragma unroll
-            for (int q = 0; q < 4; q++) digests[4 * di + q] = h[q];
+                for (int q = 0; q < 4; q++) digests[4 * di + q] = h[q];
+            }
         }
         __syncthreads();
         if (t < nodes) {
@@ -145,8 +159,9 @@ __global__ void __launch_bounds__(T) merkle_fold_kernel(uint64_t *__restrict__ d
     const uint64_t cta_nodes = count - i0 < (uint64_t)T ? count - i0 : (uint64_t)T;
     if (t < cta_nodes) {
         const uint64_t di = merkle_node_index(g, (i0 + t) << u0, u0);
+        const bool ok = ZK_IN_BOUNDS(4 * di + 3, merkle_digest_words(g), OOB_MERKLE_NODE);
 #pragma unroll
-        for (int q = 0; q < 4; q++) node[t][q] = digests[4 * di + q];
+        for (int q = 0; q < 4; q++) node[t][q] = ok ? digests[4 * di + q] : 0;
     }
     const uint32_t top = g.log_sub - 1;  // highest stored height
     uint32_t U = 0;
@@ -159,8 +174,10 @@ __global__ void __launch_bounds__(T) merkle_fold_kernel(uint64_t *__restrict__ d
         if (act) {
             hash_two<H>(node[2 * t], node[2 * t + 1], h);
             const uint64_t di = merkle_node_index(g, (i0 + ((uint64_t)t << v)) << u0, u0 + v);
+            if (ZK_IN_BOUNDS(4 * di + 3, merkle_digest_words(g), OOB_MERKLE_DIGEST)) {
 #pragma unroll
-            for (int q = 0; q < 4; q++) digests[4 * di + q] = h[q];
+                for (int q = 0; q < 4; q++) digests[4 * di + q] = h[q];
+            }
         }
         __syncthreads();
         if (act) {
@@ -176,8 +193,10 @@ __global__ void __launch_bounds__(T) merkle_fold_kernel(uint64_t *__restrict__ d
             uint64_t h[4];
             hash_two<H>(node[2 * t], node[2 * t + 1], h);
             const uint64_t k = ((i0 << u0) >> g.log_sub) + t;
+            if (ZK_IN_BOUNDS(4 * k + 3, 4 * (uint64_t)g.n_caps, OOB_MERKLE_CAP)) {
 #pragma unroll
-            for (int q = 0; q < 4; q++) caps[4 * k + q] = h[q];
+                for (int q = 0; q < 4; q++) caps[4 * k + q] = h[q];
+            }
         }
     }
 }
@@ -193,10 +212,13 @@ __global__ void __launch_bounds__(256) merkle_tail_kernel(uint64_t *__restrict__
     __shared__ uint64_t bufb[MAXM / 2][4];
     const uint64_t k = blockIdx.x;
     uint64_t *sub = digests + k * g.sub_digests * 4;
+    const uint64_t sub0 = k * g.sub_digests * 4;  // sub's first word in the digest buffer
     uint32_t m = (uint32_t)(g.sub_leaves >> u0);
-    for (uint32_t j = threadIdx.x; j < m; j += blockDim.x)
+    for (uint32_t j = threadIdx.x; j < m; j += blockDim.x) {
+        const bool ok = ZK_IN_BOUNDS(sub0 + 4 * (m - 2 + j) + 3, merkle_digest_words(g), OOB_MERKLE_NODE);
 #pragma unroll
-        for (int q = 0; q < 4; q++) bufa[j][q] = sub[4 * (m - 2 + j) + q];
+        for (int q = 0; q < 4; q++) bufa[j][q] = ok ? sub[4 * (m - 2 + j) + q] : 0;
+    }
     uint64_t(*src)[4] = bufa;
     uint64_t(*dst)[4] = bufb;
     while (m > 2) {
@@ -205,9 +227,10 @@ __global__ void __launch_bounds__(256) merkle_tail_kernel(uint64_t *__restrict__
         for (uint32_t j = threadIdx.x; j < half; j += blockDim.x) {
             uint64_t h[4];
             hash_two<H>(src[2 * j], src[2 * j + 1], h);
+            const bool ok = ZK_IN_BOUNDS(sub0 + 4 * (half - 2 + j) + 3, merkle_digest_words(g), OOB_MERKLE_DIGEST);
 #pragma unroll
             for (int q = 0; q < 4; q++) {
-                sub[4 * (half - 2 + j) + q] = h[q];
+                if (ok) sub[4 * (half - 2 + j) + q] = h[q];
                 dst[j][q] = h[q];
             }
         }
@@ -220,8 +243,10 @@ __global__ void __launch_bounds__(256) merkle_tail_kernel(uint64_t *__restrict__
     if (threadIdx.x == 0) {
         uint64_t h[4];
         hash_two<H>(src[0], src[1], h);
+        if (ZK_IN_BOUNDS(4 * k + 3, 4 * (uint64_t)g.n_caps, OOB_MERKLE_CAP)) {
 #pragma unroll
-        for (int q = 0; q < 4; q++) caps[4 * k + q] = h[q];
+            for (int q = 0; q < 4; q++) caps[4 * k + q] = h[q];
+        }
     }
 }
 
@@ -235,6 +260,10 @@ __global__ void merkle_level_kernel(uint64_t *__restrict__ digests, MerkleGeom g
         uint64_t k = x / per_sub, j = x % per_sub;
         uint64_t *sub = digests + k * g.sub_digests * 4;
         uint64_t start = per_sub - 2, child = 2 * per_sub - 2;
+        const uint64_t sub0 = k * g.sub_digests * 4;
+        if (!ZK_IN_BOUNDS(sub0 + 4 * (child + 2 * j + 1) + 3, merkle_digest_words(g), OOB_MERKLE_NODE) ||
+            !ZK_IN_BOUNDS(sub0 + 4 * (start + j) + 3, merkle_digest_words(g), OOB_MERKLE_DIGEST))
+            continue;
         uint64_t h[4];
         hash_two<H>(sub + 4 * (child + 2 * j), sub + 4 * (child + 2 * j + 1), h);
 #pragma unroll
@@ -264,8 +293,14 @@ __global__ void __launch_bounds__(T)
     if ((gi & ~7ULL) >= g.n_leaves) return;  // the whole warp is past the end
     const uint64_t i = gi < g.n_leaves ? gi : g.n_leaves - 1;
     uint64_t d[4];
-    sponge_hash_one_coop<H>(leaves + i * g.leaf_size, g.leaf_size, d, c);
-    if (c.q == 0 && gi < g.n_leaves) {
+    // (every thread of the warp runs the permutation: a row out of range is
+    // hashed from row 0 and its digest not written)
+    const bool row_ok = !g.leaf_size || ZK_IN_BOUNDS((i + 1) * g.leaf_size - 1, merkle_leaf_words(g), OOB_MERKLE_LEAF);
+    sponge_hash_one_coop<H>(leaves + (row_ok ? i : 0) * g.leaf_size, g.leaf_size, d, c);
+    const bool dst_ok = g.sub_leaves == 1
+                            ? ZK_IN_BOUNDS(4 * gi + 3, 4 * (uint64_t)g.n_caps, OOB_MERKLE_CAP)
+                            : ZK_IN_BOUNDS(4 * merkle_node_index(g, gi, 0) + 3, merkle_digest_words(g), OOB_MERKLE_DIGEST);
+    if (c.q == 0 && gi < g.n_leaves && row_ok && dst_ok) {
         uint64_t *dst = g.sub_leaves == 1 ? caps + 4 * gi : digests + 4 * merkle_node_index(g, gi, 0);
 #pragma unroll
         for (int q = 0; q < 4; q++) dst[q] = d[q];
@@ -286,8 +321,10 @@ __global__ void __launch_bounds__(T) merkle_fold_coop_kernel(uint64_t *__restric
     const uint64_t count = g.n_leaves >> u0;
     const uint64_t i0 = (uint64_t)blockIdx.x * NG;
     const uint64_t cta_nodes = count - i0 < (uint64_t)NG ? count - i0 : (uint64_t)NG;
-    for (uint32_t t = threadIdx.x; t < 4 * cta_nodes; t += T)
-        node[t >> 2][t & 3] = digests[4 * merkle_node_index(g, (i0 + (t >> 2)) << u0, u0) + (t & 3)];
+    for (uint32_t t = threadIdx.x; t < 4 * cta_nodes; t += T) {
+        const uint64_t wi = 4 * merkle_node_index(g, (i0 + (t >> 2)) << u0, u0) + (t & 3);
+        node[t >> 2][t & 3] = ZK_IN_BOUNDS(wi, merkle_digest_words(g), OOB_MERKLE_NODE) ? digests[wi] : 0;
+    }
     const uint32_t top = g.log_sub - 1;
     uint32_t U = 0;
     while ((1u << (U + 1)) <= NG && u0 + U + 1 <= top) U++;
@@ -302,8 +339,10 @@ __global__ void __launch_bounds__(T) merkle_fold_coop_kernel(uint64_t *__restric
             sponge_hash_two_coop<H>(node[2 * src], node[2 * src + 1], h, c);
             if (act && c.q == 0) {
                 const uint64_t di = merkle_node_index(g, (i0 + ((uint64_t)grp << v)) << u0, u0 + v);
+                if (ZK_IN_BOUNDS(4 * di + 3, merkle_digest_words(g), OOB_MERKLE_DIGEST)) {
 #pragma unroll
-                for (int q = 0; q < 4; q++) digests[4 * di + q] = h[q];
+                    for (int q = 0; q < 4; q++) digests[4 * di + q] = h[q];
+                }
             }
         }
         __syncthreads();
@@ -323,8 +362,10 @@ __global__ void __launch_bounds__(T) merkle_fold_coop_kernel(uint64_t *__restric
             sponge_hash_two_coop<H>(node[2 * src], node[2 * src + 1], h, c);
             if (act && c.q == 0) {
                 const uint64_t k = ((i0 << u0) >> g.log_sub) + grp;
+                if (ZK_IN_BOUNDS(4 * k + 3, 4 * (uint64_t)g.n_caps, OOB_MERKLE_CAP)) {
 #pragma unroll
-                for (int q = 0; q < 4; q++) caps[4 * k + q] = h[q];
+                    for (int q = 0; q < 4; q++) caps[4 * k + q] = h[q];
+                }
             }
         }
     }
@@ -344,8 +385,11 @@ __global__ void __launch_bounds__(256) merkle_tail_coop_kernel(uint64_t *__restr
     const uint32_t grp = threadIdx.x >> 2;
     const uint64_t k = blockIdx.x;
     uint64_t *sub = digests + k * g.sub_digests * 4;
+    const uint64_t sub0 = k * g.sub_digests * 4;
     uint32_t m = (uint32_t)(g.sub_leaves >> u0);
-    for (uint32_t j = threadIdx.x; j < 4 * m; j += 256) bufa[j >> 2][j & 3] = sub[4 * (m - 2) + j];
+    for (uint32_t j = threadIdx.x; j < 4 * m; j += 256)
+        bufa[j >> 2][j & 3] =
+            ZK_IN_BOUNDS(sub0 + 4 * (m - 2) + j, merkle_digest_words(g), OOB_MERKLE_NODE) ? sub[4 * (m - 2) + j] : 0;
     uint64_t(*src)[4] = bufa;
     uint64_t(*dst)[4] = bufb;
     while (m > 2) {
@@ -358,9 +402,10 @@ __global__ void __launch_bounds__(256) merkle_tail_coop_kernel(uint64_t *__restr
             uint64_t h[4];
             sponge_hash_two_coop<H>(src[2 * jj], src[2 * jj + 1], h, c);
             if (act && c.q == 0) {
+                const bool ok = ZK_IN_BOUNDS(sub0 + 4 * (half - 2 + j) + 3, merkle_digest_words(g), OOB_MERKLE_DIGEST);
 #pragma unroll
                 for (int q = 0; q < 4; q++) {
-                    sub[4 * (half - 2 + j) + q] = h[q];
+                    if (ok) sub[4 * (half - 2 + j) + q] = h[q];
                     dst[j][q] = h[q];
                 }
             }
@@ -374,7 +419,7 @@ __global__ void __launch_bounds__(256) merkle_tail_coop_kernel(uint64_t *__restr
     if (threadIdx.x < 32) {
         uint64_t h[4];
         sponge_hash_two_coop<H>(src[0], src[1], h, c);
-        if (threadIdx.x == 0) {
+        if (threadIdx.x == 0 && ZK_IN_BOUNDS(4 * k + 3, 4 * (uint64_t)g.n_caps, OOB_MERKLE_CAP)) {
 #pragma unroll
             for (int q = 0; q < 4; q++) caps[4 * k + q] = h[q];
         }

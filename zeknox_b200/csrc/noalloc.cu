@@ -167,3 +167,7 @@ extern "C" RustError zeknox_lde_rows_noalloc(size_t device_id, uint64_t *rows, c
     }
     return r;
 }
+
+namespace zk {
+cudaError_t oob_take_noalloc(uint64_t r[4]) { return oob_take_local(r); }
+}  // namespace zk

@@ -139,6 +139,9 @@ struct DifJob {
     uint64_t *scratch;
     const RowScatter *scatter;  // row output over several buffers (null: dst)
     uint64_t col0;              // first column of this chunk (scattered row output)
+    // extents in words of src, dst (each scatter destination), tab and
+    // scratch, read only by the checked build's range checks
+    uint64_t src_len, dst_len, tab_len, scratch_len;
 };
 
 static void run_dif(DeviceCtx &c, const DifJob &j)
@@ -155,6 +158,8 @@ static void run_dif(DeviceCtx &c, const DifJob &j)
         const bool first = pi == 0, last = pi + 1 == passes.size();
         NttPassArgs a{};
         a.src = first ? j.src : (j.rows ? j.scratch : j.dst);
+        a.src_len = first ? j.src_len : (j.rows ? j.scratch_len : j.dst_len);
+        a.tab_len = j.tab_len;
         a.src_stride = first ? j.src_stride : (j.rows ? n : j.dst_stride);
         a.tab = j.tab;
         a.n_src = j.n_src;
@@ -170,6 +175,7 @@ static void run_dif(DeviceCtx &c, const DifJob &j)
         if (store_rows) {
             a.dst = j.dst;
             a.dst_stride = 0;
+            a.dst_len = j.dst_len;
             if (j.scatter) {
                 a.dst_tab = j.scatter->dst_tab;
                 a.log_rows_per_dst = j.scatter->log_rows_per_dst;
@@ -178,6 +184,7 @@ static void run_dif(DeviceCtx &c, const DifJob &j)
         } else {
             a.dst = j.rows ? j.scratch : j.dst;
             a.dst_stride = j.rows ? n : j.dst_stride;
+            a.dst_len = j.rows ? j.scratch_len : j.dst_len;
         }
         const int load = first ? j.load : LOAD_PLAIN;
         if (store_rows && ps.logr > MAX_ROWS_LOGR) throw arg_failure("row-output pass radix above the tile");
@@ -215,13 +222,14 @@ static void run_dif(DeviceCtx &c, const DifJob &j)
 
 // bit-reversed (per virtual column) -> natural, with factor mul and optional table
 static void reorder(DeviceCtx &c, const uint64_t *src, uint64_t src_stride, uint64_t *dst, uint64_t dst_stride,
-                    uint32_t lg_t, uint32_t rate, uint64_t cols, uint64_t mul, const uint64_t *tab)
+                    uint32_t lg_t, uint32_t rate, uint64_t cols, uint64_t mul, const uint64_t *tab, uint64_t src_len,
+                    uint64_t dst_len)
 {
     const uint32_t a = lg_t >= 10 ? 5 : lg_t / 2;
     const uint64_t blocks = cols * (1ULL << (lg_t - 2 * a)) * (1ULL << rate);
     if (blocks > 0x7FFFFFFFULL) throw arg_failure("reorder too large for one launch");
     bitrev_reorder_kernel<<<(unsigned)blocks, 256, 0, c.stream>>>(src, dst, src_stride, dst_stride, lg_t, rate, cols, mul,
-                                                                  tab);
+                                                                  tab, src_len, dst_len);
     note_launch();
     ZK_CUDA(cudaGetLastError());
 }
@@ -252,8 +260,10 @@ void ntt_batch_device(DeviceCtx &c, uint64_t *inout, uint32_t lg, uint64_t batch
         j.dst_stride = n;
         j.vcols = batches;
         j.L = lg;
+        j.src_len = j.dst_len = n * batches;
+        j.tab_len = n;
         run_dif(c, j);
-        reorder(c, tp, n, inout, n, lg, 0, batches, 1, nullptr);
+        reorder(c, tp, n, inout, n, lg, 0, batches, 1, nullptr, n * batches, n * batches);
     } else {
         DifJob j{};
         j.src = inout;
@@ -264,9 +274,11 @@ void ntt_batch_device(DeviceCtx &c, uint64_t *inout, uint32_t lg, uint64_t batch
         j.vcols = batches;
         j.L = lg;
         j.inverse = true;
+        j.src_len = j.dst_len = n * batches;
         run_dif(c, j);
         // reference order: coset multiply (forward powers) then n^-1 (ntt.cu:137-143)
-        reorder(c, tp, n, inout, n, lg, 0, batches, H_SIZE_INV[lg], with_coset ? c.coset_powers(lg) : nullptr);
+        reorder(c, tp, n, inout, n, lg, 0, batches, H_SIZE_INV[lg], with_coset ? c.coset_powers(lg) : nullptr,
+                n * batches, n * batches);
     }
 }
 
@@ -292,8 +304,11 @@ void lde_batch_device(DeviceCtx &c, uint64_t *out, const uint64_t *in, uint32_t 
         j.vcols = batches << rate;
         j.L = lg_n;
         j.rate = rate;
+        j.src_len = n * batches;
+        j.tab_len = N;
+        j.dst_len = N * batches;
         run_dif(c, j);
-        reorder(c, tmp.p, n, out, N, lg_n, rate, batches, 1, nullptr);
+        reorder(c, tmp.p, n, out, N, lg_n, rate, batches, 1, nullptr, N * batches, N * batches);
     } else {
         // zero-extended inverse transform of size N (ntt.cu:529-535)
         DifJob j{};
@@ -306,8 +321,11 @@ void lde_batch_device(DeviceCtx &c, uint64_t *out, const uint64_t *in, uint32_t 
         j.vcols = batches;
         j.L = lgN;
         j.inverse = true;
+        j.src_len = n * batches;
+        j.dst_len = N * batches;
         run_dif(c, j);
-        reorder(c, tmp.p, N, out, N, lgN, 0, batches, H_SIZE_INV[lgN], with_coset ? c.coset_powers(lgN) : nullptr);
+        reorder(c, tmp.p, N, out, N, lgN, 0, batches, H_SIZE_INV[lgN], with_coset ? c.coset_powers(lgN) : nullptr,
+                N * batches, N * batches);
     }
 }
 
@@ -367,6 +385,9 @@ void lde_rows_explicit(cudaStream_t stream, uint64_t *rows, const uint64_t *coef
             a.row_stride = cols;
             a.dst = last ? rows + c0 : scratch;
             a.dst_stride = n;
+            a.src_len = first ? (cols - c0) * n : (n << rate) * chunk_cols;
+            a.dst_len = last ? (n << rate) * cols - c0 : (n << rate) * chunk_cols;
+            a.tab_len = n << rate;
             uint64_t grid;
             uint32_t tile;
             if (last) {
@@ -454,6 +475,10 @@ void lde_rows_device(DeviceCtx &c, uint64_t *rows, const uint64_t *coeffs, uint3
         j.cols = (uint32_t)cc;
         j.rows = true;
         j.scratch = scratch;
+        j.src_len = (cols - c0) * n;
+        j.tab_len = n << rate;
+        j.dst_len = scatter ? (1ULL << scatter->log_rows_per_dst) * scatter->row_stride : (n << rate) * cols - c0;
+        j.scratch_len = multi ? (n << rate) * chunk : 0;
         run_dif(c, j);
     }
 }
@@ -512,5 +537,7 @@ void salt_device(DeviceCtx &c, uint64_t *out, uint64_t count)
     note_launch();
     ZK_CUDA(cudaGetLastError());
 }
+
+cudaError_t oob_take_ntt(uint64_t r[4]) { return oob_take_local(r); }
 
 }  // namespace zk

@@ -24,6 +24,7 @@
 #pragma once
 #include <stdint.h>
 
+#include "bounds.cuh"
 #include "gl64.cuh"
 
 namespace zk {
@@ -266,6 +267,9 @@ struct NttPassArgs {
     uint64_t *const *dst_tab;
     uint32_t log_rows_per_dst;
     uint64_t col_offset;
+    // extents in words of src, dst (each destination buffer for dst_tab) and
+    // tab from the pass's first element on: read only by the checked build
+    uint64_t src_len, dst_len, tab_len;
 };
 
 // Sub-step of the in-CTA R-point DIF: every task owns E elements spaced Q apart
@@ -435,18 +439,30 @@ __global__ void __launch_bounds__(NT, pass_threads_per_sm<LOGR, LOADM, STOREM>()
     // the load-mode transform of the element at (vcol, pos); elements of one
     // group member run m -> m + q are `step` positions apart
     auto load_elem = [&](uint64_t vcol, uint64_t pos) -> uint64_t {
-        if (LOADM == LOAD_PLAIN) return a.src[vcol * a.src_stride + pos];
-        if (LOADM == LOAD_SCALE) return gl_mul_nc(a.src[vcol * a.src_stride + pos], __ldg(a.tab + pos));
-        if (LOADM == LOAD_COSETS)
-            return gl_mul_nc(a.src[(vcol >> a.rate) * a.src_stride + pos], __ldg(a.tab + ((vcol & rmask) << a.L) + pos));
-        return pos < a.n_src ? a.src[vcol * a.src_stride + pos] : 0;  // LOAD_EXTEND
+        if (LOADM == LOAD_PLAIN) {
+            const uint64_t si = vcol * a.src_stride + pos;
+            return ZK_IN_BOUNDS(si, a.src_len, OOB_NTT_SRC) ? a.src[si] : 0;
+        }
+        if (LOADM == LOAD_SCALE) {
+            const uint64_t si = vcol * a.src_stride + pos;
+            return gl_mul_nc(ZK_IN_BOUNDS(si, a.src_len, OOB_NTT_SRC) ? a.src[si] : 0,
+                             ZK_IN_BOUNDS(pos, a.tab_len, OOB_NTT_TAB) ? __ldg(a.tab + pos) : 0);
+        }
+        if (LOADM == LOAD_COSETS) {
+            const uint64_t si = (vcol >> a.rate) * a.src_stride + pos, ti = ((vcol & rmask) << a.L) + pos;
+            return gl_mul_nc(ZK_IN_BOUNDS(si, a.src_len, OOB_NTT_SRC) ? a.src[si] : 0,
+                             ZK_IN_BOUNDS(ti, a.tab_len, OOB_NTT_TAB) ? __ldg(a.tab + ti) : 0);
+        }
+        if (pos >= a.n_src) return 0;  // LOAD_EXTEND
+        const uint64_t si = vcol * a.src_stride + pos;
+        return ZK_IN_BOUNDS(si, a.src_len, OOB_NTT_SRC) ? a.src[si] : 0;
     };
     // pass twiddle (S > 1) and the store of one element
     auto store_elem = [&](uint64_t vcol, uint64_t pos, uint32_t m, uint64_t val) {
         if (S > 1) {
             const uint64_t o = pos & (S - 1);
             const uint64_t f = bitrev32(m, LOGR);
-            val = gl_mul_nc(val, __ldg(a.tw_pass + o * f));
+            val = gl_mul_nc(val, ZK_IN_BOUNDS(o * f, 1ULL << log_m, OOB_NTT_TWIDDLE) ? __ldg(a.tw_pass + o * f) : 0);
         }
         val = gl_canon(val);  // global memory holds canonical values
         if (STOREM == STORE_ROWS) {
@@ -455,13 +471,14 @@ __global__ void __launch_bounds__(NT, pass_threads_per_sm<LOGR, LOADM, STOREM>()
                 const uint64_t row = ((uint64_t)bitrev32((uint32_t)(vcol & rmask), a.rate) << a.L) + pos;
                 if (a.dst_tab) {
                     uint64_t *d = a.dst_tab[row >> a.log_rows_per_dst];
-                    d[(row & ((1ULL << a.log_rows_per_dst) - 1)) * a.row_stride + a.col_offset + b] = val;
+                    const uint64_t di = (row & ((1ULL << a.log_rows_per_dst) - 1)) * a.row_stride + a.col_offset + b;
+                    if (ZK_IN_BOUNDS(di, a.dst_len, OOB_NTT_SCATTER)) d[di] = val;
                 } else {
-                    a.dst[row * a.row_stride + b] = val;
+                    if (ZK_IN_BOUNDS(row * a.row_stride + b, a.dst_len, OOB_NTT_ROWS)) a.dst[row * a.row_stride + b] = val;
                 }
             }
         } else if (vcol < a.vcols) {
-            a.dst[vcol * a.dst_stride + pos] = val;
+            if (ZK_IN_BOUNDS(vcol * a.dst_stride + pos, a.dst_len, OOB_NTT_DST)) a.dst[vcol * a.dst_stride + pos] = val;
         }
     };
     // linear index e -> (g, m) so that consecutive e are consecutive addresses
@@ -572,7 +589,8 @@ __global__ void __launch_bounds__(NT, pass_threads_per_sm<LOGR, LOADM, STOREM>()
                 const uint32_t sb = swz((c << LOGR) + w0);
 #pragma unroll
                 for (uint32_t k = 0; k < R / 16; k++) {
-                    *d = gl_canon(sm[sb ^ swz_c(16 * k)]);
+                    if (ZK_IN_BOUNDS((row0 + 16 * k) * a.row_stride + b, a.dst_len, OOB_NTT_ROWS))
+                        *d = gl_canon(sm[sb ^ swz_c(16 * k)]);
                     d += dstep;
                 }
             }
@@ -606,7 +624,8 @@ __global__ void __launch_bounds__(NT, pass_threads_per_sm<LOGR, LOADM, STOREM>()
 static __global__ void __launch_bounds__(256) bitrev_reorder_kernel(const uint64_t *__restrict__ src, uint64_t *__restrict__ dst,
                                                              uint64_t src_stride, uint64_t dst_stride, uint32_t lg_t,
                                                              uint32_t rate, uint64_t cols, uint64_t mul,
-                                                             const uint64_t *__restrict__ tab)
+                                                             const uint64_t *__restrict__ tab, uint64_t src_len,
+                                                             uint64_t dst_len)
 {
     // Natural output index i = c + 2^rate * t, t < 2^lg_t, c < 2^rate.
     // Source: virtual column (v << rate) + c, position rev(t).
@@ -632,7 +651,8 @@ static __global__ void __launch_bounds__(256) bitrev_reorder_kernel(const uint64
         if (tx < A) {
             uint64_t q = ((uint64_t)bitrev32(ry, a) << (lg_t - a)) + (rmid << a) + tx;
             // tx = rev(hi) -> hi = rev(tx)
-            tile[ry][bitrev32(tx, a)] = s[q];
+            const uint64_t si = ((v << rate) + c) * src_stride + q;
+            tile[ry][bitrev32(tx, a)] = ZK_IN_BOUNDS(si, src_len, OOB_REORDER_SRC) ? src[si] : 0;
         }
     }
     __syncthreads();
@@ -645,7 +665,7 @@ static __global__ void __launch_bounds__(256) bitrev_reorder_kernel(const uint64
             uint64_t val = tile[tx][hy];
             if (mul != 1) val = gl_mul(val, mul);
             if (tab) val = gl_mul(val, __ldg(tab + i));
-            d[i] = val;
+            if (ZK_IN_BOUNDS(v * dst_stride + i, dst_len, OOB_REORDER_DST)) d[i] = val;
         }
     }
 }
@@ -665,13 +685,14 @@ static __global__ void __launch_bounds__(256) transpose_rev_kernel(const uint64_
     for (uint32_t e = threadIdx.x; e < TI * TB; e += 256) {
         const uint32_t r = e / TI, c = e % TI;
         const uint64_t b = b0 + r, i = i0 + c;
-        if (b < cols && i < n) tile[r][c] = in[b * n + i];
+        if (b < cols && i < n && ZK_IN_BOUNDS(b * n + i, n * cols, OOB_TRANSPOSE_IN)) tile[r][c] = in[b * n + i];
     }
     __syncthreads();
     for (uint32_t e = threadIdx.x; e < TI * TB; e += 256) {
         const uint32_t r = e / TB, c = e % TB;
         const uint64_t i = i0 + r, b = b0 + c;
-        if (b < cols && i < n) out[bitrev64(i, lg) * cols + b] = tile[c][r];
+        const uint64_t oi = bitrev64(i, lg) * cols + b;
+        if (b < cols && i < n && ZK_IN_BOUNDS(oi, n * cols, OOB_TRANSPOSE_OUT)) out[oi] = tile[c][r];
     }
 }
 
@@ -693,7 +714,8 @@ static __global__ void __launch_bounds__(256) transpose_rev_v2_kernel(const uint
     for (uint32_t e = threadIdx.x; e < TI * TB / 2; e += 256) {
         const uint32_t r = e / (TI / 2), c = 2 * (e % (TI / 2));
         const uint64_t b = b0 + r, i = i0 + c;
-        if (b < cols && i < n) {  // i even and n even: i + 1 < n too
+        if (b < cols && i < n && ZK_IN_BOUNDS(b * n + i + 1, n * cols, OOB_TRANSPOSE_IN)) {
+            // i even and n even: i + 1 < n too
             const ulonglong2 v = *(const ulonglong2 *)(in + b * n + i);
             tile[r][c] = v.x;
             tile[r][c + 1] = v.y;
@@ -703,11 +725,13 @@ static __global__ void __launch_bounds__(256) transpose_rev_v2_kernel(const uint
     for (uint32_t e = threadIdx.x; e < TI * TB / 2; e += 256) {
         const uint32_t r = e / (TB / 2), c = 2 * (e % (TB / 2));
         const uint64_t i = i0 + r, b = b0 + c;
-        if (b < cols && i < n) {  // b even and cols even: b + 1 < cols too
+        const uint64_t oi = bitrev64(i, lg) * cols + b;
+        if (b < cols && i < n && ZK_IN_BOUNDS(oi + 1, n * cols, OOB_TRANSPOSE_OUT)) {
+            // b even and cols even: b + 1 < cols too
             ulonglong2 v;
             v.x = tile[c][r];
             v.y = tile[c + 1][r];
-            *(ulonglong2 *)(out + bitrev64(i, lg) * cols + b) = v;
+            *(ulonglong2 *)(out + oi) = v;
         }
     }
 }
