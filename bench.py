@@ -15,9 +15,10 @@ no data-path collective).  Rank 0 prints one JSON line.
 At N = 1 the same line also carries the uneven batch (64 jobs, one CUDA graph
 per memory wave vs one plain C-ABI call per stage per job: batched_over_plain,
 batched_elems_per_s, plain_elems_per_s, and the batch's Poseidon permutation
-floor) and the serving stream (Poisson requests at 0.7 of the serial capacity:
-serve_p50_ms, serve_p99_ms, delivered and offered elements/s); --no-extras
-skips them.
+floor), the alternative-hash forests (Poseidon2, Monolith and Keccak over 2^20
+leaves x 135, in one batch and alone: alt_hash_forests) and the serving stream
+(Poisson requests at 0.7 of the serial capacity: serve_p50_ms, serve_p99_ms,
+delivered and offered elements/s); --no-extras skips them.
 """
 import argparse
 import json
@@ -352,6 +353,7 @@ def run_ours(args, rank, world):
         del ev_cols
         torch.cuda.empty_cache()
         batch = measure_batch(args.batch_steps, args.budget_gb)
+        forests = measure_hashes(3)
         serve = measure_serve(args.requests)
         extras = {"batched_over_plain": batch["batched_over_plain"],
                   "batched_elems_per_s": batch["batched_elems_per_s"],
@@ -359,7 +361,8 @@ def run_ours(args, rank, world):
                   "serve_p50_ms": serve["p50_ms"], "serve_p99_ms": serve["p99_ms"],
                   "serve_delivered_elems_per_s": serve["delivered_elems_per_s"],
                   "serve_offered_elems_per_s": serve["offered_elems_per_s"],
-                  "uneven_batch": batch, "serving": serve}
+                  "forests_batched_leaves_per_s": forests["batched_leaves_per_s"],
+                  "uneven_batch": batch, "alt_hash_forests": forests, "serving": serve}
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": "elems/s", "n_gpus": world, "steps": args.steps,
@@ -396,7 +399,7 @@ def run_stage(args):
         elif args.only == "transpose":
             zk.transpose_rev(0, leaves, ev_cols, lg + RATE, COLS)
         else:
-            zk.fill_digests_buf_linear_gpu(dig, caps, leaves, N, COLS, CAP, HASH)
+            zk.fill_digests_buf_linear_gpu(dig, caps, leaves, N, COLS, CAP, args.hash)
     torch.cuda.synchronize()
     print("stage %s lg_n %d done, %d launches" % (args.only, lg, zk.launch_count()))
 
@@ -548,12 +551,13 @@ def run_batch(args):
     print(json.dumps(line), flush=True)
 
 
-def run_hashes(args):
+def measure_hashes(steps):
     """Alternative hashes at scale: 2^20 leaves x 135 elements, cap_height 4,
-    Poseidon2 + Monolith + Keccak forests built as one batch (one graph)."""
+    Poseidon2 + Monolith + Keccak forests built as one batch (one graph), and
+    each forest alone through fill_digests_buf_linear_gpu_with_gpu_ptr (CUDA
+    events on the legacy stream the Merkle call queues on)."""
     import torch
     import zeknox_b200 as zk
-    torch.cuda.set_device(0)
     nl, ls, ch = 1 << 20, 135, 4
     trees = []
     for k, h in enumerate((3, 4, 1)):
@@ -565,27 +569,38 @@ def run_hashes(args):
     jobs = [zk.merkle_job(l, d, c, nl, ls, ch, h) for h, l, d, c in trees]
     zk.merkle_batch(0, jobs)
     torch.cuda.synchronize()
+    legacy = torch.cuda.default_stream()
     a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    a.record()
-    for _ in range(args.steps):
+    a.record(legacy)
+    for _ in range(steps):
         zk.merkle_batch(0, jobs)
-    b.record()
+    b.record(legacy)
     torch.cuda.synchronize()
-    batch_ms = a.elapsed_time(b) / args.steps
+    batch_ms = a.elapsed_time(b) / steps
     per = {}
     for h, l, d, c in trees:
-        a.record()
-        for _ in range(args.steps):
-            zk.fill_digests_buf_linear_gpu(d, c, l, nl, ls, ch, h)
-        b.record()
+        zk.fill_digests_buf_linear_gpu(d, c, l, nl, ls, ch, h)
         torch.cuda.synchronize()
-        ms = a.elapsed_time(b) / args.steps
+        a.record(legacy)
+        for _ in range(steps):
+            zk.fill_digests_buf_linear_gpu(d, c, l, nl, ls, ch, h)
+        b.record(legacy)
+        torch.cuda.synchronize()
+        ms = a.elapsed_time(b) / steps
         name = {3: "poseidon2", 4: "monolith", 1: "keccak"}[h]
-        perms = nl * ((ls + 7) // 8) + (nl - (1 << ch)) if h != 1 else nl * ((ls * 8) // 136 + 1) + (nl - (1 << ch))
+        perms = perms_of(nl, ls, ch) if h != 1 else nl * ((ls * 8) // 136 + 1) + (nl - (1 << ch))
         per[name] = {"ms": ms, "leaves_per_s": nl / (ms * 1e-3), "perms_per_s": perms / (ms * 1e-3)}
-    line = {"metric": "Merkle forests (2^20 leaves x 135, cap 4) leaves/s", "unit": "leaves/s",
-            "batched_value": 3 * nl / (batch_ms * 1e-3), "batched_ms": batch_ms, "per_hash": per, "steps": args.steps,
-            "dtype": "u64", "config": {"workload": "Poseidon2 + Monolith + Keccak forests, 2^20 leaves x 135, cap 4"}}
+    del trees, jobs
+    torch.cuda.empty_cache()
+    return {"batched_leaves_per_s": 3 * nl / (batch_ms * 1e-3), "batched_ms": batch_ms, "per_hash": per,
+            "steps": steps, "workload": "Poseidon2 + Monolith + Keccak forests, 2^20 leaves x 135, cap 4, one batch"}
+
+
+def run_hashes(args):
+    import torch
+    torch.cuda.set_device(0)
+    d = measure_hashes(args.steps)
+    line = {"metric": "Merkle forests (2^20 leaves x 135, cap 4) leaves/s", "unit": "leaves/s", "dtype": "u64", **d}
     print(json.dumps(line), flush=True)
 
 
@@ -719,6 +734,8 @@ def main():
     ap.add_argument("--lg-n", type=int, default=LG_N, help="log2 coefficients per column (profiling cases)")
     ap.add_argument("--only", default=None, choices=["lde", "merkle", "transpose"],
                     help="profiling: run only this stage for warmup+steps iterations and exit")
+    ap.add_argument("--hash", type=int, default=HASH, help="--only merkle: hash type (0 Poseidon, 1 Keccak, "
+                    "2 Poseidon-BN128, 3 Poseidon2, 4 Monolith)")
     ap.add_argument("--requests", type=int, default=96, help="serve workload: number of requests")
     ap.add_argument("--batch-steps", type=int, default=1, help="uneven batch: timed passes per wave")
     ap.add_argument("--no-extras", action="store_true",
