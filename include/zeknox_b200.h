@@ -248,6 +248,16 @@ RustError zeknox_permute(size_t device_id, uint64_t *states, uint64_t n, uint32_
  * counterpart (a sanitizer stand-in). */
 RustError zeknox_bounds_report(size_t device_id, uint64_t *record);
 
+/* Bounded device waits.  Kernels that wait on bulk-async copies (the
+ * transpose's shared-memory stages) give each wait a limit of 1 s; a CTA whose
+ * stage has not completed by then stops and raises a status word, and the
+ * call returns -cudaErrorLaunchTimeout (calls queued on a caller's stream:
+ * the device's next synchronous call).  This test hook makes the next `count`
+ * such transposes on the device declare 16 bytes more than they copy, so one
+ * wait runs out (after 20 ms) without any fault; the context stays usable.
+ * No reference counterpart. */
+RustError zeknox_inject_wait_timeout(size_t device_id, uint32_t count);
+
 /* Number of kernels this library has launched so far in the process. */
 uint64_t zeknox_launch_count(void);
 

@@ -114,6 +114,49 @@ def test_transpose_rev_unaligned_buffers(lg, b):
     assert torch.equal(aligned, out[1:])
 
 
+@pytest.mark.parametrize("lg,b", [(6, 2), (6, 64), (7, 34), (11, 96), (13, 258), (16, 40), (18, 64)])
+def test_transpose_rev_bulk_and_plain_forms(lg, b):
+    """Every tile shape of the bulk-copy staged transpose (knob
+    transpose_bulk 1..8: persistent CTAs, 2-8 stages; ragged last column tile,
+    fewer tiles than CTAs, many tiles per CTA) and the 16-byte form (0) give
+    the oracle's matrix."""
+    x = O.field_data(5 * lg + b, b << lg)
+    src = to_dev(x)
+    exp = O.transpose_rev(x, lg, b)
+    outs = []
+    try:
+        for form in (1, 2, 3, 4, 5, 6, 7, 8, 0):
+            zk.tune_set("transpose_bulk", form)
+            out = torch.zeros(b << lg, dtype=torch.int64, device="cuda")
+            zk.transpose_rev_batch(0, out, src, lg, b)
+            outs.append(out)
+    finally:
+        zk.tune_set("transpose_bulk", zk.TRANSPOSE_AUTO)
+    assert np.array_equal(to_np(outs[0]), exp)
+    for o in outs[1:]:
+        assert torch.equal(outs[0], o)
+
+
+def test_transpose_rev_bounded_wait_times_out():
+    """A stage whose byte count never completes (injected: 16 bytes declared
+    and not copied) ends its CTA's wait after the limit; the call returns
+    -cudaErrorLaunchTimeout, and the next transposes on the same context are
+    bit-exact.  Nothing faults or hangs: the copies all complete, only the
+    barrier's expected count is never reached."""
+    lg, b = 12, 64
+    x = O.field_data(4242, b << lg)
+    src = to_dev(x)
+    out = torch.zeros(b << lg, dtype=torch.int64, device="cuda")
+    zk.inject_wait_timeout(0, 1)
+    with pytest.raises(zk.ZeknoxError) as e:
+        zk.transpose_rev_batch(0, out, src, lg, b)
+    assert e.value.code == -702  # cudaErrorLaunchTimeout
+    for _ in range(2):
+        out = torch.zeros(b << lg, dtype=torch.int64, device="cuda")
+        zk.transpose_rev_batch(0, out, src, lg, b)
+        assert np.array_equal(to_np(out), O.transpose_rev(x, lg, b))
+
+
 def test_argument_errors():
     t = torch.zeros(16, dtype=torch.int64, device="cuda")
     with pytest.raises(zk.ZeknoxError) as e:

@@ -43,7 +43,8 @@ EXT_SYMBOLS = ["zeknox_last_error", "zeknox_commit", "zeknox_commit_batch", "zek
                "zeknox_server_release", "zeknox_server_stats", "zeknox_server_destroy", "zeknox_server_prepare",
                "zeknox_server_cancel", "zeknox_server_inject_failure", "zeknox_tune_set",
                "zeknox_tune_get", "zeknox_tune_clear", "zeknox_tune_load", "zeknox_transpose_rev",
-               "zeknox_lde_rows_scatter", "zeknox_field_selftest", "zeknox_permute", "zeknox_bounds_report"]
+               "zeknox_lde_rows_scatter", "zeknox_field_selftest", "zeknox_permute", "zeknox_bounds_report",
+               "zeknox_inject_wait_timeout"]
 
 # Tuning table measured on B200 by ``python -m zeknox_b200.autotune``; loaded
 # by load() unless ZEKNOX_TUNE_FILE names another table ("" or "none": no table).
@@ -210,6 +211,8 @@ def load():
     L.zeknox_field_selftest.argtypes = [sz, vp, vp, vp, u64, vp, vp]
     L.zeknox_bounds_report.restype = RustError
     L.zeknox_bounds_report.argtypes = [sz, ctypes.POINTER(ctypes.c_uint64)]
+    L.zeknox_inject_wait_timeout.restype = RustError
+    L.zeknox_inject_wait_timeout.argtypes = [sz, u32]
     L.zeknox_permute.restype = RustError
     L.zeknox_permute.argtypes = [sz, vp, u64, u32, u32, vp]
     L.zeknox_lde_rows_scatter.argtypes = [sz, ctypes.POINTER(ctypes.c_void_p), u32, vp, u32, u32, u32, u32, u32, u64, vp]
@@ -457,6 +460,17 @@ def bounds_report(device_id=0):
     if err.code not in (0, 801):  # 801: cudaErrorNotSupported, the normal build
         raise ZeknoxError(err.code, "zeknox_bounds_report")
     return err.code == 0, [int(v) for v in rec]
+
+
+# Values of the "transpose_bulk" knob: 0 the 16-byte transpose, 1..8 a tile
+# shape of the bulk-copy transpose, TRANSPOSE_AUTO (the default) by column count.
+TRANSPOSE_AUTO = 9
+
+
+def inject_wait_timeout(device_id=0, count=1):
+    """zeknox_inject_wait_timeout: the next `count` bulk-copy transposes on the
+    device declare more bytes than they copy, so a bounded wait runs out."""
+    _check(load().zeknox_inject_wait_timeout(device_id, count))
 
 
 def permute(device_id, states, hash_type, cooperative=False, stream=None):

@@ -678,6 +678,18 @@ extern "C" RustError zeknox_bounds_report(size_t device_id, uint64_t *record)
     });
 }
 
+// Test hook for the bounded waits: the next `count` bulk-copy transposes on
+// this device declare 16 bytes more than they copy, so one stage's wait runs
+// out; the call that ran it returns -cudaErrorLaunchTimeout.
+extern "C" RustError zeknox_inject_wait_timeout(size_t device_id, uint32_t count)
+{
+    return guarded([&] {
+        zk::DeviceCtx &c = zk::device(device_id);
+        std::lock_guard<std::recursive_mutex> lk(c.mu);
+        c.inject_wait_timeouts = count;
+    });
+}
+
 // Register-resident Goldilocks multiply throughput: every thread runs 8
 // independent chains x <- x * y of `iters` multiplies, with the lazily reduced
 // product the permutations use (any 64-bit representative; IMAD selects the

@@ -498,6 +498,29 @@ void prepare_tables(DeviceCtx &c, uint32_t lg_n, uint32_t rate, uint64_t coset_g
     }
 }
 
+// The bulk-copy transpose: persistent CTAs, as many as fit on the SMs with
+// their stage buffers.
+template <uint32_t TI, uint32_t TB, uint32_t ST>
+static void launch_transpose_bulk(DeviceCtx &c, uint64_t *out, const uint64_t *in, uint32_t lg, uint64_t cols,
+                                  uint32_t extra, uint64_t wait_ns)
+{
+    using G = TrBulk<TI, TB, ST>;
+    static int per_sm_of[64] = {};  // per device, set once under its lock
+    int &per_sm = per_sm_of[c.id & 63];
+    if (!per_sm) {
+        ZK_CUDA(cudaFuncSetAttribute(transpose_rev_bulk_kernel<TI, TB, ST>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)G::SMEM_BYTES));
+        ZK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, transpose_rev_bulk_kernel<TI, TB, ST>, G::THREADS,
+                                                              G::SMEM_BYTES));
+        if (per_sm < 1) per_sm = 1;
+    }
+    const uint64_t n = 1ULL << lg;
+    const uint64_t tiles_i = n / TI, n_tiles = tiles_i * ((cols + TB - 1) / TB);
+    const uint64_t ctas = std::min<uint64_t>(n_tiles, (uint64_t)c.sm_count * per_sm);
+    transpose_rev_bulk_kernel<TI, TB, ST><<<(unsigned)ctas, G::THREADS, G::SMEM_BYTES, c.stream>>>(
+        in, out, lg, cols, tiles_i, n_tiles, c.wait_status(), extra, wait_ns);
+}
+
 void transpose_rev_device(DeviceCtx &c, uint64_t *out, const uint64_t *in, uint32_t lg, uint64_t cols)
 {
     NvtxRange range("zeknox transpose_rev");
@@ -506,8 +529,35 @@ void transpose_rev_device(DeviceCtx &c, uint64_t *out, const uint64_t *in, uint3
     dim3 grid((unsigned)((n + 63) / 64), (unsigned)((cols + 31) / 32));
     if (grid.y > 65535) throw arg_failure("too many columns for transpose");
     const bool vec16 = lg >= 1 && cols % 2 == 0 && ((uintptr_t)in % 16) == 0 && ((uintptr_t)out % 16) == 0;
-    if (vec16) transpose_rev_v2_kernel<<<grid, 256, 0, c.stream>>>(in, out, lg, cols);
-    else transpose_rev_kernel<<<grid, 256, 0, c.stream>>>(in, out, lg, cols);
+    // knob transpose_bulk: 0 the 16-byte form, 1..8 a bulk-copy tile shape,
+    // 9 (default) by column count: 64 x 64 tiles with 3 stages from 48
+    // columns, else 64 x 32 with 4 (measured on B200: 0.198 against 0.213 ms
+    // for the 16-byte form at 256 x 2^18, 0.223 against 0.240 ms at 16 x 2^22)
+    uint64_t form = vec16 ? tune_get("transpose_bulk", lg, 9) : 0;
+    if (form == 9) form = cols >= 48 ? 3 : 1;
+    if (form >= 1 && form <= 8 && lg >= (form == 4 || form == 5 ? 7u : 6u)) {
+        uint32_t extra = 0;
+        uint64_t wait_ns = 1000000000ULL;  // 1 s: a stage of tens of KiB lands in microseconds
+        if (c.inject_wait_timeouts) {
+            c.inject_wait_timeouts--;
+            extra = 16;
+            wait_ns = 20000000ULL;
+        }
+        switch (form) {
+        case 1: launch_transpose_bulk<64, 32, 4>(c, out, in, lg, cols, extra, wait_ns); break;
+        case 2: launch_transpose_bulk<64, 32, 2>(c, out, in, lg, cols, extra, wait_ns); break;
+        case 3: launch_transpose_bulk<64, 64, 3>(c, out, in, lg, cols, extra, wait_ns); break;
+        case 4: launch_transpose_bulk<128, 32, 3>(c, out, in, lg, cols, extra, wait_ns); break;
+        case 5: launch_transpose_bulk<128, 32, 2>(c, out, in, lg, cols, extra, wait_ns); break;
+        case 6: launch_transpose_bulk<64, 32, 8>(c, out, in, lg, cols, extra, wait_ns); break;
+        case 7: launch_transpose_bulk<64, 64, 2>(c, out, in, lg, cols, extra, wait_ns); break;
+        default: launch_transpose_bulk<32, 64, 4>(c, out, in, lg, cols, extra, wait_ns); break;
+        }
+    } else if (vec16) {
+        transpose_rev_v2_kernel<<<grid, 256, 0, c.stream>>>(in, out, lg, cols);
+    } else {
+        transpose_rev_kernel<<<grid, 256, 0, c.stream>>>(in, out, lg, cols);
+    }
     note_launch();
     ZK_CUDA(cudaGetLastError());
 }

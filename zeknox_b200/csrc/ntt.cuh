@@ -25,6 +25,7 @@
 #include <stdint.h>
 
 #include "bounds.cuh"
+#include "bulk.cuh"
 #include "gl64.cuh"
 
 namespace zk {
@@ -732,6 +733,107 @@ static __global__ void __launch_bounds__(256) transpose_rev_v2_kernel(const uint
             v.x = tile[c][r];
             v.y = tile[c + 1][r];
             *(ulonglong2 *)(out + oi) = v;
+        }
+    }
+}
+
+// The same transpose with the column tiles staged by bulk-async copies:
+// persistent CTAs walk the tiles (tile t: positions (t mod tiles_i) * TI,
+// columns (t / tiles_i) * TB); warp 0 keeps STAGES tiles in flight, one
+// TI * 8-byte cp.async.bulk per column of the tile into a padded row of the
+// stage (row pitch TI + 2 words, 16-byte aligned), completed on the stage's
+// mbarrier.  The threads then write the tile as bit-reversed leaf rows: a warp
+// writes 4 rows x 8 column pairs, 128 contiguous bytes per row, and reads the
+// stage without bank conflicts (words 8m + 2r mod 32 over pairs m < 4, rows
+// r < 4).  Needs n >= TI, an even column count and 16-byte aligned buffers.  A
+// stage that is not complete after wait_ns sets *status and the CTA stops
+// (after waiting, bounded again, for the copies it has in flight); extra_tx > 0
+// declares that many bytes more than CTA 0's first tile delivers (a test of
+// that path).
+template <uint32_t TI, uint32_t TB, uint32_t STAGES>
+struct TrBulk {
+    static constexpr uint32_t THREADS = 256, PITCH = TI + 2, STAGE_WORDS = TB * PITCH;
+    static constexpr uint32_t SMEM_BYTES = STAGES * STAGE_WORDS * 8;
+    static_assert((PITCH * 8) % 16 == 0 && (STAGE_WORDS * 8) % 16 == 0, "bulk copy destinations must be 16-byte aligned");
+    static_assert(TB % 16 == 0 && TI % 4 == 0 && (TI * TB / 2) % THREADS == 0, "tile shape");
+};
+
+template <uint32_t TI, uint32_t TB, uint32_t STAGES>
+static __global__ void __launch_bounds__(256)
+    transpose_rev_bulk_kernel(const uint64_t *__restrict__ in, uint64_t *__restrict__ out, uint32_t lg, uint64_t cols,
+                              uint64_t tiles_i, uint64_t n_tiles, unsigned *status, uint32_t extra_tx, uint64_t wait_ns)
+{
+    using G = TrBulk<TI, TB, STAGES>;
+    constexpr uint32_t THREADS = G::THREADS, PITCH = G::PITCH, STAGE_WORDS = G::STAGE_WORDS;
+    extern __shared__ __align__(128) uint64_t stage_buf[];
+    __shared__ __align__(8) uint64_t full[STAGES];
+    const uint64_t n = 1ULL << lg;
+    const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    if (tid == 0) {
+#pragma unroll
+        for (uint32_t s = 0; s < STAGES; s++) mbar_init(smem_u32(&full[s]), 1);
+        mbar_init_fence();
+    }
+    __syncthreads();
+    // warp 0: local tile k into stage k % STAGES
+    auto issue = [&](uint64_t k) {
+        const uint64_t t = blockIdx.x + k * gridDim.x;
+        if (t >= n_tiles) return;
+        const uint32_t s = (uint32_t)(k % STAGES);
+        const uint64_t i0 = (t % tiles_i) * TI, b0 = (t / tiles_i) * TB;
+        const uint32_t nb = (uint32_t)(cols - b0 < TB ? cols - b0 : TB);
+        const uint32_t bar = smem_u32(&full[s]);
+        if (lane == 0) mbar_arrive_expect_tx(bar, nb * TI * 8 + (k == 0 && blockIdx.x == 0 ? extra_tx : 0));
+        __syncwarp();
+        for (uint32_t j = lane; j < nb; j += 32)
+            if (ZK_IN_BOUNDS((b0 + j) * n + i0 + TI - 1, n * cols, OOB_TRANSPOSE_IN))
+                bulk_load(smem_u32(stage_buf + s * STAGE_WORDS + j * PITCH), in + (b0 + j) * n + i0, TI * 8, bar);
+    };
+    if (warp == 0) {
+#pragma unroll 1
+        for (uint32_t k = 0; k < STAGES; k++) issue(k);
+    }
+    uint64_t k = 0;
+    bool failed = false;
+#pragma unroll 1
+    for (;; k++) {
+        const uint64_t t = blockIdx.x + k * gridDim.x;
+        if (t >= n_tiles) break;
+        const uint32_t s = (uint32_t)(k % STAGES);
+        const bool ok = mbar_wait_bounded(smem_u32(&full[s]), (uint32_t)(k / STAGES) & 1, wait_ns);
+        if (__syncthreads_or(!ok)) {
+            failed = true;
+            break;
+        }
+        const uint64_t i0 = (t % tiles_i) * TI, b0 = (t / tiles_i) * TB;
+        const uint64_t *tile = stage_buf + s * STAGE_WORDS;
+#pragma unroll
+        for (uint32_t q = 0; q < TI * TB / 2 / THREADS; q++) {
+            const uint32_t u = tid + q * THREADS, w = u >> 5, l = u & 31;
+            const uint32_t r = 4 * (w / (TB / 16)) + (l >> 3), c = 2 * (8 * (w % (TB / 16)) + (l & 7));
+            const uint64_t b = b0 + c;
+            const uint64_t oi = bitrev64(i0 + r, lg) * cols + b;
+            // b even and cols even: b + 1 < cols too
+            if (b < cols && ZK_IN_BOUNDS(oi + 1, n * cols, OOB_TRANSPOSE_OUT)) {
+                ulonglong2 v;
+                v.x = tile[c * PITCH + r];
+                v.y = tile[(c + 1) * PITCH + r];
+                *(ulonglong2 *)(out + oi) = v;
+            }
+        }
+        __syncthreads();
+        if (warp == 0) {
+            fence_proxy_async_smem();
+            issue(k + STAGES);
+        }
+    }
+    if (failed && tid == 0) {
+        atomicAdd_system(status, 1u);
+        // the copies still in flight target this CTA's shared memory: wait
+        // for them (bounded) before the CTA ends
+        for (uint64_t j = k; j < k + STAGES; j++) {
+            if (blockIdx.x + j * gridDim.x >= n_tiles) break;
+            (void)mbar_wait_bounded(smem_u32(&full[j % STAGES]), (uint32_t)(j / STAGES) & 1, wait_ns / 8);
         }
     }
 }

@@ -182,7 +182,35 @@ void DeviceCtx::free(void *p)
     if (p) (void)cudaFreeAsync(p, stream);
 }
 
-void DeviceCtx::sync() { ZK_CUDA(cudaStreamSynchronize(stream)); }
+void DeviceCtx::sync()
+{
+    ZK_CUDA(cudaStreamSynchronize(stream));
+    check_waits();
+}
+
+unsigned *DeviceCtx::wait_status()
+{
+    if (!wait_status_dev) {
+        void *h = nullptr;
+        ZK_CUDA(cudaHostAlloc(&h, sizeof(unsigned), cudaHostAllocMapped | cudaHostAllocPortable));
+        *(volatile unsigned *)h = 0;
+        void *d = nullptr;
+        ZK_CUDA(cudaHostGetDevicePointer(&d, h, 0));
+        wait_status_host = (unsigned *)h;
+        wait_status_dev = (unsigned *)d;
+    }
+    return wait_status_dev;
+}
+
+void DeviceCtx::check_waits()
+{
+    if (!wait_status_host) return;
+    const unsigned n = *(volatile unsigned *)wait_status_host;
+    if (!n) return;
+    *(volatile unsigned *)wait_status_host = 0;
+    throw cuda_failure(-(int)cudaErrorLaunchTimeout,
+                       std::to_string(n) + " CTA(s) stopped: a bulk-copy stage did not complete within its wait limit");
+}
 
 static uint64_t *build_powers(DeviceCtx &c, uint64_t w, uint64_t count)
 {

@@ -66,7 +66,21 @@ struct DeviceCtx {
 
     uint64_t *alloc(size_t bytes);
     void free(void *p);
+    // Synchronises the stream, then reports a bounded device wait that ran
+    // out since the last check (cuda_failure, -cudaErrorLaunchTimeout).
     void sync();
+
+    // Status word of the bounded device waits (bulk-copy stages): mapped
+    // pinned memory, so kernels raise it with a system-scope atomic and sync()
+    // reads it without a copy.  Calls queued on a caller's stream are reported
+    // by the device's next synchronous call.
+    unsigned *wait_status_host = nullptr;
+    unsigned *wait_status_dev = nullptr;
+    unsigned *wait_status();
+    void check_waits();
+    // Test hook: the next inject_wait_timeouts bulk transposes declare 16
+    // bytes more than they copy, so one stage's wait runs out.
+    uint32_t inject_wait_timeouts = 0;
 };
 
 int device_count();
@@ -92,7 +106,8 @@ uint32_t ilog2_exact(uint64_t x);  // -1u if x is not a power of two
 // (zeknox_tune_set / zeknox_tune_load); tune_get falls back to the size-free
 // entry and then to `dflt`.  Knobs: "leaf_threads.<hash>" (64/128/256),
 // "lde_chunk_mib", "lde_host_chunk_mib", "lde_last_logr" (1..8), "wide_level_nodes.<hash>",
-// "coop_leaves.<hash>".
+// "coop_leaves.<hash>", "transpose_bulk" (0 16-byte form, 1..8 bulk-copy tile
+// shape, 9 by column count).
 uint64_t tune_get(const std::string &name, uint32_t lg, uint64_t dflt);
 void tune_set(const std::string &name, uint32_t lg, uint64_t value);
 void tune_clear();
