@@ -480,7 +480,10 @@ def measure_batch(steps, budget_gb):
     call per stage per job (plain: compute_batched_lde -> compute_transpose_rev ->
     fill_digests_buf_linear_gpu_with_gpu_ptr), same jobs, same buffers, caps
     compared.  Also the batch's Poseidon permutation count at the measured
-    forest rate: no schedule of these jobs on these kernels beats that time."""
+    forest rate: no schedule of these jobs on these kernels beats that time;
+    and the sum of the batch's own stages (each job's fused LDE and forest)
+    run one at a time: the graph's time against it shows how much idle time
+    and overlap the schedule has."""
     import torch
     import zeknox_b200 as zk
     jobs = uneven_jobs()
@@ -498,6 +501,7 @@ def measure_batch(steps, budget_gb):
     total_elems = sum((1 << (j["lg_n"] + j["rate"])) * j["cols"] for j in jobs)
     total_perms = sum(perms_of(1 << (j["lg_n"] + j["rate"]), j["cols"], j["cap"]) for j in jobs)
     t_batch, t_plain = 0.0, 0.0
+    t_stages = {"lde": 0.0, "forest": 0.0}
     for wave in waves:
         bufs, cjobs = [], []
         for jb in wave:
@@ -539,6 +543,20 @@ def measure_batch(steps, budget_gb):
                 t_plain += a.elapsed_time(b) / steps
         for cb, bb in zip(caps_b, bufs):
             assert torch.equal(cb, bb[3]), "batched and plain commitments differ"
+        # the batch's own stages one at a time: each job's fused LDE and its
+        # forest, each call alone and waited for (what the graph would take
+        # if nothing overlapped and nothing were left idle)
+        for jb, (inp, leaves, dig, caps, n_dig, n_cap) in zip(wave, bufs):
+            N = 1 << (jb["lg_n"] + jb["rate"])
+            for stage in ("lde", "forest"):
+                a.record()
+                if stage == "lde":
+                    zk.lde_rows(0, leaves, inp, jb["lg_n"], jb["rate"], jb["cols"])
+                else:
+                    zk.fill_digests_buf_linear_gpu(dig, caps, leaves, N, jb["cols"], jb["cap"], jb["hash"])
+                b.record()
+                torch.cuda.synchronize()
+                t_stages[stage] += a.elapsed_time(b)
         del bufs, cjobs, caps_b, ev_all
         torch.cuda.empty_cache()
     rate = poseidon_perm_rate()
@@ -547,6 +565,8 @@ def measure_batch(steps, budget_gb):
             "batched_over_plain": t_plain / t_batch, "batched_ms": t_batch, "plain_ms": t_plain,
             "poseidon_perms": total_perms, "poseidon_perms_per_s": rate, "perm_floor_ms": floor_ms,
             "batched_frac_of_perm_floor": floor_ms / t_batch, "plain_bound_over_floor": t_plain / floor_ms,
+            "stage_sum_ms": t_stages["lde"] + t_stages["forest"], "stage_lde_ms": t_stages["lde"],
+            "stage_forest_ms": t_stages["forest"], "batched_over_stage_sum": t_batch / (t_stages["lde"] + t_stages["forest"]),
             "jobs": len(jobs), "waves": len(waves), "elements": total_elems, "steps": steps,
             "workload": "64 jobs: lg_n U{10..20}, cols U{8..400}, rate_bits U{1,2,3}, Poseidon, cap_height min(4, lg N), "
                         "seed 3; waves of <= %g GiB" % budget_gb}
