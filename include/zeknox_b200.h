@@ -149,6 +149,23 @@ typedef struct {
 } zk_serve_result;
 
 RustError zeknox_server_create(size_t device_id, uint64_t budget_bytes, uint32_t slots, void **server);
+/* zeknox_server_create with flags.  ZK_SERVE_DEVICE_LOOP: a device-resident
+ * request loop runs the admitted requests.  Admission is the same (arrival
+ * order, the budget, at most min(slots, 16) requests in flight).  The server
+ * thread plans each request's stages, copies the plan to device memory and
+ * posts it to a ring in mapped host memory. One persistent cooperative
+ * kernel then takes the ring's entries and runs every stage itself, one
+ * request at a time across the whole GPU, with grid barriers between the
+ * stages: the fused LDE's passes, then the forest's leaf, level, fold and tail
+ * steps. The kernel marks each entry done in host memory, and exits after
+ * 20 ms without requests (the next post relaunches it).  Every wait of the
+ * kernel is bounded in time.  A request whose wait runs out fails with
+ * -cudaErrorLaunchTimeout.  Requests in this mode: coefficients
+ * (input_is_values 0), Poseidon (0) or Poseidon2 (3), 2^9 <= 2^lg_n <= 2^22.
+ * No reference counterpart. */
+#define ZK_SERVE_DEVICE_LOOP 1u
+RustError zeknox_server_create_ex(size_t device_id, uint64_t budget_bytes, uint32_t slots, uint32_t flags,
+                                  void **server);
 /* Build and keep resident every table a request of lg_n in [lg_n_min,
  * lg_n_max] with this rate and coset generator (0 means 7) reads -- twiddles
  * of every pass, inverse twiddles, the LDE coset tables -- so no request waits
@@ -174,6 +191,10 @@ RustError zeknox_server_cancel(void *server, uint64_t ticket);
 #define ZK_SERVE_FAIL_ALLOC 1
 #define ZK_SERVE_FAIL_SHAPE 2
 #define ZK_SERVE_FAIL_LAUNCH 3
+/* Device-loop servers only: the next request is posted with its start gate
+ * shut, so the loop's bounded wait for it runs out after 20 ms; the request
+ * fails with -cudaErrorLaunchTimeout and the loop goes on with the next. */
+#define ZK_SERVE_FAIL_GATE 4
 RustError zeknox_server_inject_failure(void *server, int stage);
 /* Free the ticket's device results (returns their bytes to the budget). */
 RustError zeknox_server_release(void *server, uint64_t ticket);

@@ -26,7 +26,8 @@ HASH_POSEIDON, HASH_KECCAK, HASH_POSEIDON_BN128, HASH_POSEIDON2, HASH_MONOLITH =
 FORWARD, INVERSE = 0, 1
 SELFTEST_OPS = 34  # ZK_SELFTEST_OPS of include/zeknox_b200.h
 SERVE_CANCELLED = -10000  # ZK_SERVE_CANCELLED
-SERVE_FAIL_ALLOC, SERVE_FAIL_SHAPE, SERVE_FAIL_LAUNCH = 1, 2, 3  # ZK_SERVE_FAIL_*
+SERVE_FAIL_ALLOC, SERVE_FAIL_SHAPE, SERVE_FAIL_LAUNCH, SERVE_FAIL_GATE = 1, 2, 3, 4  # ZK_SERVE_FAIL_*
+SERVE_DEVICE_LOOP = 1  # ZK_SERVE_DEVICE_LOOP
 
 # Exported C symbols (include/lib.h, include/merkle/merkle.h, include/zeknox_b200.h).
 ABI_SYMBOLS = [
@@ -39,7 +40,7 @@ ABI_SYMBOLS = [
 ]
 EXT_SYMBOLS = ["zeknox_last_error", "zeknox_commit", "zeknox_commit_batch", "zeknox_commit_scratch_words",
                "zeknox_lde_rows", "zeknox_launch_count", "zeknox_measure_mul_rate", "zeknox_merkle_batch",
-               "zeknox_lde_rows_noalloc", "zeknox_server_create", "zeknox_server_submit", "zeknox_server_wait",
+               "zeknox_lde_rows_noalloc", "zeknox_server_create", "zeknox_server_create_ex", "zeknox_server_submit", "zeknox_server_wait",
                "zeknox_server_release", "zeknox_server_stats", "zeknox_server_destroy", "zeknox_server_prepare",
                "zeknox_server_cancel", "zeknox_server_inject_failure", "zeknox_tune_set",
                "zeknox_tune_get", "zeknox_tune_clear", "zeknox_tune_load", "zeknox_transpose_rev",
@@ -188,6 +189,8 @@ def load():
     L.zeknox_lde_rows_noalloc.argtypes = [sz, vp, vp, u32, u32, u32, u64, vp]
     L.zeknox_server_create.restype = RustError
     L.zeknox_server_create.argtypes = [sz, u64, u32, ctypes.POINTER(ctypes.c_void_p)]
+    L.zeknox_server_create_ex.restype = RustError
+    L.zeknox_server_create_ex.argtypes = [sz, u64, u32, u32, ctypes.POINTER(ctypes.c_void_p)]
     L.zeknox_server_submit.restype = RustError
     L.zeknox_server_submit.argtypes = [vp, ctypes.POINTER(ServeRequest), ctypes.POINTER(u64)]
     L.zeknox_server_wait.restype = RustError
@@ -543,11 +546,13 @@ def merkle_batch(device_id, jobs):
 class Server:
     """Continuous-batching commit server (zeknox_server_*): requests are admitted
     in arrival order as slots and the device-memory budget allow, and overlap on
-    the GPU."""
+    the GPU.  device_loop=True: a persistent device-resident loop runs the
+    admitted requests (zeknox_server_create_ex with ZK_SERVE_DEVICE_LOOP)."""
 
-    def __init__(self, device_id=0, budget_bytes=120 << 30, slots=8):
+    def __init__(self, device_id=0, budget_bytes=120 << 30, slots=8, device_loop=False):
         h = ctypes.c_void_p()
-        _check(load().zeknox_server_create(device_id, budget_bytes, slots, ctypes.byref(h)))
+        _check(load().zeknox_server_create_ex(device_id, budget_bytes, slots,
+                                              SERVE_DEVICE_LOOP if device_loop else 0, ctypes.byref(h)))
         self._h = h
 
     def submit(self, lg_n, rate_bits, cols, cap_height, hash_type, inp, caps_host=None, input_is_values=False,

@@ -90,11 +90,9 @@ struct Pass {
 // 32-byte sectors); a row-output pass spans at most 2^(LT - 4) positions of 16
 // columns.  Single-pass transforms may use the whole tile.
 
-static std::vector<Pass> plan_passes(uint32_t L, bool rows)
+static std::vector<Pass> plan_passes_last(uint32_t L, bool rows, uint32_t last_rows)
 {
     std::vector<uint32_t> sizes;
-    // last pass of a row-output transform: radix 2^lde_last_logr (tuned)
-    uint32_t last_rows = (uint32_t)tune_get("lde_last_logr", L, MAX_ROWS_LOGR);
     last_rows = last_rows < 1 ? 1 : (last_rows > MAX_ROWS_LOGR ? MAX_ROWS_LOGR : last_rows);
     const uint32_t last_max = rows ? last_rows : LOG_PASS_TILE;
     if (L <= last_max) {
@@ -115,6 +113,12 @@ static std::vector<Pass> plan_passes(uint32_t L, bool rows)
         p.push_back({hi, k});
     }
     return p;
+}
+
+// The last pass of a row-output transform has radix 2^lde_last_logr (tuned).
+static std::vector<Pass> plan_passes(uint32_t L, bool rows)
+{
+    return plan_passes_last(L, rows, (uint32_t)tune_get("lde_last_logr", L, MAX_ROWS_LOGR));
 }
 
 // Batched DIF over `vcols` virtual columns of size 2^L; output in bit-reversed
@@ -405,6 +409,81 @@ void lde_rows_explicit(cudaStream_t stream, uint64_t *rows, const uint64_t *coef
             ZK_CUDA(cudaGetLastError());
         }
     }
+}
+
+// ------------------------------------------- planned passes (serving loop)
+//
+// The fused LDE's passes as data instead of launches, for a persistent kernel
+// that runs every tile of each pass itself (serve_loop.cu): the same chunks,
+// arguments and tables as lde_rows_device, with the row-output pass at radix
+// 2^8 whatever the tuning table says (the loop compiles a fixed set of pass
+// shapes; every split gives the same rows).
+static constexpr uint32_t LOOP_LAST_LOGR = MAX_ROWS_LOGR;
+
+bool lde_rows_plan_tables_resident(DeviceCtx &c, uint32_t lg_n, uint32_t rate, uint64_t coset_gen)
+{
+    if (!c.lde_tabs.count(std::make_tuple(lg_n, rate, coset_gen % GL_P)) || !c.tw[0][12]) return false;
+    for (const Pass &ps : plan_passes_last(lg_n, true, LOOP_LAST_LOGR))
+        if (ps.s_lo && !c.tw[0][ps.s_lo + ps.logr]) return false;
+    return true;
+}
+
+void lde_rows_plan_tables(DeviceCtx &c, uint32_t lg_n, uint32_t rate, uint64_t coset_gen)
+{
+    c.lde_table(lg_n, rate, coset_gen % GL_P);
+    c.twiddles(12, false);
+    for (const Pass &ps : plan_passes_last(lg_n, true, LOOP_LAST_LOGR))
+        if (ps.s_lo) c.twiddles(ps.s_lo + ps.logr, false);
+}
+
+std::vector<PlannedPass> lde_rows_plan(DeviceCtx &c, uint64_t *rows, const uint64_t *coeffs, uint32_t lg_n,
+                                       uint32_t rate, uint64_t cols, uint64_t coset_gen, uint64_t *scratch)
+{
+    if (!lde_rows_plan_tables_resident(c, lg_n, rate, coset_gen)) throw arg_failure("tables of this shape not built");
+    const uint64_t n = 1ULL << lg_n;
+    const auto passes = plan_passes_last(lg_n, true, LOOP_LAST_LOGR);
+    const bool multi = passes.size() > 1;
+    const uint64_t chunk = multi ? lde_rows_chunk_cols(lg_n, rate, cols) : cols;
+    if (multi && !scratch) throw arg_failure("null scratch");
+    const uint64_t *tab = c.lde_table(lg_n, rate, coset_gen % GL_P);
+    std::vector<PlannedPass> out;
+    for (uint64_t c0 = 0; c0 < cols; c0 += chunk) {
+        const uint64_t cc = cols - c0 < chunk ? cols - c0 : chunk;
+        for (size_t pi = 0; pi < passes.size(); pi++) {
+            const Pass &ps = passes[pi];
+            const bool first = pi == 0, last = pi + 1 == passes.size();
+            PlannedPass pp{};
+            NttPassArgs &a = pp.a;
+            a.src = first ? coeffs + c0 * n : scratch;
+            a.src_stride = n;
+            a.tab = tab;
+            a.tw_small = c.twiddles(12, false);
+            a.tw_pass = ps.s_lo ? c.twiddles(ps.s_lo + ps.logr, false) : nullptr;
+            a.vcols = cc << rate;
+            a.L = lg_n;
+            a.s_lo = ps.s_lo;
+            a.rate = rate;
+            a.cols = (uint32_t)cc;
+            a.row_stride = cols;
+            a.dst = last ? rows + c0 : scratch;
+            a.dst_stride = n;
+            a.src_len = first ? (cols - c0) * n : (n << rate) * chunk;
+            a.dst_len = last ? (n << rate) * cols - c0 : (n << rate) * chunk;
+            a.tab_len = n << rate;
+            if (last) {
+                const uint32_t W = (uint32_t)std::min<uint64_t>(n, PASS_TILE / 16);
+                pp.grid = (n / W) * ((cc + 15) / 16) * (1ULL << rate);
+            } else {
+                pp.grid = a.vcols * (n / std::min<uint64_t>(n, PASS_TILE));
+            }
+            pp.logr = ps.logr;
+            pp.load = first ? LOAD_COSETS : LOAD_PLAIN;
+            pp.store = last ? STORE_ROWS : STORE_SAME;
+            pp.direct = direct_io(ps.logr, a, last) ? 1 : 0;
+            out.push_back(pp);
+        }
+    }
+    return out;
 }
 
 // Passes of the fused LDE of 2^lg_n-point columns: (s_lo, log radix) pairs.

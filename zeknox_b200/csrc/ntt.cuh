@@ -27,6 +27,7 @@
 #include "bounds.cuh"
 #include "bulk.cuh"
 #include "gl64.cuh"
+#include "ntt_args.h"
 
 namespace zk {
 
@@ -235,44 +236,6 @@ __device__ __forceinline__ void dif_regs(uint64_t *x)
 // power-of-two access stride used below hits 16 distinct 8-byte banks.
 __device__ __forceinline__ uint32_t swz(uint32_t w) { return w ^ (((w >> 4) ^ (w >> 8) ^ (w >> 12)) & 15u); }
 
-enum NttLoad : int {
-    LOAD_PLAIN = 0,      // src[v * src_stride + j]
-    LOAD_SCALE = 1,      // src[v * src_stride + j] * tab[j]              (coset powers g^j)
-    LOAD_COSETS = 2,     // src[(v >> rate) * src_stride + j] * tab[(v & (2^rate-1)) * n + j]
-    LOAD_EXTEND = 3,     // j < n_src ? src[v * src_stride + j] : 0        (zero-extended transform)
-};
-
-enum NttStore : int {
-    STORE_SAME = 0,      // dst[v * dst_stride + position]
-    STORE_ROWS = 1,      // leaf-major: dst[(rev_rate(v & mask) * n + position) * cols + (v >> rate)]
-};
-
-struct NttPassArgs {
-    const uint64_t *src;
-    uint64_t *dst;
-    const uint64_t *tab;      // LOAD_SCALE / LOAD_COSETS / LOAD_EXTEND_SCALE table
-    const uint64_t *tw_pass;  // w_M^t, t < M   (M = R * S); unused when S == 1
-    const uint64_t *tw_small; // w_4096^t, t < 4096 (inverse roots for INV)
-    uint64_t src_stride;      // elements between consecutive source columns
-    uint64_t dst_stride;
-    uint64_t n_src;           // LOAD_EXTEND: nonzero prefix length
-    uint64_t vcols;           // virtual columns
-    uint32_t L;               // log2 transform size
-    uint32_t s_lo;            // lowest stage of this pass
-    uint32_t rate;            // LOAD_COSETS / STORE_ROWS: log2 cosets per column
-    uint32_t cols;            // STORE_ROWS: real columns in this launch
-    uint64_t row_stride;      // STORE_ROWS: words per output row (>= cols; dst points at the first column)
-    // STORE_ROWS scattered over destination buffers (null: one buffer, dst):
-    // row r goes to dst_tab[r >> log_rows_per_dst] at row r & (2^log_rows_per_dst - 1),
-    // column col_offset + b -- the buffers may be other GPUs' memory (P2P stores)
-    uint64_t *const *dst_tab;
-    uint32_t log_rows_per_dst;
-    uint64_t col_offset;
-    // extents in words of src, dst (each destination buffer for dst_tab) and
-    // tab from the pass's first element on: read only by the checked build
-    uint64_t src_len, dst_len, tab_len;
-};
-
 // Sub-step of the in-CTA R-point DIF: every task owns E elements spaced Q apart
 // inside a block of size R_cur = E * Q.  The task base (block * R_cur + m_lo,
 // m_lo < Q) and the element offsets e * Q occupy disjoint bits, and swz() is
@@ -386,232 +349,25 @@ __host__ __device__ constexpr int pass_threads_per_sm()
     return (LOADM == LOAD_COSETS && STOREM == STORE_SAME && LOGR < 10) ? 1280 : 1024;
 }
 
+// One CTA's work of a pass: tile ZK_PASS_BLK of the launch described by `a`,
+// with TILE words of shared memory at sm.  ntt_pass_kernel runs it for its own
+// block index; ntt_pass_body for any tile (the persistent serving loop runs
+// every tile of a pass through it).
 template <int LOGR, int INV, int NT, int TILE, int LOADM, int STOREM, int DIRECT>
 __global__ void __launch_bounds__(NT, pass_threads_per_sm<LOGR, LOADM, STOREM>() / NT) ntt_pass_kernel(NttPassArgs a)
 {
     extern __shared__ uint64_t sm[];
-    constexpr uint32_t R = 1u << LOGR;
-    constexpr uint32_t LOG_CW = 4, CW = 1u << LOG_CW;
-    constexpr uint32_t LOG_TILE = __builtin_ctz(TILE);
-    constexpr int E0 = LOGR >= 4 ? 4 : LOGR;     // log2 size of the first sub-step
-    constexpr int LAST = last_substep_log(LOGR);  // log2 size of the last sub-step
-    // all sizes are powers of two: index math is shifts and masks
-    const uint32_t s_lo = a.s_lo;
-    const uint32_t S = 1u << s_lo;
-    const uint32_t log_m = s_lo + LOGR;  // log2 M, M = R * S
-    const uint32_t rmask = (1u << a.rate) - 1;
-    const uint32_t log_w = (STOREM == STORE_ROWS) ? (a.L < LOG_TILE - LOG_CW ? a.L : LOG_TILE - LOG_CW) : 0;
-    const uint32_t log_tile = (STOREM == STORE_ROWS) ? LOG_CW + log_w : (a.L < LOG_TILE ? a.L : LOG_TILE);
-    const uint32_t tile = 1u << log_tile;
-    const uint32_t log_g = log_tile - LOGR;       // groups per tile
-    const uint32_t log_gw = log_w - LOGR;         // groups per virtual column (row tiles)
+#define ZK_PASS_BLK blockIdx.x
+#include "ntt_pass_body.inc"
+#undef ZK_PASS_BLK
+}
 
-    uint64_t v0, pos0;
-    if (STOREM == STORE_ROWS) {
-        const uint32_t log_per_v = a.L - log_w;
-        const uint64_t t = blockIdx.x;
-        const uint64_t posblk = t & ((1ULL << log_per_v) - 1), cg = t >> log_per_v;
-        const uint64_t ncg = (a.cols + CW - 1) >> LOG_CW;
-        const uint64_t coset = cg / ncg, colg = cg - coset * ncg;
-        v0 = ((colg << LOG_CW) << a.rate) | coset;
-        pos0 = posblk << log_w;
-    } else {
-        const uint32_t log_tpv = a.L - log_tile;
-        v0 = (uint64_t)blockIdx.x >> log_tpv;
-        pos0 = ((uint64_t)blockIdx.x & ((1ULL << log_tpv) - 1)) << log_tile;
-    }
-    const uint64_t gid0 = pos0 >> LOGR;
-
-    // tile element (group g, member m) -> (virtual column, position)
-    auto gpos = [&](uint32_t g, uint32_t m, uint64_t &vcol, uint64_t &pos) {
-        if (STOREM == STORE_ROWS) {
-            const uint32_t c = g >> log_gw, gg = g & ((1u << log_gw) - 1);
-            vcol = v0 + ((uint64_t)c << a.rate);
-            pos = pos0 + ((uint64_t)gg << LOGR) + m;
-        } else {
-            vcol = v0;
-            const uint64_t gid = gid0 + g;
-            pos = ((gid >> s_lo) << log_m) + ((uint64_t)m << s_lo) + (gid & (S - 1));
-        }
-    };
-    auto col_ok = [&](uint64_t vcol) {
-        return (STOREM == STORE_ROWS) ? ((vcol >> a.rate) < a.cols) : (vcol < a.vcols);
-    };
-    // the load-mode transform of the element at (vcol, pos); elements of one
-    // group member run m -> m + q are `step` positions apart
-    auto load_elem = [&](uint64_t vcol, uint64_t pos) -> uint64_t {
-        if (LOADM == LOAD_PLAIN) {
-            const uint64_t si = vcol * a.src_stride + pos;
-            return ZK_IN_BOUNDS(si, a.src_len, OOB_NTT_SRC) ? a.src[si] : 0;
-        }
-        if (LOADM == LOAD_SCALE) {
-            const uint64_t si = vcol * a.src_stride + pos;
-            return gl_mul_nc(ZK_IN_BOUNDS(si, a.src_len, OOB_NTT_SRC) ? a.src[si] : 0,
-                             ZK_IN_BOUNDS(pos, a.tab_len, OOB_NTT_TAB) ? __ldg(a.tab + pos) : 0);
-        }
-        if (LOADM == LOAD_COSETS) {
-            const uint64_t si = (vcol >> a.rate) * a.src_stride + pos, ti = ((vcol & rmask) << a.L) + pos;
-            return gl_mul_nc(ZK_IN_BOUNDS(si, a.src_len, OOB_NTT_SRC) ? a.src[si] : 0,
-                             ZK_IN_BOUNDS(ti, a.tab_len, OOB_NTT_TAB) ? __ldg(a.tab + ti) : 0);
-        }
-        if (pos >= a.n_src) return 0;  // LOAD_EXTEND
-        const uint64_t si = vcol * a.src_stride + pos;
-        return ZK_IN_BOUNDS(si, a.src_len, OOB_NTT_SRC) ? a.src[si] : 0;
-    };
-    // pass twiddle (S > 1) and the store of one element
-    auto store_elem = [&](uint64_t vcol, uint64_t pos, uint32_t m, uint64_t val) {
-        if (S > 1) {
-            const uint64_t o = pos & (S - 1);
-            const uint64_t f = bitrev32(m, LOGR);
-            val = gl_mul_nc(val, ZK_IN_BOUNDS(o * f, 1ULL << log_m, OOB_NTT_TWIDDLE) ? __ldg(a.tw_pass + o * f) : 0);
-        }
-        val = gl_canon(val);  // global memory holds canonical values
-        if (STOREM == STORE_ROWS) {
-            const uint64_t b = vcol >> a.rate;
-            if (b < a.cols) {
-                const uint64_t row = ((uint64_t)bitrev32((uint32_t)(vcol & rmask), a.rate) << a.L) + pos;
-                if (a.dst_tab) {
-                    uint64_t *d = a.dst_tab[row >> a.log_rows_per_dst];
-                    const uint64_t di = (row & ((1ULL << a.log_rows_per_dst) - 1)) * a.row_stride + a.col_offset + b;
-                    if (ZK_IN_BOUNDS(di, a.dst_len, OOB_NTT_SCATTER)) d[di] = val;
-                } else {
-                    if (ZK_IN_BOUNDS(row * a.row_stride + b, a.dst_len, OOB_NTT_ROWS)) a.dst[row * a.row_stride + b] = val;
-                }
-            }
-        } else if (vcol < a.vcols) {
-            if (ZK_IN_BOUNDS(vcol * a.dst_stride + pos, a.dst_len, OOB_NTT_DST)) a.dst[vcol * a.dst_stride + pos] = val;
-        }
-    };
-    // linear index e -> (g, m) so that consecutive e are consecutive addresses
-    auto split_in = [&](uint32_t e, uint32_t &g, uint32_t &m) {
-        if (STOREM == STORE_ROWS) {
-            const uint32_t c = e >> log_w, w = e & ((1u << log_w) - 1);
-            g = (c << log_gw) + (w >> LOGR);
-            m = w & (R - 1);
-        } else if (s_lo >= log_g) {
-            g = e & ((1u << log_g) - 1);
-            m = e >> log_g;
-        } else {
-            const uint32_t blk = e >> log_m, rem = e & ((1u << log_m) - 1);
-            m = rem >> s_lo;
-            g = (blk << s_lo) + (rem & (S - 1));
-        }
-    };
-
-    if constexpr (!DIRECT) {
-        // ---- load
-        for (uint32_t e = threadIdx.x; e < tile; e += NT) {
-            uint32_t g, m;
-            split_in(e, g, m);
-            uint64_t vcol, pos;
-            gpos(g, m, vcol, pos);
-            sm[swz((g << LOGR) + m)] = col_ok(vcol) ? load_elem(vcol, pos) : 0;
-        }
-        __syncthreads();
-        // ---- R-point DIF in sub-steps of up to 16 points
-        dif_substeps<LOGR, INV, NT, LOGR>(sm, tile, a.tw_small);
-    } else {
-        // ---- first sub-step straight from global memory: task (g, m_lo)
-        // holds members m_lo + e * Q0; lanes of a warp take consecutive
-        // positions (consecutive m_lo for row tiles, consecutive g otherwise)
-        constexpr uint32_t Q0 = 1u << (LOGR - E0);
-        constexpr bool FUSED = (STOREM == STORE_SAME) && (LAST == LOGR);  // one sub-step, global to global
-        const uint32_t tasks = tile >> E0;
-        for (uint32_t t = threadIdx.x; t < tasks; t += NT) {
-            uint32_t g, m_lo;
-            if (STOREM == STORE_ROWS) {
-                m_lo = t & (Q0 - 1);
-                g = t >> (LOGR - E0);
-            } else {
-                g = t & ((1u << log_g) - 1);
-                m_lo = t >> log_g;
-            }
-            uint64_t vcol, pos;
-            gpos(g, m_lo, vcol, pos);
-            const uint64_t step = (STOREM == STORE_ROWS) ? (uint64_t)Q0 : ((uint64_t)Q0 << s_lo);
-            const bool ok = col_ok(vcol);
-            uint64_t x[1 << E0];
-#pragma unroll
-            for (int e = 0; e < (1 << E0); e++) x[e] = ok ? load_elem(vcol, pos + e * step) : 0;
-            dif_regs<E0, INV>(x);
-            if constexpr (FUSED) {
-                // block of R consecutive members, bit-reversed in place
-#pragma unroll
-                for (int e = 0; e < (1 << E0); e++) store_elem(vcol, pos + e * step, (uint32_t)e, x[e]);
-            } else {
-                first_substep_twiddles<E0, LOGR>(x, m_lo, a.tw_small);
-                const uint32_t sb = swz((g << LOGR) + m_lo);
-#pragma unroll
-                for (int e = 0; e < (1 << E0); e++) sm[sb ^ swz_c(e * Q0)] = x[e];
-            }
-        }
-        if constexpr (FUSED) return;
-        __syncthreads();
-        if constexpr (STOREM == STORE_ROWS) {
-            if constexpr (LOGR > 4) dif_substeps<LOGR, INV, NT, LOGR - 4>(sm, tile, a.tw_small);
-        } else {
-            dif_middle_substeps<INV, NT, LOGR - 4, LAST>(sm, tile, a.tw_small);
-            // ---- last sub-step (blocks of 2^LAST consecutive members) straight
-            // to global memory with the pass twiddle; lanes take consecutive g
-            constexpr uint32_t EL = 1u << LAST;
-            const uint32_t ltasks = tile >> LAST;
-            for (uint32_t t = threadIdx.x; t < ltasks; t += NT) {
-                const uint32_t g = t & ((1u << log_g) - 1);
-                const uint32_t mb = (t >> log_g) << LAST;
-                const uint32_t sb = swz((g << LOGR) + mb);
-                uint64_t x[EL];
-#pragma unroll
-                for (int e = 0; e < (int)EL; e++) x[e] = sm[sb ^ swz_c((uint32_t)e)];
-                dif_regs<LAST, INV>(x);
-                uint64_t vcol, pos;
-                gpos(g, mb, vcol, pos);
-#pragma unroll
-                for (int e = 0; e < (int)EL; e++) store_elem(vcol, pos + ((uint64_t)e << s_lo), mb + e, x[e]);
-            }
-            return;
-        }
-    }
-
-    if constexpr (STOREM == STORE_ROWS && NT == 256 && LOGR >= 4) {
-        // Row tile of 16 virtual columns (one coset, consecutive real columns)
-        // x 2^LOGR consecutive positions, the groups being whole rows of the
-        // tile (log_w == LOGR): thread (c, w0) writes column c of rows w0,
-        // w0 + 16, ...; a warp stores two 128-byte row segments per step.
-        // The destination advances by 16 rows per step and the shared-memory
-        // index by a compile-time constant (swz is linear over XOR, and c,
-        // w0 and the step occupy disjoint bits).
-        if (log_w == (uint32_t)LOGR && !a.dst_tab) {
-            const uint32_t c = threadIdx.x & 15u, w0 = threadIdx.x >> 4;
-            const uint64_t b = (v0 >> a.rate) + c;
-            if (b < a.cols) {
-                const uint64_t row0 = ((uint64_t)bitrev32((uint32_t)(v0 & rmask), a.rate) << a.L) + pos0 + w0;
-                uint64_t *d = a.dst + row0 * a.row_stride + b;
-                const uint64_t dstep = 16 * a.row_stride;
-                const uint32_t sb = swz((c << LOGR) + w0);
-#pragma unroll
-                for (uint32_t k = 0; k < R / 16; k++) {
-                    if (ZK_IN_BOUNDS((row0 + 16 * k) * a.row_stride + b, a.dst_len, OOB_NTT_ROWS))
-                        *d = gl_canon(sm[sb ^ swz_c(16 * k)]);
-                    d += dstep;
-                }
-            }
-            return;
-        }
-    }
-    // ---- pass twiddle + store through shared memory
-    for (uint32_t e = threadIdx.x; e < tile; e += NT) {
-        uint32_t g, m;
-        if (STOREM == STORE_ROWS) {
-            const uint32_t w = e >> LOG_CW, c = e & (CW - 1);  // consecutive e -> consecutive columns of one row
-            g = (c << log_gw) + (w >> LOGR);
-            m = w & (R - 1);
-        } else {
-            split_in(e, g, m);
-        }
-        uint64_t vcol, pos;
-        gpos(g, m, vcol, pos);
-        store_elem(vcol, pos, m, sm[swz((g << LOGR) + m)]);
-    }
+template <int LOGR, int INV, int NT, int TILE, int LOADM, int STOREM, int DIRECT>
+__device__ __forceinline__ void ntt_pass_body(const NttPassArgs &a, uint32_t blk, uint64_t *sm)
+{
+#define ZK_PASS_BLK blk
+#include "ntt_pass_body.inc"
+#undef ZK_PASS_BLK
 }
 
 // ------------------------------------------------------------------ reorders

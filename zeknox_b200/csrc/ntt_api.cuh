@@ -5,6 +5,7 @@
 #include <utility>
 #include <vector>
 
+#include "ntt_args.h"
 #include "runtime.cuh"
 
 namespace zk {
@@ -50,6 +51,22 @@ void lde_rows_explicit(cudaStream_t stream, uint64_t *rows, const uint64_t *coef
                        uint64_t cols, const uint64_t *lde_tab, const uint64_t *const *tw, uint64_t *scratch,
                        uint64_t chunk_cols);
 std::vector<std::pair<uint32_t, uint32_t>> lde_rows_passes(uint32_t lg_n);
+
+// The fused LDE's passes as data (the persistent serving loop runs them):
+// every pass of every column chunk with its arguments, tile count and kernel
+// shape (radix, load and store modes, direct first sub-step), the row-output
+// pass at radix 2^8.  The tables must be resident (lde_rows_plan_tables, on a
+// stream no persistent kernel occupies); `scratch` as for lde_rows_device.
+struct PlannedPass {
+    NttPassArgs a;
+    uint64_t grid;
+    uint32_t logr;
+    int load, store, direct;
+};
+bool lde_rows_plan_tables_resident(DeviceCtx &c, uint32_t lg_n, uint32_t rate, uint64_t coset_gen);
+void lde_rows_plan_tables(DeviceCtx &c, uint32_t lg_n, uint32_t rate, uint64_t coset_gen);
+std::vector<PlannedPass> lde_rows_plan(DeviceCtx &c, uint64_t *rows, const uint64_t *coeffs, uint32_t lg_n,
+                                       uint32_t rate, uint64_t cols, uint64_t coset_gen, uint64_t *scratch);
 
 // Build every table a commit of this shape uses (before graph capture).
 void prepare_tables(DeviceCtx &c, uint32_t lg_n, uint32_t rate, uint64_t coset_gen, bool values);

@@ -19,6 +19,12 @@
 // Device side: jobs on different slots overlap; twiddle, coset and
 // round-constant tables stay resident in the device context across requests
 // (zeknox_server_prepare builds them ahead of the stream).
+//
+// Device-loop mode (zeknox_server_create_ex with ZK_SERVE_DEVICE_LOOP): the
+// same admission, but an admitted job is not launched from the host.  Its
+// stages are planned on the host, copied to device memory and posted to a
+// ring in mapped host memory, and a persistent cooperative kernel
+// (serve_loop.cuh) runs them, one request at a time across the whole GPU.
 #include <cuda_runtime.h>
 #include <string.h>
 
@@ -33,7 +39,10 @@
 
 #include "../../include/zeknox_b200.h"
 #include "batch.cuh"
+#include "ntt_api.cuh"
 #include "runtime.cuh"
+#include "serve_loop.cuh"
+#include "zk_constants.h"
 
 namespace zk {
 namespace {
@@ -117,6 +126,20 @@ struct Server {
     int inject_next = 0;        // test hook: the next start fails at this stage (ZK_SERVE_FAIL_*)
     bool stop = false;
     std::thread worker;
+
+    // device-loop mode
+    bool device_loop = false;
+    LoopRing *ring = nullptr, *ring_dev = nullptr;  // mapped host memory, and its device address
+    LoopCtl *ctl = nullptr;                         // device
+    LoopStage *plans = nullptr;                     // device: LOOP_RING x LOOP_MAX_STAGES
+    LoopStage *plans_host = nullptr;                // pinned staging of the same shape
+    cudaStream_t loop_stream = nullptr, copy_stream = nullptr;
+    cudaEvent_t loop_exit = nullptr;
+    bool loop_live = false;
+    int loop_grid = 0;
+    uint64_t posted = 0, retired = 0;               // ring entries posted / retired by this host
+    uint64_t ring_ticket[LOOP_RING] = {};
+    uint32_t loop_depth = 1;                        // entries in flight at most
 
     // Arena bytes of a job: leaves, digests, caps and LDE scratch, each
     // starting on an ARENA_ALIGN boundary.
@@ -212,8 +235,270 @@ struct Server {
         }
     }
 
+    // ---------------------------------------------------- device-loop mode
+
+    // The loop kernel is running (it exits after an idle period).
+    bool loop_running()
+    {
+        if (!loop_live) return false;
+        const cudaError_t q = cudaEventQuery(loop_exit);
+        if (q == cudaErrorNotReady) return true;
+        loop_live = false;
+        if (q != cudaSuccess) (void)cudaGetLastError();
+        return false;
+    }
+
+    // Launch the loop if entries wait and it is not running.
+    void loop_ensure()
+    {
+        if (loop_running()) return;
+        const uint64_t tail = __atomic_load_n(&ring->tail, __ATOMIC_ACQUIRE);
+        if (tail >= posted) return;
+        LoopCtl init{};
+        init.taken = tail;
+        ZK_CUDA(cudaMemcpyAsync(ctl, &init, sizeof init, cudaMemcpyHostToDevice, loop_stream));
+        void *args[] = {(void *)&ring_dev, (void *)&ctl};
+        ZK_CUDA(cudaLaunchCooperativeKernel((const void *)serve_loop_kernel, dim3(loop_grid), dim3(LOOP_THREADS), args,
+                                            LOOP_SMEM_BYTES, loop_stream));
+        note_launch();
+        ZK_CUDA(cudaEventRecord(loop_exit, loop_stream));
+        loop_live = true;
+    }
+
+    // Let the loop finish what is posted and exit (so kernels on other streams
+    // get the SMs: table builds).
+    void loop_stop()
+    {
+        if (!loop_running()) return;
+        __atomic_store_n(&ring->close, 1u, __ATOMIC_RELEASE);
+        (void)cudaEventSynchronize(loop_exit);
+        __atomic_store_n(&ring->close, 0u, __ATOMIC_RELEASE);
+        loop_live = false;
+    }
+
+    // Stages of the forest, as merkle.cu launches them for Poseidon and
+    // Poseidon2 (cooperative leaves up to coop_leaves, node-parallel wide
+    // levels, the cooperative fold, levels beyond the tail's capacity, the
+    // cooperative tail); every stage gives the same digests as its kernel.
+    static void merkle_stages(std::vector<LoopStage> &out, uint64_t *digests, uint64_t *caps, const uint64_t *leaves,
+                              uint64_t n_leaves, uint64_t leaf_size, uint32_t cap_height, uint32_t hash)
+    {
+        MerkleGeom g{};
+        g.n_leaves = n_leaves;
+        g.leaf_size = leaf_size;
+        g.n_caps = 1u << cap_height;
+        g.sub_leaves = n_leaves >> cap_height;
+        g.sub_digests = 2 * g.sub_leaves - 2;
+        g.log_sub = ilog2_exact(g.sub_leaves);
+        auto stage = [&](uint32_t kind, uint32_t u, uint64_t blocks) {
+            LoopStage st{};
+            st.kind = kind;
+            st.hash = hash;
+            st.u = u;
+            st.blocks = blocks;
+            st.leaves = leaves;
+            st.digests = digests;
+            st.caps = caps;
+            st.g = g;
+            out.push_back(st);
+        };
+        const uint32_t lg_leaves = ilog2_exact(n_leaves);
+        const std::string h = std::to_string(hash);
+        if (n_leaves <= tune_get("coop_leaves." + h, lg_leaves, 1ULL << 13))
+            stage(LS_LEAF_COOP, 0, (n_leaves + LOOP_THREADS / 4 - 1) / (LOOP_THREADS / 4));
+        else
+            stage(LS_LEAF, 0, (n_leaves + LOOP_THREADS - 1) / LOOP_THREADS);
+        if (g.sub_leaves == 1) return;
+        const uint64_t wide = tune_get("wide_level_nodes." + h, lg_leaves, 1ULL << 15);
+        const uint32_t top = g.log_sub - 1;
+        uint32_t u0 = 0;
+        while (u0 + 1 <= top && (n_leaves >> (u0 + 1)) >= wide) {
+            u0++;
+            stage(LS_LEVEL, u0, ((n_leaves >> u0) + LOOP_THREADS - 1) / LOOP_THREADS);
+        }
+        constexpr uint32_t NG = LOOP_THREADS / 4;
+        stage(LS_FOLD_COOP, u0, ((n_leaves >> u0) + NG - 1) / NG);
+        if ((g.sub_leaves >> u0) <= NG) return;  // caps written by the fold
+        uint32_t U = 0;
+        while ((1u << (U + 1)) <= NG && u0 + U + 1 <= top) U++;
+        u0 += U;
+        while ((g.sub_leaves >> u0) > LOOP_TAIL_MAXM) {
+            u0++;
+            stage(LS_LEVEL, u0, (((g.sub_leaves >> u0) * g.n_caps) + LOOP_THREADS - 1) / LOOP_THREADS);
+        }
+        stage(LS_TAIL_COOP, u0, g.n_caps);
+    }
+
+    // Plan an admitted job, copy the plan to the device and post it to the
+    // ring.  Server thread, without `mu`; returns 1 or a negative status.
+    int loop_start(Ticket &t, uint64_t id, int inject)
+    {
+        const zk_serve_request &r = t.req;
+        NvtxRange range("zeknox serve post");
+        std::lock_guard<std::recursive_mutex> lk(ctx->mu);
+        try {
+            const uint64_t N = 1ULL << (r.lg_n + r.rate_bits);
+            if (inject == ZK_SERVE_FAIL_ALLOC)
+                throw cuda_failure(-(int)cudaErrorMemoryAllocation, "device allocation refused (injected)");
+            if (inject == ZK_SERVE_FAIL_SHAPE) throw arg_failure("shape rejected (injected)");
+            const uint64_t gen = (r.coset_gen ? r.coset_gen : ZK_GENERATOR) % GL_P;
+            if (!lde_rows_plan_tables_resident(*ctx, r.lg_n, r.rate_bits, gen)) {
+                // the table kernels need SMs the loop occupies
+                loop_stop();
+                lde_rows_plan_tables(*ctx, r.lg_n, r.rate_bits, gen);
+                ctx->sync();
+            }
+            std::vector<LoopStage> plan;
+            for (const PlannedPass &pp :
+                 lde_rows_plan(*ctx, t.leaves, r.input, r.lg_n, r.rate_bits, r.cols, gen, t.scratch)) {
+                const bool ok = pp.direct && ((pp.load == LOAD_COSETS && pp.store == STORE_SAME && pp.logr >= 1 &&
+                                               pp.logr <= 10) ||
+                                              (pp.load == LOAD_PLAIN && pp.store == STORE_SAME && pp.logr >= 5 &&
+                                               pp.logr <= 7) ||
+                                              (pp.load == LOAD_PLAIN && pp.store == STORE_ROWS && pp.logr == 8));
+                if (!ok) throw arg_failure("a pass shape the device loop does not run");
+                LoopStage st{};
+                st.kind = LS_PASS;
+                st.logr = pp.logr;
+                st.load = (uint32_t)pp.load;
+                st.store = (uint32_t)pp.store;
+                st.blocks = pp.grid;
+                st.a = pp.a;
+                plan.push_back(st);
+            }
+            merkle_stages(plan, t.digests, t.caps, t.leaves, N, r.cols, r.cap_height, r.hash_type);
+            if (plan.size() > LOOP_MAX_STAGES) throw arg_failure("request needs more stages than a ring entry holds");
+            if (inject == ZK_SERVE_FAIL_LAUNCH)
+                throw cuda_failure(-(int)cudaErrorLaunchFailure, "kernel launch refused (injected)");
+            const uint32_t k = (uint32_t)(posted % LOOP_RING);
+            LoopStage *host = plans_host + (uint64_t)k * LOOP_MAX_STAGES;
+            LoopStage *dev = plans + (uint64_t)k * LOOP_MAX_STAGES;
+            memcpy(host, plan.data(), plan.size() * sizeof(LoopStage));
+            ZK_CUDA(cudaMemcpyAsync(dev, host, plan.size() * sizeof(LoopStage), cudaMemcpyHostToDevice, copy_stream));
+            ZK_CUDA(cudaStreamSynchronize(copy_stream));
+            LoopSlot &sl = ring->slot[k];
+            sl.n_stages = (uint32_t)plan.size();
+            sl.stages = dev;
+            const bool gate_shut = inject == ZK_SERVE_FAIL_GATE;
+            sl.ready_ns = gate_shut ? 20000000ULL : 10000000000ULL;
+            __atomic_store_n(&sl.done, (uint32_t)LOOP_DONE_NONE, __ATOMIC_RELAXED);
+            __atomic_store_n(&sl.ready, gate_shut ? 0u : 1u, __ATOMIC_RELEASE);
+            ring_ticket[k] = id;
+            posted++;
+            __atomic_store_n(&ring->head, posted, __ATOMIC_RELEASE);
+            loop_ensure();
+            return 1;
+        } catch (const std::exception &e) {
+            const cuda_failure *cf = dynamic_cast<const cuda_failure *>(&e);
+            const arg_failure *af = dynamic_cast<const arg_failure *>(&e);
+            (void)cudaGetLastError();
+            return cf ? (cf->code < 0 ? cf->code : -1) : af ? -af->code : -1;
+        }
+    }
+
+    // Retire ring entries in order (caller holds mu); true if any finished.
+    bool loop_retire()
+    {
+        bool progressed = false;
+        while (retired < posted) {
+            const uint32_t k = (uint32_t)(retired % LOOP_RING);
+            LoopSlot &sl = ring->slot[k];
+            const uint32_t d = __atomic_load_n(&sl.done, __ATOMIC_ACQUIRE);
+            if (d == LOOP_DONE_NONE) {
+                // not done: relaunch the loop if it exited before taking it
+                std::lock_guard<std::recursive_mutex> dl(ctx->mu);
+                try {
+                    loop_ensure();
+                } catch (const std::exception &) {
+                    (void)cudaGetLastError();
+                }
+                break;
+            }
+            Ticket &t = tickets[ring_ticket[k]];
+            int status = 2;
+            if (d == LOOP_DONE_OK) {
+                if (t.req.caps_host) {
+                    const uint64_t n_caps = 1ULL << t.req.cap_height;
+                    cudaError_t e = cudaMemcpyAsync(t.req.caps_host, t.caps, n_caps * 32, cudaMemcpyDeviceToHost,
+                                                    copy_stream);
+                    if (e == cudaSuccess) e = cudaStreamSynchronize(copy_stream);
+                    if (e != cudaSuccess) status = -(int)e;
+                }
+            } else {
+                status = -(int)cudaErrorLaunchTimeout;  // a bounded wait of the loop ran out
+            }
+            t.status = status;
+            t.t_done = Clock::now();
+            __atomic_store_n(&sl.done, (uint32_t)LOOP_DONE_NONE, __ATOMIC_RELAXED);
+            ring_ticket[k] = 0;
+            retired++;
+            completed++;
+            progressed = true;
+        }
+        return progressed;
+    }
+
+    void loop_device_mode()
+    {
+        std::unique_lock<std::mutex> lk(mu);
+        while (true) {
+            if (loop_retire()) cv.notify_all();
+            while (!queue.empty() && posted - retired < loop_depth) {
+                auto pick = queue.begin();
+                if (!ranges.fits(tickets[*pick].bytes)) {
+                    if (blocked_head != *pick) {
+                        blocked_head = *pick;
+                        bypassed = 0;
+                    }
+                    if (bypassed >= loop_depth) break;
+                    for (++pick; pick != queue.end(); ++pick) {
+                        const uint64_t b = tickets[*pick].bytes;
+                        if (b <= budget / 8 && ranges.fits(b)) break;
+                    }
+                    if (pick == queue.end()) break;
+                    bypassed++;
+                }
+                const uint64_t id = *pick;
+                Ticket &t = tickets[id];
+                queue.erase(pick);
+                t.off = ranges.take(t.bytes);
+                in_use += t.bytes;
+                peak = in_use > peak ? in_use : peak;
+                place(t);
+                t.t_admit = Clock::now();
+                t.status = 1;
+                const int inject = inject_next;
+                inject_next = 0;
+                lk.unlock();
+                const int st = loop_start(t, id, inject);
+                lk.lock();
+                if (st < 0) {
+                    t.status = st;
+                    t.t_done = Clock::now();
+                    unadmit(t);
+                }
+                cv.notify_all();
+            }
+            const bool busy = retired < posted;
+            if (stop && !busy && queue.empty()) break;
+            if (busy) {
+                lk.unlock();
+                std::this_thread::sleep_for(std::chrono::microseconds(50));
+                lk.lock();
+            } else {
+                cv.wait_for(lk, std::chrono::milliseconds(5));
+            }
+        }
+        std::lock_guard<std::recursive_mutex> dl(ctx->mu);
+        loop_stop();
+    }
+
     void loop()
     {
+        if (device_loop) {
+            loop_device_mode();
+            return;
+        }
         std::unique_lock<std::mutex> lk(mu);
         while (true) {
             // retire finished jobs
@@ -330,12 +615,72 @@ RustError guard(F &&f)
 
 using zk::Server;
 
+namespace zk {
+namespace {
+
+// The device-loop resources of a server: the ring, the loop's control block,
+// the plan buffers, two streams and the launch shape (every CTA resident).
+void create_device_loop(Server *s, uint32_t slots)
+{
+    DeviceCtx &c = *s->ctx;
+    int coop = 0;
+    ZK_CUDA(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, c.id));
+    if (!coop) throw arg_failure("the device does not support cooperative launches");
+    ZK_CUDA(cudaFuncSetAttribute(serve_loop_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)LOOP_SMEM_BYTES));
+    int per_sm = 0;
+    ZK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, serve_loop_kernel, LOOP_THREADS, LOOP_SMEM_BYTES));
+    if (per_sm < 1) throw arg_failure("the device loop does not fit on an SM");
+    s->loop_grid = per_sm * c.sm_count;
+    void *h = nullptr;
+    ZK_CUDA(cudaHostAlloc(&h, sizeof(LoopRing), cudaHostAllocMapped | cudaHostAllocPortable));
+    memset(h, 0, sizeof(LoopRing));
+    s->ring = (LoopRing *)h;
+    void *d = nullptr;
+    ZK_CUDA(cudaHostGetDevicePointer(&d, h, 0));
+    s->ring_dev = (LoopRing *)d;
+    s->ring->idle_ns = 20000000ULL;      // 20 ms without a request: the kernel exits
+    s->ring->barrier_ns = 10000000000ULL;  // 10 s: the longest stage (2^25 leaves x 32 permutations) takes ~1.3 s
+    ZK_CUDA(cudaMalloc((void **)&s->ctl, sizeof(LoopCtl)));
+    ZK_CUDA(cudaMalloc((void **)&s->plans, sizeof(LoopStage) * LOOP_RING * LOOP_MAX_STAGES));
+    ZK_CUDA(cudaHostAlloc((void **)&s->plans_host, sizeof(LoopStage) * LOOP_RING * LOOP_MAX_STAGES,
+                          cudaHostAllocDefault));
+    ZK_CUDA(cudaStreamCreateWithFlags(&s->loop_stream, cudaStreamNonBlocking));
+    ZK_CUDA(cudaStreamCreateWithFlags(&s->copy_stream, cudaStreamNonBlocking));
+    ZK_CUDA(cudaEventCreateWithFlags(&s->loop_exit, cudaEventDisableTiming));
+    s->loop_depth = slots < LOOP_RING ? slots : LOOP_RING;
+    s->device_loop = true;
+}
+
+void free_device_loop(Server *s)
+{
+    if (s->loop_stream) {
+        cudaStreamSynchronize(s->loop_stream);
+        cudaStreamDestroy(s->loop_stream);
+    }
+    if (s->copy_stream) cudaStreamDestroy(s->copy_stream);
+    if (s->loop_exit) cudaEventDestroy(s->loop_exit);
+    if (s->ctl) cudaFree(s->ctl);
+    if (s->plans) cudaFree(s->plans);
+    if (s->plans_host) cudaFreeHost(s->plans_host);
+    if (s->ring) cudaFreeHost(s->ring);
+}
+
+}  // namespace
+}  // namespace zk
+
 extern "C" RustError zeknox_server_create(size_t device_id, uint64_t budget_bytes, uint32_t slots, void **server)
+{
+    return zeknox_server_create_ex(device_id, budget_bytes, slots, 0, server);
+}
+
+extern "C" RustError zeknox_server_create_ex(size_t device_id, uint64_t budget_bytes, uint32_t slots, uint32_t flags,
+                                             void **server)
 {
     return zk::guard([&] {
         if (!server) throw zk::arg_failure("null out pointer");
         if (slots == 0 || slots > 64) throw zk::arg_failure("slots must be 1..64");
         if (budget_bytes < zk::ARENA_ALIGN) throw zk::arg_failure("budget below one allocation unit");
+        if (flags & ~(uint32_t)ZK_SERVE_DEVICE_LOOP) throw zk::arg_failure("unknown server flags");
         zk::DeviceCtx &c = zk::device(device_id);
         Server *s = new Server();
         try {
@@ -354,11 +699,16 @@ extern "C" RustError zeknox_server_create(size_t device_id, uint64_t budget_byte
             s->slot_ticket.assign(slots, 0);
             for (auto &st : s->slot_stream) ZK_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
             ZK_CUDA(cudaEventCreateWithFlags(&s->tables_ready, cudaEventDisableTiming));
+            if (flags & ZK_SERVE_DEVICE_LOOP) {
+                std::lock_guard<std::recursive_mutex> dl(c.mu);
+                zk::create_device_loop(s, slots);
+            }
         } catch (...) {
             for (auto &st : s->slot_stream)
                 if (st) cudaStreamDestroy(st);
             if (s->tables_ready) cudaEventDestroy(s->tables_ready);
             if (s->arena) cudaFree(s->arena);
+            zk::free_device_loop(s);
             delete s;
             throw;
         }
@@ -386,6 +736,11 @@ extern "C" RustError zeknox_server_submit(void *server, const zk_serve_request *
         j.digests = (uint64_t *)1;
         j.caps = (uint64_t *)1;
         zk::check_job(j);
+        if (s->device_loop &&
+            (req->input_is_values || (req->hash_type != zk::HASH_POSEIDON && req->hash_type != zk::HASH_POSEIDON2) ||
+             req->lg_n < 9 || req->lg_n > 22))
+            throw zk::arg_failure("the device loop takes coefficient inputs of 2^9 .. 2^22 per column and "
+                                  "Poseidon or Poseidon2 forests");
         const uint64_t bytes = Server::job_bytes(*req);
         std::lock_guard<std::mutex> lk(s->mu);
         if (bytes > s->budget) throw zk::arg_failure("request needs more device memory than the server's budget");
@@ -467,6 +822,9 @@ extern "C" RustError zeknox_server_prepare(void *server, uint32_t lg_n_min, uint
             j.coset_gen = coset_gen;
             j.input_is_values = 1;  // the inverse tables too
             zk::prepare_job(*s->ctx, j);
+            // the device loop's pass split (row-output radix 2^8)
+            if (s->device_loop)
+                zk::lde_rows_plan_tables(*s->ctx, lg, rate_bits, (coset_gen ? coset_gen : ZK_GENERATOR) % zk::GL_P);
         }
         s->ctx->sync();
     });
@@ -497,7 +855,8 @@ extern "C" RustError zeknox_server_inject_failure(void *server, int stage)
 {
     return zk::guard([&] {
         Server *s = zk::as_server(server);
-        if (stage < 0 || stage > ZK_SERVE_FAIL_LAUNCH) throw zk::arg_failure("unknown failure stage");
+        if (stage < 0 || stage > ZK_SERVE_FAIL_GATE) throw zk::arg_failure("unknown failure stage");
+        if (stage == ZK_SERVE_FAIL_GATE && !s->device_loop) throw zk::arg_failure("the start gate is the device loop's");
         std::lock_guard<std::mutex> lk(s->mu);
         s->inject_next = stage;
     });
@@ -520,6 +879,7 @@ extern "C" RustError zeknox_server_destroy(void *server)
             cudaStreamDestroy(st);
         }
         cudaEventDestroy(s->tables_ready);
+        zk::free_device_loop(s);
         cudaFree(s->arena);
         delete s;
     });

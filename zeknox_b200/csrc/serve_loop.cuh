@@ -1,0 +1,457 @@
+// serve_loop.cuh -- the device-resident request loop of the commit server.
+//
+// One cooperative, persistent kernel (every CTA resident at once) takes
+// requests from a ring in mapped host memory and runs each request's stages
+// itself, across the whole GPU: the fused LDE's passes (ntt_pass_body, every
+// tile of a pass handed out to the CTAs in turn), then the Merkle forest
+// (leaf hashes, node-parallel levels, the cooperative fold and tail).  A grid
+// barrier separates the stages.  The host admits requests against the arena
+// budget, plans their stages, copies the plan into device memory and posts
+// the ring entry; the kernel marks the entry done in host memory, and exits
+// after an idle period (the host relaunches it when the next entry arrives).
+//
+// Every wait is bounded by %globaltimer: the ring poll (idle_ns: then the
+// kernel exits), an entry's start gate (ready_ns: the entry fails with
+// LOOP_DONE_TIMEOUT and the loop goes on) and the grid barrier (barrier_ns:
+// the CTA that runs out raises `abort`, every CTA leaves, and the entry fails).
+//
+// Memory ordering: the host posts an entry with a release store after the
+// plan's copy has completed; the leader reads `head` with ld.acquire.sys and
+// every CTA acquires the barrier's generation at gpu scope before it reads the
+// plan or data, so weak loads after a barrier see the stores before it.  Data
+// that changes while the kernel runs (plans, leaves, digests, scratch) is
+// never read through the non-coherent load path; tables (twiddles, coset
+// powers) are built before a launch and never change under it.
+#pragma once
+#include <stdint.h>
+
+#include "bulk.cuh"
+#include "coop.cuh"
+#include "hash.cuh"
+#include "merkle.cuh"
+#include "ntt.cuh"
+
+namespace zk {
+
+constexpr uint32_t LOOP_RING = 16;        // ring entries (requests posted and not yet retired)
+constexpr uint32_t LOOP_MAX_STAGES = 160;  // stages of one request
+constexpr uint32_t LOOP_THREADS = 256;
+constexpr uint32_t LOOP_TAIL_MAXM = 1024;  // nodes a tail CTA takes (as merkle.cu)
+constexpr uint32_t LOOP_PASS_TILE = 4096;  // words of an NTT pass tile (as ntt.cu)
+constexpr uint32_t LOOP_SMEM_BYTES = (LOOP_TAIL_MAXM + LOOP_TAIL_MAXM / 2) * 32;  // tail buffers >= pass tile
+static_assert(LOOP_SMEM_BYTES >= LOOP_PASS_TILE * 8, "shared memory of a pass tile");
+
+enum LoopStageKind : uint32_t {
+    LS_PASS = 1,       // one NTT pass: a.grid tiles
+    LS_LEAF = 2,       // leaf digests, one leaf per thread
+    LS_LEAF_COOP = 3,  // leaf digests, one leaf per group of four threads
+    LS_LEVEL = 4,      // one tree level (height u), one node per thread
+    LS_FOLD_COOP = 5,  // 64 nodes of height u per CTA folded upwards in shared memory
+    LS_TAIL_COOP = 6,  // one subtree per CTA from height u to its cap
+};
+
+enum LoopDone : uint32_t { LOOP_DONE_NONE = 0, LOOP_DONE_OK = 1, LOOP_DONE_TIMEOUT = 2, LOOP_DONE_ABORT = 3 };
+
+struct LoopStage {
+    uint32_t kind, hash;                 // LoopStageKind; hash type of Merkle stages
+    uint32_t logr, load, store, u;       // LS_PASS kernel shape; Merkle height
+    uint64_t blocks;                     // CTA-sized work items
+    NttPassArgs a;                       // LS_PASS
+    const uint64_t *leaves;              // Merkle stages
+    uint64_t *digests, *caps;
+    MerkleGeom g;
+};
+static_assert(sizeof(LoopStage) % 8 == 0, "stages are copied as 8-byte words");
+
+// One ring entry (mapped host memory; the plan itself is in device memory).
+struct LoopSlot {
+    uint32_t ready;      // host: the entry may start (the test hook leaves it 0)
+    uint32_t done;       // device: LoopDone
+    uint32_t n_stages;
+    uint32_t pad;
+    uint64_t ready_ns;   // limit of the start-gate wait
+    const LoopStage *stages;  // device memory
+};
+
+struct LoopRing {  // mapped host memory
+    uint64_t head;       // host: entries posted
+    uint64_t tail;       // device: entries finished (done set)
+    uint32_t close;      // host: exit as soon as the ring is empty
+    uint32_t status;     // device: bit 0 an entry's gate ran out, bit 1 a barrier ran out
+    uint64_t idle_ns, barrier_ns;
+    LoopSlot slot[LOOP_RING];
+};
+
+struct LoopCtl {  // device memory, zeroed before each launch
+    unsigned arrive, gen, abort;
+    int cur;            // ring slot being run; -1 exit; -2 nothing to run
+    uint64_t taken;     // entries taken so far (the device's copy of tail)
+};
+
+__device__ __forceinline__ uint64_t ld_acquire_sys_u64(const uint64_t *p)
+{
+    uint64_t v;
+    asm volatile("ld.acquire.sys.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ uint32_t ld_acquire_sys_u32(const uint32_t *p)
+{
+    uint32_t v;
+    asm volatile("ld.acquire.sys.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_release_sys_u32(uint32_t *p, uint32_t v)
+{
+    asm volatile("st.release.sys.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+__device__ __forceinline__ void st_release_sys_u64(uint64_t *p, uint64_t v)
+{
+    asm volatile("st.release.sys.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+__device__ __forceinline__ unsigned ld_volatile_u32(const unsigned *p) { return *(const volatile unsigned *)p; }
+
+// Grid barrier of the cooperative launch, bounded by limit_ns; false when this
+// or another CTA gave up (every CTA then leaves the loop).
+__device__ __forceinline__ bool loop_grid_sync(LoopCtl *ctl, uint64_t limit_ns)
+{
+    __shared__ unsigned s_ok;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned ok = 1;
+        const unsigned gen = ld_volatile_u32(&ctl->gen);
+        __threadfence();
+        if (atomicAdd(&ctl->arrive, 1u) == gridDim.x - 1) {
+            atomicExch(&ctl->arrive, 0u);
+            __threadfence();
+            atomicAdd(&ctl->gen, 1u);
+        } else {
+            const uint64_t t0 = globaltimer_ns();
+            while (ld_volatile_u32(&ctl->gen) == gen) {
+                if (ld_volatile_u32(&ctl->abort)) {
+                    ok = 0;
+                    break;
+                }
+                if (globaltimer_ns() - t0 > limit_ns) {
+                    atomicExch(&ctl->abort, 1u);
+                    ok = 0;
+                    break;
+                }
+                __nanosleep(64);
+            }
+        }
+        __threadfence();
+        s_ok = ok && !ld_volatile_u32(&ctl->abort);
+    }
+    __syncthreads();
+    return s_ok != 0;
+}
+
+// ---------------------------------------------------------------- stages
+
+template <int LOGR, int LOADM, int STOREM>
+__device__ __forceinline__ void loop_pass(const NttPassArgs &a, uint64_t blocks, uint64_t *sm)
+{
+    for (uint64_t b = blockIdx.x; b < blocks; b += gridDim.x) {
+        ntt_pass_body<LOGR, 0, LOOP_THREADS, LOOP_PASS_TILE, LOADM, STOREM, 1>(a, (uint32_t)b, sm);
+        __syncthreads();
+    }
+}
+
+// The pass shapes a planned fused LDE of 2^9 .. 2^22-point columns uses with
+// the row-output radix 2^8 (the host rejects any other before posting).
+__device__ __forceinline__ void loop_run_pass(const LoopStage &st, const NttPassArgs &a, uint64_t *sm)
+{
+    if (st.load == LOAD_COSETS && st.store == STORE_SAME) {
+        switch (st.logr) {
+        case 1: loop_pass<1, LOAD_COSETS, STORE_SAME>(a, st.blocks, sm); break;
+        case 2: loop_pass<2, LOAD_COSETS, STORE_SAME>(a, st.blocks, sm); break;
+        case 3: loop_pass<3, LOAD_COSETS, STORE_SAME>(a, st.blocks, sm); break;
+        case 4: loop_pass<4, LOAD_COSETS, STORE_SAME>(a, st.blocks, sm); break;
+        case 5: loop_pass<5, LOAD_COSETS, STORE_SAME>(a, st.blocks, sm); break;
+        case 6: loop_pass<6, LOAD_COSETS, STORE_SAME>(a, st.blocks, sm); break;
+        case 7: loop_pass<7, LOAD_COSETS, STORE_SAME>(a, st.blocks, sm); break;
+        case 8: loop_pass<8, LOAD_COSETS, STORE_SAME>(a, st.blocks, sm); break;
+        case 9: loop_pass<9, LOAD_COSETS, STORE_SAME>(a, st.blocks, sm); break;
+        default: loop_pass<10, LOAD_COSETS, STORE_SAME>(a, st.blocks, sm); break;
+        }
+    } else if (st.store == STORE_SAME) {
+        switch (st.logr) {
+        case 5: loop_pass<5, LOAD_PLAIN, STORE_SAME>(a, st.blocks, sm); break;
+        case 6: loop_pass<6, LOAD_PLAIN, STORE_SAME>(a, st.blocks, sm); break;
+        default: loop_pass<7, LOAD_PLAIN, STORE_SAME>(a, st.blocks, sm); break;
+        }
+    } else {
+        loop_pass<8, LOAD_PLAIN, STORE_ROWS>(a, st.blocks, sm);
+    }
+}
+
+template <int H>
+__device__ __forceinline__ void loop_leaf(const LoopStage &st)
+{
+    const MerkleGeom &g = st.g;
+    for (uint64_t b = blockIdx.x; b < st.blocks; b += gridDim.x) {
+        const uint64_t i = b * LOOP_THREADS + threadIdx.x;
+        if (i >= g.n_leaves) continue;
+        uint64_t *dst = g.sub_leaves == 1 ? st.caps + 4 * i : st.digests + 4 * merkle_node_index(g, i, 0);
+        uint64_t d[4];
+        leaf_hash<H>(st.leaves + i * g.leaf_size, g.leaf_size, d);
+#pragma unroll
+        for (int q = 0; q < 4; q++) dst[q] = d[q];
+    }
+}
+
+template <int H>
+__device__ __forceinline__ void loop_leaf_coop(const LoopStage &st)
+{
+    const MerkleGeom &g = st.g;
+    CoopGroup c;
+    c.init();
+    for (uint64_t b = blockIdx.x; b < st.blocks; b += gridDim.x) {
+        const uint64_t gi = (b * LOOP_THREADS + threadIdx.x) >> 2;
+        if ((gi & ~7ULL) >= g.n_leaves) continue;  // the whole warp is past the end
+        const uint64_t i = gi < g.n_leaves ? gi : g.n_leaves - 1;
+        uint64_t d[4];
+        sponge_hash_one_coop<H>(st.leaves + i * g.leaf_size, g.leaf_size, d, c);
+        if (c.q == 0 && gi < g.n_leaves) {
+            uint64_t *dst = g.sub_leaves == 1 ? st.caps + 4 * gi : st.digests + 4 * merkle_node_index(g, gi, 0);
+#pragma unroll
+            for (int q = 0; q < 4; q++) dst[q] = d[q];
+        }
+    }
+}
+
+template <int H>
+__device__ __forceinline__ void loop_level(const LoopStage &st)
+{
+    const MerkleGeom &g = st.g;
+    const uint64_t per_sub = g.sub_leaves >> st.u, total = per_sub * g.n_caps;
+    for (uint64_t b = blockIdx.x; b < st.blocks; b += gridDim.x) {
+        const uint64_t x = b * LOOP_THREADS + threadIdx.x;
+        if (x >= total) continue;
+        const uint64_t k = x / per_sub, j = x % per_sub;
+        uint64_t *sub = st.digests + k * g.sub_digests * 4;
+        const uint64_t start = per_sub - 2, child = 2 * per_sub - 2;
+        uint64_t h[4];
+        hash_two<H>(sub + 4 * (child + 2 * j), sub + 4 * (child + 2 * j + 1), h);
+#pragma unroll
+        for (int q = 0; q < 4; q++) sub[4 * (start + j) + q] = h[q];
+    }
+}
+
+// 64 consecutive nodes of height u per work item, folded upwards inside the
+// CTA (the cooperative fold of merkle.cuh, with the caps of whole subtrees).
+template <int H>
+__device__ __forceinline__ void loop_fold_coop(const LoopStage &st, uint64_t (*node)[4])
+{
+    constexpr uint32_t NG = LOOP_THREADS / 4;
+    const MerkleGeom &g = st.g;
+    const uint32_t u0 = st.u;
+    CoopGroup c;
+    c.init();
+    const uint32_t grp = threadIdx.x >> 2;
+    const uint32_t wg = grp & ~7u;
+    const uint64_t count = g.n_leaves >> u0;
+    const uint32_t top = g.log_sub - 1;
+    uint32_t U = 0;
+    while ((1u << (U + 1)) <= NG && u0 + U + 1 <= top) U++;
+    for (uint64_t b = blockIdx.x; b < st.blocks; b += gridDim.x) {
+        const uint64_t i0 = b * NG;
+        const uint64_t cta_nodes = count - i0 < (uint64_t)NG ? count - i0 : (uint64_t)NG;
+        for (uint32_t t = threadIdx.x; t < 4 * cta_nodes; t += LOOP_THREADS)
+            node[t >> 2][t & 3] = st.digests[4 * merkle_node_index(g, (i0 + (t >> 2)) << u0, u0) + (t & 3)];
+        for (uint32_t v = 1; v <= U; v++) {
+            __syncthreads();
+            const uint32_t nodes = NG >> v;
+            const bool act = grp < nodes && ((uint64_t)grp << v) < cta_nodes;
+            const bool wact = wg < nodes && ((uint64_t)wg << v) < cta_nodes;
+            uint64_t h[4];
+            if (wact) {
+                const uint32_t src = act ? grp : wg;
+                sponge_hash_two_coop<H>(node[2 * src], node[2 * src + 1], h, c);
+                if (act && c.q == 0) {
+                    const uint64_t di = merkle_node_index(g, (i0 + ((uint64_t)grp << v)) << u0, u0 + v);
+#pragma unroll
+                    for (int q = 0; q < 4; q++) st.digests[4 * di + q] = h[q];
+                }
+            }
+            __syncthreads();
+            if (act && c.q == 0) {
+#pragma unroll
+                for (int q = 0; q < 4; q++) node[grp][q] = h[q];
+            }
+        }
+        const uint64_t sub_nodes = g.sub_leaves >> u0;
+        if (u0 + U == top && sub_nodes <= (uint64_t)NG) {
+            __syncthreads();
+            const uint32_t subs = (uint32_t)(cta_nodes / sub_nodes);
+            if (wg < subs) {
+                const bool act = grp < subs;
+                const uint32_t src = act ? grp : wg;
+                uint64_t h[4];
+                sponge_hash_two_coop<H>(node[2 * src], node[2 * src + 1], h, c);
+                if (act && c.q == 0) {
+                    const uint64_t k = ((i0 << u0) >> g.log_sub) + grp;
+#pragma unroll
+                    for (int q = 0; q < 4; q++) st.caps[4 * k + q] = h[q];
+                }
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// One subtree per work item, from height u to its cap (the cooperative tail
+// of merkle.cuh).
+template <int H>
+__device__ __forceinline__ void loop_tail_coop(const LoopStage &st, uint64_t (*bufa)[4], uint64_t (*bufb)[4])
+{
+    constexpr uint32_t NG = LOOP_THREADS / 4;
+    const MerkleGeom &g = st.g;
+    CoopGroup c;
+    c.init();
+    const uint32_t grp = threadIdx.x >> 2;
+    for (uint64_t k = blockIdx.x; k < st.blocks; k += gridDim.x) {
+        uint64_t *sub = st.digests + k * g.sub_digests * 4;
+        uint32_t m = (uint32_t)(g.sub_leaves >> st.u);
+        for (uint32_t j = threadIdx.x; j < 4 * m; j += LOOP_THREADS) bufa[j >> 2][j & 3] = sub[4 * (m - 2) + j];
+        uint64_t(*src)[4] = bufa;
+        uint64_t(*dst)[4] = bufb;
+        while (m > 2) {
+            __syncthreads();
+            const uint32_t half = m / 2;
+            for (uint32_t base = grp & ~7u; base < half; base += NG) {
+                const uint32_t j = base + (grp & 7u);
+                const bool act = j < half;
+                const uint32_t jj = act ? j : base;
+                uint64_t h[4];
+                sponge_hash_two_coop<H>(src[2 * jj], src[2 * jj + 1], h, c);
+                if (act && c.q == 0) {
+#pragma unroll
+                    for (int q = 0; q < 4; q++) {
+                        sub[4 * (half - 2 + j) + q] = h[q];
+                        dst[j][q] = h[q];
+                    }
+                }
+            }
+            uint64_t(*tmp)[4] = src;
+            src = dst;
+            dst = tmp;
+            m = half;
+        }
+        __syncthreads();
+        if (threadIdx.x < 32) {
+            uint64_t h[4];
+            sponge_hash_two_coop<H>(src[0], src[1], h, c);
+            if (threadIdx.x == 0) {
+#pragma unroll
+                for (int q = 0; q < 4; q++) st.caps[4 * k + q] = h[q];
+            }
+        }
+        __syncthreads();
+    }
+}
+
+template <int H>
+__device__ __forceinline__ void loop_run_merkle(const LoopStage &st, uint64_t *sm)
+{
+    switch (st.kind) {
+    case LS_LEAF: loop_leaf<H>(st); break;
+    case LS_LEAF_COOP: loop_leaf_coop<H>(st); break;
+    case LS_LEVEL: loop_level<H>(st); break;
+    case LS_FOLD_COOP: loop_fold_coop<H>(st, (uint64_t(*)[4])sm); break;
+    default:
+        loop_tail_coop<H>(st, (uint64_t(*)[4])sm, (uint64_t(*)[4])(sm + 4 * LOOP_TAIL_MAXM));
+        break;
+    }
+}
+
+// The loop.  Launched cooperatively with LOOP_THREADS threads and
+// LOOP_SMEM_BYTES of dynamic shared memory per CTA.
+__global__ void __launch_bounds__(LOOP_THREADS, 4) serve_loop_kernel(LoopRing *ring, LoopCtl *ctl)
+{
+    extern __shared__ __align__(16) uint64_t loop_sm[];
+    __shared__ LoopStage s_stage;
+    __shared__ int s_cur;
+    __shared__ uint32_t s_n;
+    __shared__ const LoopStage *s_plan;
+    const bool leader = blockIdx.x == 0 && threadIdx.x == 0;
+    const uint64_t barrier_ns = ring->barrier_ns;
+    for (;;) {
+        if (leader) {
+            int cur = -1;
+            const uint64_t taken = ctl->taken;
+            const uint64_t t0 = globaltimer_ns();
+            bool have = false;
+            for (;;) {
+                if (ld_acquire_sys_u64(&ring->head) > taken) {
+                    have = true;
+                    break;
+                }
+                if (ld_acquire_sys_u32(&ring->close) || globaltimer_ns() - t0 > ring->idle_ns) break;
+                __nanosleep(1000);
+            }
+            if (have) {
+                LoopSlot *sl = &ring->slot[taken % LOOP_RING];
+                const uint64_t t1 = globaltimer_ns();
+                bool ready = false;
+                for (;;) {
+                    if (ld_acquire_sys_u32(&sl->ready)) {
+                        ready = true;
+                        break;
+                    }
+                    if (globaltimer_ns() - t1 > sl->ready_ns) break;
+                    __nanosleep(1000);
+                }
+                if (ready) {
+                    cur = (int)(taken % LOOP_RING);
+                } else {
+                    // only the leader writes status: no atomics on host memory
+                    st_release_sys_u32(&ring->status, *(volatile uint32_t *)&ring->status | 1u);
+                    st_release_sys_u32(&sl->done, LOOP_DONE_TIMEOUT);
+                    ctl->taken = taken + 1;
+                    st_release_sys_u64(&ring->tail, taken + 1);
+                    cur = -2;
+                }
+            }
+            ctl->cur = cur;
+        }
+        if (!loop_grid_sync(ctl, barrier_ns)) break;
+        if (threadIdx.x == 0) {
+            s_cur = *(volatile int *)&ctl->cur;
+            if (s_cur >= 0) {
+                s_n = *(volatile uint32_t *)&ring->slot[s_cur].n_stages;
+                s_plan = *(const LoopStage *const volatile *)&ring->slot[s_cur].stages;
+            }
+        }
+        __syncthreads();
+        const int cur = s_cur;
+        if (cur == -1) break;
+        if (cur == -2) continue;
+        const uint32_t n = s_n < LOOP_MAX_STAGES ? s_n : LOOP_MAX_STAGES;
+        bool ok = true;
+        for (uint32_t s = 0; s < n && ok; s++) {
+            // the stage description into shared memory (volatile loads: the
+            // plan buffer is rewritten between requests)
+            for (uint32_t w = threadIdx.x; w < sizeof(LoopStage) / 8; w += LOOP_THREADS)
+                ((uint64_t *)&s_stage)[w] = ((const volatile uint64_t *)(s_plan + s))[w];
+            __syncthreads();
+            const LoopStage &st = s_stage;
+            if (st.kind == LS_PASS) loop_run_pass(st, st.a, loop_sm);
+            else if (st.hash == HASH_POSEIDON2) loop_run_merkle<HASH_POSEIDON2>(st, loop_sm);
+            else loop_run_merkle<HASH_POSEIDON>(st, loop_sm);
+            ok = loop_grid_sync(ctl, barrier_ns);
+        }
+        if (leader) {
+            LoopSlot *sl = &ring->slot[cur];
+            const uint64_t taken = ctl->taken + 1;
+            __threadfence_system();
+            if (!ok) st_release_sys_u32(&ring->status, *(volatile uint32_t *)&ring->status | 2u);
+            st_release_sys_u32(&sl->done, ok ? LOOP_DONE_OK : LOOP_DONE_ABORT);
+            ctl->taken = taken;
+            st_release_sys_u64(&ring->tail, taken);
+        }
+        if (!ok) break;
+    }
+}
+
+}  // namespace zk
