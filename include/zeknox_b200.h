@@ -196,6 +196,13 @@ RustError zeknox_server_cancel(void *server, uint64_t ticket);
  * fails with -cudaErrorLaunchTimeout and the loop goes on with the next. */
 #define ZK_SERVE_FAIL_GATE 4
 RustError zeknox_server_inject_failure(void *server, int stage);
+/* Device-loop servers: the per-stage trace of a finished request (until it is
+ * released).  *n = its number of stages; for the first `max` of them kinds[q]
+ * = the stage (16 + log2 radix: an LDE pass; 2 leaves; 3 leaves, four threads
+ * per leaf; 4 a tree level; 5 the cooperative fold; 6 the tail) and ns[q] =
+ * its time on the device, barrier to barrier (%globaltimer).  Either array may
+ * be NULL.  Requests of the host-driven mode have no trace (*n = 0). */
+RustError zeknox_server_trace(void *server, uint64_t ticket, uint32_t *kinds, uint64_t *ns, uint32_t max, uint32_t *n);
 /* Free the ticket's device results (returns their bytes to the budget). */
 RustError zeknox_server_release(void *server, uint64_t ticket);
 /* Bytes currently admitted against the budget, and the peak so far. */

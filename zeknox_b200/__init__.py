@@ -42,7 +42,7 @@ EXT_SYMBOLS = ["zeknox_last_error", "zeknox_commit", "zeknox_commit_batch", "zek
                "zeknox_lde_rows", "zeknox_launch_count", "zeknox_measure_mul_rate", "zeknox_merkle_batch",
                "zeknox_lde_rows_noalloc", "zeknox_server_create", "zeknox_server_create_ex", "zeknox_server_submit", "zeknox_server_wait",
                "zeknox_server_release", "zeknox_server_stats", "zeknox_server_destroy", "zeknox_server_prepare",
-               "zeknox_server_cancel", "zeknox_server_inject_failure", "zeknox_tune_set",
+               "zeknox_server_cancel", "zeknox_server_inject_failure", "zeknox_server_trace", "zeknox_tune_set",
                "zeknox_tune_get", "zeknox_tune_clear", "zeknox_tune_load", "zeknox_transpose_rev",
                "zeknox_lde_rows_scatter", "zeknox_field_selftest", "zeknox_permute", "zeknox_bounds_report",
                "zeknox_inject_wait_timeout"]
@@ -189,6 +189,8 @@ def load():
     L.zeknox_lde_rows_noalloc.argtypes = [sz, vp, vp, u32, u32, u32, u64, vp]
     L.zeknox_server_create.restype = RustError
     L.zeknox_server_create.argtypes = [sz, u64, u32, ctypes.POINTER(ctypes.c_void_p)]
+    L.zeknox_server_trace.restype = RustError
+    L.zeknox_server_trace.argtypes = [vp, u64, ctypes.POINTER(u32), ctypes.POINTER(u64), u32, ctypes.POINTER(u32)]
     L.zeknox_server_create_ex.restype = RustError
     L.zeknox_server_create_ex.argtypes = [sz, u64, u32, u32, ctypes.POINTER(ctypes.c_void_p)]
     L.zeknox_server_submit.restype = RustError
@@ -581,6 +583,16 @@ class Server:
     def inject_failure(self, stage):
         """Test hook: the next request started fails at `stage` (SERVE_FAIL_*)."""
         _check(load().zeknox_server_inject_failure(self._h, stage))
+
+    def trace(self, ticket):
+        """zeknox_server_trace: [(stage kind, device ns)] of a finished
+        device-loop request (16 + log2 radix: LDE pass; 2/3 leaves; 4 level;
+        5 fold; 6 tail)."""
+        n = ctypes.c_uint32()
+        _check(load().zeknox_server_trace(self._h, ticket, None, None, 0, ctypes.byref(n)))
+        kinds, ns = (ctypes.c_uint32 * max(n.value, 1))(), (ctypes.c_uint64 * max(n.value, 1))()
+        _check(load().zeknox_server_trace(self._h, ticket, kinds, ns, n.value, ctypes.byref(n)))
+        return [(int(kinds[q]), int(ns[q])) for q in range(n.value)]
 
     def stats(self):
         a, b, c = ctypes.c_uint64(), ctypes.c_uint64(), ctypes.c_uint64()

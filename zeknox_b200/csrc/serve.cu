@@ -106,6 +106,9 @@ struct Ticket {
     uint64_t off = NO_RANGE;   // its range in the arena while admitted
     uint64_t *leaves = nullptr, *digests = nullptr, *caps = nullptr, *scratch = nullptr;
     cudaEvent_t done_ev = nullptr;
+    // device-loop mode: each stage's kind and its duration on the device
+    std::vector<uint32_t> trace_kind;
+    std::vector<uint64_t> trace_ns;
 };
 
 struct Server {
@@ -417,6 +420,18 @@ struct Server {
             Ticket &t = tickets[ring_ticket[k]];
             int status = 2;
             if (d == LOOP_DONE_OK) {
+                // per-stage trace: the stage kinds from the plan, the times
+                // from the loop's stamps
+                const LoopStage *plan = plans_host + (uint64_t)k * LOOP_MAX_STAGES;
+                const uint32_t n = sl.n_stages < LOOP_MAX_STAGES ? sl.n_stages : LOOP_MAX_STAGES;
+                t.trace_kind.resize(n);
+                t.trace_ns.resize(n);
+                uint64_t prev = sl.t_start;
+                for (uint32_t q = 0; q < n; q++) {
+                    t.trace_kind[q] = plan[q].kind == LS_PASS ? 16 + plan[q].logr : plan[q].kind;
+                    t.trace_ns[q] = sl.t_stage[q] - prev;
+                    prev = sl.t_stage[q];
+                }
                 if (t.req.caps_host) {
                     const uint64_t n_caps = 1ULL << t.req.cap_height;
                     cudaError_t e = cudaMemcpyAsync(t.req.caps_host, t.caps, n_caps * 32, cudaMemcpyDeviceToHost,
@@ -631,6 +646,7 @@ void create_device_loop(Server *s, uint32_t slots)
     ZK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, serve_loop_kernel, LOOP_THREADS, LOOP_SMEM_BYTES));
     if (per_sm < 1) throw arg_failure("the device loop does not fit on an SM");
     s->loop_grid = per_sm * c.sm_count;
+    if (s->loop_grid > (int)LOOP_MAX_CTAS) s->loop_grid = (int)LOOP_MAX_CTAS / c.sm_count * c.sm_count;
     void *h = nullptr;
     ZK_CUDA(cudaHostAlloc(&h, sizeof(LoopRing), cudaHostAllocMapped | cudaHostAllocPortable));
     memset(h, 0, sizeof(LoopRing));
@@ -791,6 +807,25 @@ extern "C" RustError zeknox_server_release(void *server, uint64_t ticket)
         s->unadmit(t);  // its work has finished: the range is free at once
         s->tickets.erase(it);
         s->cv.notify_all();
+    });
+}
+
+extern "C" RustError zeknox_server_trace(void *server, uint64_t ticket, uint32_t *kinds, uint64_t *ns, uint32_t max,
+                                         uint32_t *n)
+{
+    return zk::guard([&] {
+        Server *s = zk::as_server(server);
+        if (!n) throw zk::arg_failure("null count");
+        std::lock_guard<std::mutex> lk(s->mu);
+        auto it = s->tickets.find(ticket);
+        if (it == s->tickets.end()) throw zk::arg_failure("unknown ticket");
+        const zk::Ticket &t = it->second;
+        const uint32_t m = (uint32_t)t.trace_ns.size();
+        for (uint32_t q = 0; q < m && q < max; q++) {
+            if (kinds) kinds[q] = t.trace_kind[q];
+            if (ns) ns[q] = t.trace_ns[q];
+        }
+        *n = m;
     });
 }
 

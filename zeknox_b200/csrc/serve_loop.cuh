@@ -71,6 +71,10 @@ struct LoopSlot {
     uint32_t pad;
     uint64_t ready_ns;   // limit of the start-gate wait
     const LoopStage *stages;  // device memory
+    // device: %globaltimer when the entry started and when each stage's
+    // barrier released (the per-stage trace zeknox_server_trace returns)
+    uint64_t t_start;
+    uint64_t t_stage[LOOP_MAX_STAGES];
 };
 
 struct LoopRing {  // mapped host memory
@@ -82,10 +86,16 @@ struct LoopRing {  // mapped host memory
     LoopSlot slot[LOOP_RING];
 };
 
+constexpr uint32_t LOOP_MAX_CTAS = 2048;
+
 struct LoopCtl {  // device memory, zeroed before each launch
     unsigned arrive, gen, abort;
     int cur;            // ring slot being run; -1 exit; -2 nothing to run
     uint64_t taken;     // entries taken so far (the device's copy of tail)
+    uint32_t n_stages;  // of the entry being run (copied by the leader)
+    uint32_t rank_bad;  // the CTAs are not spread evenly over SMs: ranks = block indices
+    const LoopStage *plan;
+    uint32_t cta_sm[LOOP_MAX_CTAS];  // %smid of every CTA
 };
 
 __device__ __forceinline__ uint64_t ld_acquire_sys_u64(const uint64_t *p)
@@ -125,8 +135,12 @@ __device__ __forceinline__ bool loop_grid_sync(LoopCtl *ctl, uint64_t limit_ns)
             __threadfence();
             atomicAdd(&ctl->gen, 1u);
         } else {
+            // poll the generation word sparingly (every waiting CTA polls the
+            // same L2 line); the abort flag and the clock every 64th poll
             const uint64_t t0 = globaltimer_ns();
-            while (ld_volatile_u32(&ctl->gen) == gen) {
+            for (uint32_t it = 1; ld_volatile_u32(&ctl->gen) == gen; it++) {
+                __nanosleep(512);
+                if (it % 64) continue;
                 if (ld_volatile_u32(&ctl->abort)) {
                     ok = 0;
                     break;
@@ -136,7 +150,6 @@ __device__ __forceinline__ bool loop_grid_sync(LoopCtl *ctl, uint64_t limit_ns)
                     ok = 0;
                     break;
                 }
-                __nanosleep(64);
             }
         }
         __threadfence();
@@ -148,10 +161,16 @@ __device__ __forceinline__ bool loop_grid_sync(LoopCtl *ctl, uint64_t limit_ns)
 
 // ---------------------------------------------------------------- stages
 
+// Stage bodies are separate (not inlined) functions, so each gets the
+// register allocation of its own code, as its standalone kernel does, instead
+// of one allocation over every stage of the loop.  A pass copies its
+// arguments out of shared memory first: shared stores to the tile could
+// otherwise alias them and force a reload at every use.
 template <int LOGR, int LOADM, int STOREM>
-__device__ __forceinline__ void loop_pass(const NttPassArgs &a, uint64_t blocks, uint64_t *sm)
+__device__ __noinline__ void loop_pass(const NttPassArgs *pa, uint64_t blocks, uint64_t *sm, uint32_t rank)
 {
-    for (uint64_t b = blockIdx.x; b < blocks; b += gridDim.x) {
+    const NttPassArgs a = *pa;
+    for (uint64_t b = rank; b < blocks; b += gridDim.x) {
         ntt_pass_body<LOGR, 0, LOOP_THREADS, LOOP_PASS_TILE, LOADM, STOREM, 1>(a, (uint32_t)b, sm);
         __syncthreads();
     }
@@ -159,37 +178,38 @@ __device__ __forceinline__ void loop_pass(const NttPassArgs &a, uint64_t blocks,
 
 // The pass shapes a planned fused LDE of 2^9 .. 2^22-point columns uses with
 // the row-output radix 2^8 (the host rejects any other before posting).
-__device__ __forceinline__ void loop_run_pass(const LoopStage &st, const NttPassArgs &a, uint64_t *sm)
+__device__ __forceinline__ void loop_run_pass(const LoopStage &st, const NttPassArgs *a, uint64_t *sm, uint32_t rank)
 {
     if (st.load == LOAD_COSETS && st.store == STORE_SAME) {
         switch (st.logr) {
-        case 1: loop_pass<1, LOAD_COSETS, STORE_SAME>(a, st.blocks, sm); break;
-        case 2: loop_pass<2, LOAD_COSETS, STORE_SAME>(a, st.blocks, sm); break;
-        case 3: loop_pass<3, LOAD_COSETS, STORE_SAME>(a, st.blocks, sm); break;
-        case 4: loop_pass<4, LOAD_COSETS, STORE_SAME>(a, st.blocks, sm); break;
-        case 5: loop_pass<5, LOAD_COSETS, STORE_SAME>(a, st.blocks, sm); break;
-        case 6: loop_pass<6, LOAD_COSETS, STORE_SAME>(a, st.blocks, sm); break;
-        case 7: loop_pass<7, LOAD_COSETS, STORE_SAME>(a, st.blocks, sm); break;
-        case 8: loop_pass<8, LOAD_COSETS, STORE_SAME>(a, st.blocks, sm); break;
-        case 9: loop_pass<9, LOAD_COSETS, STORE_SAME>(a, st.blocks, sm); break;
-        default: loop_pass<10, LOAD_COSETS, STORE_SAME>(a, st.blocks, sm); break;
+        case 1: loop_pass<1, LOAD_COSETS, STORE_SAME>(a, st.blocks, sm, rank); break;
+        case 2: loop_pass<2, LOAD_COSETS, STORE_SAME>(a, st.blocks, sm, rank); break;
+        case 3: loop_pass<3, LOAD_COSETS, STORE_SAME>(a, st.blocks, sm, rank); break;
+        case 4: loop_pass<4, LOAD_COSETS, STORE_SAME>(a, st.blocks, sm, rank); break;
+        case 5: loop_pass<5, LOAD_COSETS, STORE_SAME>(a, st.blocks, sm, rank); break;
+        case 6: loop_pass<6, LOAD_COSETS, STORE_SAME>(a, st.blocks, sm, rank); break;
+        case 7: loop_pass<7, LOAD_COSETS, STORE_SAME>(a, st.blocks, sm, rank); break;
+        case 8: loop_pass<8, LOAD_COSETS, STORE_SAME>(a, st.blocks, sm, rank); break;
+        case 9: loop_pass<9, LOAD_COSETS, STORE_SAME>(a, st.blocks, sm, rank); break;
+        default: loop_pass<10, LOAD_COSETS, STORE_SAME>(a, st.blocks, sm, rank); break;
         }
     } else if (st.store == STORE_SAME) {
         switch (st.logr) {
-        case 5: loop_pass<5, LOAD_PLAIN, STORE_SAME>(a, st.blocks, sm); break;
-        case 6: loop_pass<6, LOAD_PLAIN, STORE_SAME>(a, st.blocks, sm); break;
-        default: loop_pass<7, LOAD_PLAIN, STORE_SAME>(a, st.blocks, sm); break;
+        case 5: loop_pass<5, LOAD_PLAIN, STORE_SAME>(a, st.blocks, sm, rank); break;
+        case 6: loop_pass<6, LOAD_PLAIN, STORE_SAME>(a, st.blocks, sm, rank); break;
+        default: loop_pass<7, LOAD_PLAIN, STORE_SAME>(a, st.blocks, sm, rank); break;
         }
     } else {
-        loop_pass<8, LOAD_PLAIN, STORE_ROWS>(a, st.blocks, sm);
+        loop_pass<8, LOAD_PLAIN, STORE_ROWS>(a, st.blocks, sm, rank);
     }
 }
 
 template <int H>
-__device__ __forceinline__ void loop_leaf(const LoopStage &st)
+__device__ __noinline__ void loop_leaf(const LoopStage *pst, uint32_t rank)
 {
+    const LoopStage st = *pst;
     const MerkleGeom &g = st.g;
-    for (uint64_t b = blockIdx.x; b < st.blocks; b += gridDim.x) {
+    for (uint64_t b = rank; b < st.blocks; b += gridDim.x) {
         const uint64_t i = b * LOOP_THREADS + threadIdx.x;
         if (i >= g.n_leaves) continue;
         uint64_t *dst = g.sub_leaves == 1 ? st.caps + 4 * i : st.digests + 4 * merkle_node_index(g, i, 0);
@@ -201,12 +221,13 @@ __device__ __forceinline__ void loop_leaf(const LoopStage &st)
 }
 
 template <int H>
-__device__ __forceinline__ void loop_leaf_coop(const LoopStage &st)
+__device__ __noinline__ void loop_leaf_coop(const LoopStage *pst, uint32_t rank)
 {
+    const LoopStage st = *pst;
     const MerkleGeom &g = st.g;
     CoopGroup c;
     c.init();
-    for (uint64_t b = blockIdx.x; b < st.blocks; b += gridDim.x) {
+    for (uint64_t b = rank; b < st.blocks; b += gridDim.x) {
         const uint64_t gi = (b * LOOP_THREADS + threadIdx.x) >> 2;
         if ((gi & ~7ULL) >= g.n_leaves) continue;  // the whole warp is past the end
         const uint64_t i = gi < g.n_leaves ? gi : g.n_leaves - 1;
@@ -221,11 +242,12 @@ __device__ __forceinline__ void loop_leaf_coop(const LoopStage &st)
 }
 
 template <int H>
-__device__ __forceinline__ void loop_level(const LoopStage &st)
+__device__ __noinline__ void loop_level(const LoopStage *pst, uint32_t rank)
 {
+    const LoopStage st = *pst;
     const MerkleGeom &g = st.g;
     const uint64_t per_sub = g.sub_leaves >> st.u, total = per_sub * g.n_caps;
-    for (uint64_t b = blockIdx.x; b < st.blocks; b += gridDim.x) {
+    for (uint64_t b = rank; b < st.blocks; b += gridDim.x) {
         const uint64_t x = b * LOOP_THREADS + threadIdx.x;
         if (x >= total) continue;
         const uint64_t k = x / per_sub, j = x % per_sub;
@@ -241,8 +263,9 @@ __device__ __forceinline__ void loop_level(const LoopStage &st)
 // 64 consecutive nodes of height u per work item, folded upwards inside the
 // CTA (the cooperative fold of merkle.cuh, with the caps of whole subtrees).
 template <int H>
-__device__ __forceinline__ void loop_fold_coop(const LoopStage &st, uint64_t (*node)[4])
+__device__ __noinline__ void loop_fold_coop(const LoopStage *pst, uint64_t (*node)[4], uint32_t rank)
 {
+    const LoopStage st = *pst;
     constexpr uint32_t NG = LOOP_THREADS / 4;
     const MerkleGeom &g = st.g;
     const uint32_t u0 = st.u;
@@ -254,7 +277,7 @@ __device__ __forceinline__ void loop_fold_coop(const LoopStage &st, uint64_t (*n
     const uint32_t top = g.log_sub - 1;
     uint32_t U = 0;
     while ((1u << (U + 1)) <= NG && u0 + U + 1 <= top) U++;
-    for (uint64_t b = blockIdx.x; b < st.blocks; b += gridDim.x) {
+    for (uint64_t b = rank; b < st.blocks; b += gridDim.x) {
         const uint64_t i0 = b * NG;
         const uint64_t cta_nodes = count - i0 < (uint64_t)NG ? count - i0 : (uint64_t)NG;
         for (uint32_t t = threadIdx.x; t < 4 * cta_nodes; t += LOOP_THREADS)
@@ -303,14 +326,15 @@ __device__ __forceinline__ void loop_fold_coop(const LoopStage &st, uint64_t (*n
 // One subtree per work item, from height u to its cap (the cooperative tail
 // of merkle.cuh).
 template <int H>
-__device__ __forceinline__ void loop_tail_coop(const LoopStage &st, uint64_t (*bufa)[4], uint64_t (*bufb)[4])
+__device__ __noinline__ void loop_tail_coop(const LoopStage *pst, uint64_t (*bufa)[4], uint64_t (*bufb)[4], uint32_t rank)
 {
+    const LoopStage st = *pst;
     constexpr uint32_t NG = LOOP_THREADS / 4;
     const MerkleGeom &g = st.g;
     CoopGroup c;
     c.init();
     const uint32_t grp = threadIdx.x >> 2;
-    for (uint64_t k = blockIdx.x; k < st.blocks; k += gridDim.x) {
+    for (uint64_t k = rank; k < st.blocks; k += gridDim.x) {
         uint64_t *sub = st.digests + k * g.sub_digests * 4;
         uint32_t m = (uint32_t)(g.sub_leaves >> st.u);
         for (uint32_t j = threadIdx.x; j < 4 * m; j += LOOP_THREADS) bufa[j >> 2][j & 3] = sub[4 * (m - 2) + j];
@@ -352,22 +376,67 @@ __device__ __forceinline__ void loop_tail_coop(const LoopStage &st, uint64_t (*b
 }
 
 template <int H>
-__device__ __forceinline__ void loop_run_merkle(const LoopStage &st, uint64_t *sm)
+__device__ __forceinline__ void loop_run_merkle(const LoopStage &st, uint64_t *sm, uint32_t rank)
 {
     switch (st.kind) {
-    case LS_LEAF: loop_leaf<H>(st); break;
-    case LS_LEAF_COOP: loop_leaf_coop<H>(st); break;
-    case LS_LEVEL: loop_level<H>(st); break;
-    case LS_FOLD_COOP: loop_fold_coop<H>(st, (uint64_t(*)[4])sm); break;
+    case LS_LEAF: loop_leaf<H>(&st, rank); break;
+    case LS_LEAF_COOP: loop_leaf_coop<H>(&st, rank); break;
+    case LS_LEVEL: loop_level<H>(&st, rank); break;
+    case LS_FOLD_COOP: loop_fold_coop<H>(&st, (uint64_t(*)[4])sm, rank); break;
     default:
-        loop_tail_coop<H>(st, (uint64_t(*)[4])sm, (uint64_t(*)[4])(sm + 4 * LOOP_TAIL_MAXM));
+        loop_tail_coop<H>(&st, (uint64_t(*)[4])sm, (uint64_t(*)[4])(sm + 4 * LOOP_TAIL_MAXM), rank);
         break;
     }
 }
 
+// A CTA's rank: work item b of a stage goes to the CTA of rank b mod the
+// grid.  The cooperative grid places consecutive block indices on the same
+// SM, so a stage with fewer items than CTAs would crowd onto a few SMs;
+// ranked as (its place among the CTAs of its SM) x (SMs) + (its SM's place
+// among the SMs), the first items land on distinct SMs.  When the CTAs are not
+// spread evenly over SMs the ranks fall back to the block indices.
+__device__ uint32_t loop_rank(LoopCtl *ctl, uint64_t barrier_ns)
+{
+    __shared__ uint32_t s_sm_bits[8], s_slot, s_rank;
+    uint32_t smid;
+    asm volatile("mov.u32 %0, %%smid;" : "=r"(smid));
+    if (threadIdx.x < 8) s_sm_bits[threadIdx.x] = 0;
+    if (threadIdx.x == 0) {
+        s_slot = 0;
+        ctl->cta_sm[blockIdx.x] = smid;
+        if (smid >= 256 || gridDim.x > LOOP_MAX_CTAS) atomicExch(&ctl->rank_bad, 1u);
+    }
+    if (!loop_grid_sync(ctl, barrier_ns)) return blockIdx.x;
+    for (uint32_t j = threadIdx.x; j < gridDim.x; j += LOOP_THREADS) {
+        const uint32_t sm_j = *(volatile uint32_t *)&ctl->cta_sm[j];
+        if (sm_j < 256) atomicOr(&s_sm_bits[sm_j >> 5], 1u << (sm_j & 31));
+        if (j < blockIdx.x && sm_j == smid) atomicAdd(&s_slot, 1u);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint32_t n_sm = 0, below = 0;
+        for (int w = 0; w < 8; w++) {
+            n_sm += __popc(s_sm_bits[w]);
+            if (smid < 256) {
+                const uint32_t lim = smid >> 5;
+                if ((uint32_t)w < lim) below += __popc(s_sm_bits[w]);
+                else if ((uint32_t)w == lim) below += __popc(s_sm_bits[w] & ((1u << (smid & 31)) - 1));
+            }
+        }
+        const uint32_t per_sm = n_sm ? gridDim.x / n_sm : 0;
+        if (!n_sm || per_sm * n_sm != gridDim.x || s_slot >= per_sm) atomicExch(&ctl->rank_bad, 1u);
+        s_rank = s_slot * n_sm + below;
+    }
+    if (!loop_grid_sync(ctl, barrier_ns)) return blockIdx.x;
+    return ld_volatile_u32(&ctl->rank_bad) ? blockIdx.x : s_rank;
+}
+
 // The loop.  Launched cooperatively with LOOP_THREADS threads and
 // LOOP_SMEM_BYTES of dynamic shared memory per CTA.
-__global__ void __launch_bounds__(LOOP_THREADS, 4) serve_loop_kernel(LoopRing *ring, LoopCtl *ctl)
+#ifndef ZK_LOOP_MIN_CTAS
+#define ZK_LOOP_MIN_CTAS 4  // CTAs of the loop per SM (64 registers a thread)
+#endif
+__global__ void __launch_bounds__(LOOP_THREADS, ZK_LOOP_MIN_CTAS) serve_loop_kernel(LoopRing *ring, LoopCtl *ctl)
 {
     extern __shared__ __align__(16) uint64_t loop_sm[];
     __shared__ LoopStage s_stage;
@@ -376,6 +445,7 @@ __global__ void __launch_bounds__(LOOP_THREADS, 4) serve_loop_kernel(LoopRing *r
     __shared__ const LoopStage *s_plan;
     const bool leader = blockIdx.x == 0 && threadIdx.x == 0;
     const uint64_t barrier_ns = ring->barrier_ns;
+    const uint32_t rank = loop_rank(ctl, barrier_ns);
     for (;;) {
         if (leader) {
             int cur = -1;
@@ -404,6 +474,9 @@ __global__ void __launch_bounds__(LOOP_THREADS, 4) serve_loop_kernel(LoopRing *r
                 }
                 if (ready) {
                     cur = (int)(taken % LOOP_RING);
+                    // what every CTA needs of the entry, in device memory
+                    ctl->n_stages = *(volatile uint32_t *)&sl->n_stages;
+                    ctl->plan = *(const LoopStage *const volatile *)&sl->stages;
                 } else {
                     // only the leader writes status: no atomics on host memory
                     st_release_sys_u32(&ring->status, *(volatile uint32_t *)&ring->status | 1u);
@@ -419,8 +492,8 @@ __global__ void __launch_bounds__(LOOP_THREADS, 4) serve_loop_kernel(LoopRing *r
         if (threadIdx.x == 0) {
             s_cur = *(volatile int *)&ctl->cur;
             if (s_cur >= 0) {
-                s_n = *(volatile uint32_t *)&ring->slot[s_cur].n_stages;
-                s_plan = *(const LoopStage *const volatile *)&ring->slot[s_cur].stages;
+                s_n = *(volatile uint32_t *)&ctl->n_stages;
+                s_plan = *(const LoopStage *const volatile *)&ctl->plan;
             }
         }
         __syncthreads();
@@ -428,6 +501,7 @@ __global__ void __launch_bounds__(LOOP_THREADS, 4) serve_loop_kernel(LoopRing *r
         if (cur == -1) break;
         if (cur == -2) continue;
         const uint32_t n = s_n < LOOP_MAX_STAGES ? s_n : LOOP_MAX_STAGES;
+        if (leader) *(volatile uint64_t *)&ring->slot[cur].t_start = globaltimer_ns();
         bool ok = true;
         for (uint32_t s = 0; s < n && ok; s++) {
             // the stage description into shared memory (volatile loads: the
@@ -436,10 +510,11 @@ __global__ void __launch_bounds__(LOOP_THREADS, 4) serve_loop_kernel(LoopRing *r
                 ((uint64_t *)&s_stage)[w] = ((const volatile uint64_t *)(s_plan + s))[w];
             __syncthreads();
             const LoopStage &st = s_stage;
-            if (st.kind == LS_PASS) loop_run_pass(st, st.a, loop_sm);
-            else if (st.hash == HASH_POSEIDON2) loop_run_merkle<HASH_POSEIDON2>(st, loop_sm);
-            else loop_run_merkle<HASH_POSEIDON>(st, loop_sm);
+            if (st.kind == LS_PASS) loop_run_pass(st, &st.a, loop_sm, rank);
+            else if (st.hash == HASH_POSEIDON2) loop_run_merkle<HASH_POSEIDON2>(st, loop_sm, rank);
+            else loop_run_merkle<HASH_POSEIDON>(st, loop_sm, rank);
             ok = loop_grid_sync(ctl, barrier_ns);
+            if (leader) *(volatile uint64_t *)&ring->slot[cur].t_stage[s] = globaltimer_ns();
         }
         if (leader) {
             LoopSlot *sl = &ring->slot[cur];
