@@ -744,8 +744,9 @@ def measure_serve(requests, serial_sample=24):
                    "mean_queue_ms": float(np.mean(queue_d)), "delivered_elems_per_s": sum(elems) / span_d,
                    "delivered_over_offered": arrivals / span_d, "saturated_elems_per_s": saturated_d,
                    "saturated_over_serial": saturated_d / capacity,
-                   "form": "one persistent cooperative kernel runs every admitted request's stages, "
-                           "one request at a time; host admits and posts plans to a ring in mapped memory"}
+                   "form": "one persistent cooperative kernel runs the admitted requests' stages, the active "
+                           "request with the least work left first at every stage boundary; the host admits and "
+                           "posts plans to a ring in mapped memory"}
     del reqs, pool
     torch.cuda.empty_cache()
     return {"p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),

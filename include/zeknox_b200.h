@@ -153,11 +153,14 @@ RustError zeknox_server_create(size_t device_id, uint64_t budget_bytes, uint32_t
  * request loop runs the admitted requests.  Admission is the same (arrival
  * order, the budget, at most min(slots, 16) requests in flight).  The server
  * thread plans each request's stages, copies the plan to device memory and
- * posts it to a ring in mapped host memory. One persistent cooperative
- * kernel then takes the ring's entries and runs every stage itself, one
- * request at a time across the whole GPU, with grid barriers between the
- * stages: the fused LDE's passes, then the forest's leaf, level, fold and tail
- * steps. The kernel marks each entry done in host memory, and exits after
+ * posts it to a ring in mapped host memory.  Stages estimated above 4 ms are
+ * split into pieces (at most 64).  One persistent cooperative kernel takes
+ * the ring's entries and runs their stages itself, each stage across the
+ * whole GPU, with grid barriers between the stages: the fused LDE's passes,
+ * then the forest's leaf, level, fold and tail steps.  At every stage
+ * boundary it runs the next stage of the active request with the least
+ * estimated work left, so a small request is not held up by all of a large
+ * one.  The kernel marks each entry done in host memory, and exits after
  * 20 ms without requests (the next post relaunches it).  Every wait of the
  * kernel is bounded in time.  A request whose wait runs out fails with
  * -cudaErrorLaunchTimeout.  Requests in this mode: coefficients

@@ -28,6 +28,7 @@
 #include <cuda_runtime.h>
 #include <string.h>
 
+#include <algorithm>
 #include <chrono>
 #include <condition_variable>
 #include <deque>
@@ -141,7 +142,8 @@ struct Server {
     bool loop_live = false;
     int loop_grid = 0;
     uint64_t posted = 0, retired = 0;               // ring entries posted / retired by this host
-    uint64_t ring_ticket[LOOP_RING] = {};
+    uint64_t ring_ticket[LOOP_RING] = {};           // ticket of each slot (0: free)
+    uint64_t ring_seq[LOOP_RING] = {};              // entry number posted in each slot
     uint32_t loop_depth = 1;                        // entries in flight at most
 
     // Arena bytes of a job: leaves, digests, caps and LDE scratch, each
@@ -255,10 +257,11 @@ struct Server {
     void loop_ensure()
     {
         if (loop_running()) return;
-        const uint64_t tail = __atomic_load_n(&ring->tail, __ATOMIC_ACQUIRE);
-        if (tail >= posted) return;
+        const uint64_t taken = __atomic_load_n(&ring->taken, __ATOMIC_ACQUIRE);
+        if (taken >= posted) return;
         LoopCtl init{};
-        init.taken = tail;
+        init.taken = taken;
+        init.finished = __atomic_load_n(&ring->tail, __ATOMIC_ACQUIRE);
         ZK_CUDA(cudaMemcpyAsync(ctl, &init, sizeof init, cudaMemcpyHostToDevice, loop_stream));
         void *args[] = {(void *)&ring_dev, (void *)&ctl};
         ZK_CUDA(cudaLaunchCooperativeKernel((const void *)serve_loop_kernel, dim3(loop_grid), dim3(LOOP_THREADS), args,
@@ -283,8 +286,36 @@ struct Server {
     // Poseidon2 (cooperative leaves up to coop_leaves, node-parallel wide
     // levels, the cooperative fold, levels beyond the tail's capacity, the
     // cooperative tail); every stage gives the same digests as its kernel.
+    // Device time estimates of the scheduler (only their ratios matter): one
+    // width-12 permutation and one LDE element of the whole GPU's throughput.
+    static constexpr double PERM_NS = 1.27, LDE_ELEM_NS = 0.016;
+    static constexpr uint64_t PIECE_NS = 4000000;  // stages longer than this are split
+    static constexpr uint64_t MAX_PIECES = 64;     // into at most this many pieces
+
+    // Append a stage, split into pieces of whole multiples of the loop's grid
+    // when it is estimated above PIECE_NS, so the scheduler can switch entries
+    // between the pieces.
+    static void push_split(std::vector<LoopStage> &out, LoopStage st, double ns_per_block, uint64_t grid)
+    {
+        const uint64_t total = st.blocks;
+        st.cost_ns = (uint64_t)(ns_per_block * (double)total);
+        uint64_t piece = total;
+        if (st.cost_ns > PIECE_NS && grid) {
+            const double piece_ns = std::max((double)PIECE_NS, (double)st.cost_ns / MAX_PIECES);
+            piece = (uint64_t)(piece_ns / ns_per_block + grid - 1) / grid * grid;
+            if (piece < grid) piece = grid;
+        }
+        for (uint64_t f = 0; f < total; f += piece) {
+            LoopStage p = st;
+            p.first = f;
+            p.blocks = total - f < piece ? total - f : piece;
+            p.cost_ns = (uint64_t)(ns_per_block * (double)p.blocks);
+            out.push_back(p);
+        }
+    }
+
     static void merkle_stages(std::vector<LoopStage> &out, uint64_t *digests, uint64_t *caps, const uint64_t *leaves,
-                              uint64_t n_leaves, uint64_t leaf_size, uint32_t cap_height, uint32_t hash)
+                              uint64_t n_leaves, uint64_t leaf_size, uint32_t cap_height, uint32_t hash, uint64_t grid)
     {
         MerkleGeom g{};
         g.n_leaves = n_leaves;
@@ -293,6 +324,7 @@ struct Server {
         g.sub_leaves = n_leaves >> cap_height;
         g.sub_digests = 2 * g.sub_leaves - 2;
         g.log_sub = ilog2_exact(g.sub_leaves);
+        const double leaf_perms = leaf_size > 4 ? (double)((leaf_size + 7) / 8) : 0.0;
         auto stage = [&](uint32_t kind, uint32_t u, uint64_t blocks) {
             LoopStage st{};
             st.kind = kind;
@@ -303,7 +335,18 @@ struct Server {
             st.digests = digests;
             st.caps = caps;
             st.g = g;
-            out.push_back(st);
+            // permutations per work item: a leaf CTA hashes 256 leaves (64 in
+            // the cooperative form), a level CTA 256 nodes, a fold CTA 64 nodes
+            // and the levels above them, a tail CTA one subtree
+            double per = 0;
+            switch (kind) {
+            case LS_LEAF: per = LOOP_THREADS * leaf_perms; break;
+            case LS_LEAF_COOP: per = LOOP_THREADS / 4 * leaf_perms; break;
+            case LS_LEVEL: per = LOOP_THREADS; break;
+            case LS_FOLD_COOP: per = 2.0 * LOOP_THREADS / 4; break;
+            default: per = 2.0 * (double)(g.sub_leaves >> u); break;
+            }
+            push_split(out, st, per * PERM_NS, grid);
         };
         const uint32_t lg_leaves = ilog2_exact(n_leaves);
         const std::string h = std::to_string(hash);
@@ -367,13 +410,15 @@ struct Server {
                 st.store = (uint32_t)pp.store;
                 st.blocks = pp.grid;
                 st.a = pp.a;
-                plan.push_back(st);
+                push_split(plan, st, LOOP_PASS_TILE * LDE_ELEM_NS, (uint64_t)loop_grid);
             }
-            merkle_stages(plan, t.digests, t.caps, t.leaves, N, r.cols, r.cap_height, r.hash_type);
+            merkle_stages(plan, t.digests, t.caps, t.leaves, N, r.cols, r.cap_height, r.hash_type, (uint64_t)loop_grid);
             if (plan.size() > LOOP_MAX_STAGES) throw arg_failure("request needs more stages than a ring entry holds");
             if (inject == ZK_SERVE_FAIL_LAUNCH)
                 throw cuda_failure(-(int)cudaErrorLaunchFailure, "kernel launch refused (injected)");
-            const uint32_t k = (uint32_t)(posted % LOOP_RING);
+            uint32_t k = 0;
+            while (k < LOOP_RING && ring_ticket[k]) k++;
+            if (k == LOOP_RING) throw arg_failure("no free ring entry");  // admission keeps one free
             LoopStage *host = plans_host + (uint64_t)k * LOOP_MAX_STAGES;
             LoopStage *dev = plans + (uint64_t)k * LOOP_MAX_STAGES;
             memcpy(host, plan.data(), plan.size() * sizeof(LoopStage));
@@ -387,6 +432,8 @@ struct Server {
             __atomic_store_n(&sl.done, (uint32_t)LOOP_DONE_NONE, __ATOMIC_RELAXED);
             __atomic_store_n(&sl.ready, gate_shut ? 0u : 1u, __ATOMIC_RELEASE);
             ring_ticket[k] = id;
+            ring_seq[k] = posted;
+            __atomic_store_n(&ring->order[posted % LOOP_RING], k, __ATOMIC_RELAXED);
             posted++;
             __atomic_store_n(&ring->head, posted, __ATOMIC_RELEASE);
             loop_ensure();
@@ -399,38 +446,32 @@ struct Server {
         }
     }
 
-    // Retire ring entries in order (caller holds mu); true if any finished.
+    // Retire finished ring entries, in any order (caller holds mu); true if
+    // any finished.  Relaunches the loop when entries wait and it has exited.
     bool loop_retire()
     {
         bool progressed = false;
-        while (retired < posted) {
-            const uint32_t k = (uint32_t)(retired % LOOP_RING);
+        bool pending = false;
+        for (uint32_t k = 0; k < LOOP_RING; k++) {
+            if (!ring_ticket[k]) continue;
             LoopSlot &sl = ring->slot[k];
             const uint32_t d = __atomic_load_n(&sl.done, __ATOMIC_ACQUIRE);
             if (d == LOOP_DONE_NONE) {
-                // not done: relaunch the loop if it exited before taking it
-                std::lock_guard<std::recursive_mutex> dl(ctx->mu);
-                try {
-                    loop_ensure();
-                } catch (const std::exception &) {
-                    (void)cudaGetLastError();
-                }
-                break;
+                pending = true;
+                continue;
             }
             Ticket &t = tickets[ring_ticket[k]];
             int status = 2;
             if (d == LOOP_DONE_OK) {
-                // per-stage trace: the stage kinds from the plan, the times
-                // from the loop's stamps
+                // per-stage trace: the stage kinds from the plan, the device
+                // times from the loop
                 const LoopStage *plan = plans_host + (uint64_t)k * LOOP_MAX_STAGES;
                 const uint32_t n = sl.n_stages < LOOP_MAX_STAGES ? sl.n_stages : LOOP_MAX_STAGES;
                 t.trace_kind.resize(n);
                 t.trace_ns.resize(n);
-                uint64_t prev = sl.t_start;
                 for (uint32_t q = 0; q < n; q++) {
                     t.trace_kind[q] = plan[q].kind == LS_PASS ? 16 + plan[q].logr : plan[q].kind;
-                    t.trace_ns[q] = sl.t_stage[q] - prev;
-                    prev = sl.t_stage[q];
+                    t.trace_ns[q] = sl.t_stage[q];
                 }
                 if (t.req.caps_host) {
                     const uint64_t n_caps = 1ULL << t.req.cap_height;
@@ -449,6 +490,23 @@ struct Server {
             retired++;
             completed++;
             progressed = true;
+        }
+        if (pending) {
+            std::lock_guard<std::recursive_mutex> dl(ctx->mu);
+            if (!loop_running()) {
+                // entries the exited loop had taken and not finished (a CTA
+                // gave up on a barrier after the leader passed it) fail
+                const uint64_t taken = __atomic_load_n(&ring->taken, __ATOMIC_ACQUIRE);
+                for (uint32_t k = 0; k < LOOP_RING; k++)
+                    if (ring_ticket[k] && ring_seq[k] < taken &&
+                        __atomic_load_n(&ring->slot[k].done, __ATOMIC_ACQUIRE) == LOOP_DONE_NONE)
+                        __atomic_store_n(&ring->slot[k].done, (uint32_t)LOOP_DONE_ABORT, __ATOMIC_RELEASE);
+                try {
+                    loop_ensure();
+                } catch (const std::exception &) {
+                    (void)cudaGetLastError();
+                }
+            }
         }
         return progressed;
     }

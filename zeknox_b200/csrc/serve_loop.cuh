@@ -1,14 +1,21 @@
 // serve_loop.cuh -- the device-resident request loop of the commit server.
 //
 // One cooperative, persistent kernel (every CTA resident at once) takes
-// requests from a ring in mapped host memory and runs each request's stages
-// itself, across the whole GPU: the fused LDE's passes (ntt_pass_body, every
-// tile of a pass handed out to the CTAs in turn), then the Merkle forest
-// (leaf hashes, node-parallel levels, the cooperative fold and tail).  A grid
+// requests from a ring in mapped host memory and runs their stages itself,
+// across the whole GPU: the fused LDE's passes (ntt_pass_body, every tile of
+// a pass handed out to the CTAs in turn), then the Merkle forest (leaf
+// hashes, node-parallel levels, the cooperative fold and tail).  A grid
 // barrier separates the stages.  The host admits requests against the arena
-// budget, plans their stages, copies the plan into device memory and posts
-// the ring entry; the kernel marks the entry done in host memory, and exits
-// after an idle period (the host relaunches it when the next entry arrives).
+// budget, plans their stages (long ones split into pieces of a few
+// milliseconds), copies the plan into device memory and posts the entry.
+//
+// Scheduling: up to LOOP_RING entries are active at once; before every stage
+// the leader picks the active entry with the least estimated work left and
+// runs its next stage (shortest remaining work first, preemptive at stage
+// boundaries), so a small request that arrives behind a large one is not
+// held up by all of it.  A finished entry is marked done in host memory; the
+// kernel exits after an idle period (the host relaunches it when the next
+// entry arrives).
 //
 // Every wait is bounded by %globaltimer: the ring poll (idle_ns: then the
 // kernel exits), an entry's start gate (ready_ns: the entry fails with
@@ -34,7 +41,7 @@
 namespace zk {
 
 constexpr uint32_t LOOP_RING = 16;        // ring entries (requests posted and not yet retired)
-constexpr uint32_t LOOP_MAX_STAGES = 160;  // stages of one request
+constexpr uint32_t LOOP_MAX_STAGES = 384;  // stages (pieces) of one request
 constexpr uint32_t LOOP_THREADS = 256;
 constexpr uint32_t LOOP_TAIL_MAXM = 1024;  // nodes a tail CTA takes (as merkle.cu)
 constexpr uint32_t LOOP_PASS_TILE = 4096;  // words of an NTT pass tile (as ntt.cu)
@@ -55,7 +62,9 @@ enum LoopDone : uint32_t { LOOP_DONE_NONE = 0, LOOP_DONE_OK = 1, LOOP_DONE_TIMEO
 struct LoopStage {
     uint32_t kind, hash;                 // LoopStageKind; hash type of Merkle stages
     uint32_t logr, load, store, u;       // LS_PASS kernel shape; Merkle height
-    uint64_t blocks;                     // CTA-sized work items
+    uint64_t blocks;                     // CTA-sized work items of this piece
+    uint64_t first;                      // index of its first work item
+    uint64_t cost_ns;                    // estimated device time (the scheduler's measure of work)
     NttPassArgs a;                       // LS_PASS
     const uint64_t *leaves;              // Merkle stages
     uint64_t *digests, *caps;
@@ -71,30 +80,39 @@ struct LoopSlot {
     uint32_t pad;
     uint64_t ready_ns;   // limit of the start-gate wait
     const LoopStage *stages;  // device memory
-    // device: %globaltimer when the entry started and when each stage's
-    // barrier released (the per-stage trace zeknox_server_trace returns)
-    uint64_t t_start;
+    // device: the device time of each stage, barrier to barrier (the
+    // per-stage trace zeknox_server_trace returns)
     uint64_t t_stage[LOOP_MAX_STAGES];
 };
 
 struct LoopRing {  // mapped host memory
     uint64_t head;       // host: entries posted
-    uint64_t tail;       // device: entries finished (done set)
-    uint32_t close;      // host: exit as soon as the ring is empty
+    uint64_t taken;      // device: entries taken (activated, or failed at the start gate)
+    uint64_t tail;       // device: entries finished (done set), in any order
+    uint32_t close;      // host: exit as soon as nothing is active or posted
     uint32_t status;     // device: bit 0 an entry's gate ran out, bit 1 a barrier ran out
     uint64_t idle_ns, barrier_ns;
+    uint32_t order[LOOP_RING];  // host: the slot of entry number e is order[e mod LOOP_RING]
     LoopSlot slot[LOOP_RING];
 };
 
 constexpr uint32_t LOOP_MAX_CTAS = 2048;
 
-struct LoopCtl {  // device memory, zeroed before each launch
-    unsigned arrive, gen, abort;
-    int cur;            // ring slot being run; -1 exit; -2 nothing to run
-    uint64_t taken;     // entries taken so far (the device's copy of tail)
-    uint32_t n_stages;  // of the entry being run (copied by the leader)
-    uint32_t rank_bad;  // the CTAs are not spread evenly over SMs: ranks = block indices
+struct LoopActive {  // an entry being run
+    uint32_t slot, cursor, n, pad;
     const LoopStage *plan;
+    uint64_t remaining_ns;
+};
+
+struct LoopCtl {  // device memory, zeroed (but for taken / finished) before each launch
+    unsigned arrive, gen, abort;
+    int cur;                 // slot whose stage runs next; -1 exit
+    uint32_t pick;           // its index in active[]
+    uint32_t rank_bad;       // the CTAs are not spread evenly over SMs: ranks = block indices
+    uint64_t taken, finished;
+    const LoopStage *stage;  // the stage that runs next
+    uint32_t n_active, pad;
+    LoopActive active[LOOP_RING];
     uint32_t cta_sm[LOOP_MAX_CTAS];  // %smid of every CTA
 };
 
@@ -167,11 +185,11 @@ __device__ __forceinline__ bool loop_grid_sync(LoopCtl *ctl, uint64_t limit_ns)
 // arguments out of shared memory first: shared stores to the tile could
 // otherwise alias them and force a reload at every use.
 template <int LOGR, int LOADM, int STOREM>
-__device__ __noinline__ void loop_pass(const NttPassArgs *pa, uint64_t blocks, uint64_t *sm, uint32_t rank)
+__device__ __noinline__ void loop_pass(const NttPassArgs *pa, uint64_t first, uint64_t blocks, uint64_t *sm, uint32_t rank)
 {
     const NttPassArgs a = *pa;
     for (uint64_t b = rank; b < blocks; b += gridDim.x) {
-        ntt_pass_body<LOGR, 0, LOOP_THREADS, LOOP_PASS_TILE, LOADM, STOREM, 1>(a, (uint32_t)b, sm);
+        ntt_pass_body<LOGR, 0, LOOP_THREADS, LOOP_PASS_TILE, LOADM, STOREM, 1>(a, (uint32_t)(first + b), sm);
         __syncthreads();
     }
 }
@@ -182,25 +200,25 @@ __device__ __forceinline__ void loop_run_pass(const LoopStage &st, const NttPass
 {
     if (st.load == LOAD_COSETS && st.store == STORE_SAME) {
         switch (st.logr) {
-        case 1: loop_pass<1, LOAD_COSETS, STORE_SAME>(a, st.blocks, sm, rank); break;
-        case 2: loop_pass<2, LOAD_COSETS, STORE_SAME>(a, st.blocks, sm, rank); break;
-        case 3: loop_pass<3, LOAD_COSETS, STORE_SAME>(a, st.blocks, sm, rank); break;
-        case 4: loop_pass<4, LOAD_COSETS, STORE_SAME>(a, st.blocks, sm, rank); break;
-        case 5: loop_pass<5, LOAD_COSETS, STORE_SAME>(a, st.blocks, sm, rank); break;
-        case 6: loop_pass<6, LOAD_COSETS, STORE_SAME>(a, st.blocks, sm, rank); break;
-        case 7: loop_pass<7, LOAD_COSETS, STORE_SAME>(a, st.blocks, sm, rank); break;
-        case 8: loop_pass<8, LOAD_COSETS, STORE_SAME>(a, st.blocks, sm, rank); break;
-        case 9: loop_pass<9, LOAD_COSETS, STORE_SAME>(a, st.blocks, sm, rank); break;
-        default: loop_pass<10, LOAD_COSETS, STORE_SAME>(a, st.blocks, sm, rank); break;
+        case 1: loop_pass<1, LOAD_COSETS, STORE_SAME>(a, st.first, st.blocks, sm, rank); break;
+        case 2: loop_pass<2, LOAD_COSETS, STORE_SAME>(a, st.first, st.blocks, sm, rank); break;
+        case 3: loop_pass<3, LOAD_COSETS, STORE_SAME>(a, st.first, st.blocks, sm, rank); break;
+        case 4: loop_pass<4, LOAD_COSETS, STORE_SAME>(a, st.first, st.blocks, sm, rank); break;
+        case 5: loop_pass<5, LOAD_COSETS, STORE_SAME>(a, st.first, st.blocks, sm, rank); break;
+        case 6: loop_pass<6, LOAD_COSETS, STORE_SAME>(a, st.first, st.blocks, sm, rank); break;
+        case 7: loop_pass<7, LOAD_COSETS, STORE_SAME>(a, st.first, st.blocks, sm, rank); break;
+        case 8: loop_pass<8, LOAD_COSETS, STORE_SAME>(a, st.first, st.blocks, sm, rank); break;
+        case 9: loop_pass<9, LOAD_COSETS, STORE_SAME>(a, st.first, st.blocks, sm, rank); break;
+        default: loop_pass<10, LOAD_COSETS, STORE_SAME>(a, st.first, st.blocks, sm, rank); break;
         }
     } else if (st.store == STORE_SAME) {
         switch (st.logr) {
-        case 5: loop_pass<5, LOAD_PLAIN, STORE_SAME>(a, st.blocks, sm, rank); break;
-        case 6: loop_pass<6, LOAD_PLAIN, STORE_SAME>(a, st.blocks, sm, rank); break;
-        default: loop_pass<7, LOAD_PLAIN, STORE_SAME>(a, st.blocks, sm, rank); break;
+        case 5: loop_pass<5, LOAD_PLAIN, STORE_SAME>(a, st.first, st.blocks, sm, rank); break;
+        case 6: loop_pass<6, LOAD_PLAIN, STORE_SAME>(a, st.first, st.blocks, sm, rank); break;
+        default: loop_pass<7, LOAD_PLAIN, STORE_SAME>(a, st.first, st.blocks, sm, rank); break;
         }
     } else {
-        loop_pass<8, LOAD_PLAIN, STORE_ROWS>(a, st.blocks, sm, rank);
+        loop_pass<8, LOAD_PLAIN, STORE_ROWS>(a, st.first, st.blocks, sm, rank);
     }
 }
 
@@ -210,7 +228,7 @@ __device__ __noinline__ void loop_leaf(const LoopStage *pst, uint32_t rank)
     const LoopStage st = *pst;
     const MerkleGeom &g = st.g;
     for (uint64_t b = rank; b < st.blocks; b += gridDim.x) {
-        const uint64_t i = b * LOOP_THREADS + threadIdx.x;
+        const uint64_t i = (st.first + b) * LOOP_THREADS + threadIdx.x;
         if (i >= g.n_leaves) continue;
         uint64_t *dst = g.sub_leaves == 1 ? st.caps + 4 * i : st.digests + 4 * merkle_node_index(g, i, 0);
         uint64_t d[4];
@@ -228,7 +246,7 @@ __device__ __noinline__ void loop_leaf_coop(const LoopStage *pst, uint32_t rank)
     CoopGroup c;
     c.init();
     for (uint64_t b = rank; b < st.blocks; b += gridDim.x) {
-        const uint64_t gi = (b * LOOP_THREADS + threadIdx.x) >> 2;
+        const uint64_t gi = ((st.first + b) * LOOP_THREADS + threadIdx.x) >> 2;
         if ((gi & ~7ULL) >= g.n_leaves) continue;  // the whole warp is past the end
         const uint64_t i = gi < g.n_leaves ? gi : g.n_leaves - 1;
         uint64_t d[4];
@@ -248,7 +266,7 @@ __device__ __noinline__ void loop_level(const LoopStage *pst, uint32_t rank)
     const MerkleGeom &g = st.g;
     const uint64_t per_sub = g.sub_leaves >> st.u, total = per_sub * g.n_caps;
     for (uint64_t b = rank; b < st.blocks; b += gridDim.x) {
-        const uint64_t x = b * LOOP_THREADS + threadIdx.x;
+        const uint64_t x = (st.first + b) * LOOP_THREADS + threadIdx.x;
         if (x >= total) continue;
         const uint64_t k = x / per_sub, j = x % per_sub;
         uint64_t *sub = st.digests + k * g.sub_digests * 4;
@@ -278,7 +296,7 @@ __device__ __noinline__ void loop_fold_coop(const LoopStage *pst, uint64_t (*nod
     uint32_t U = 0;
     while ((1u << (U + 1)) <= NG && u0 + U + 1 <= top) U++;
     for (uint64_t b = rank; b < st.blocks; b += gridDim.x) {
-        const uint64_t i0 = b * NG;
+        const uint64_t i0 = (st.first + b) * NG;
         const uint64_t cta_nodes = count - i0 < (uint64_t)NG ? count - i0 : (uint64_t)NG;
         for (uint32_t t = threadIdx.x; t < 4 * cta_nodes; t += LOOP_THREADS)
             node[t >> 2][t & 3] = st.digests[4 * merkle_node_index(g, (i0 + (t >> 2)) << u0, u0) + (t & 3)];
@@ -334,7 +352,8 @@ __device__ __noinline__ void loop_tail_coop(const LoopStage *pst, uint64_t (*buf
     CoopGroup c;
     c.init();
     const uint32_t grp = threadIdx.x >> 2;
-    for (uint64_t k = rank; k < st.blocks; k += gridDim.x) {
+    for (uint64_t kb = rank; kb < st.blocks; kb += gridDim.x) {
+        const uint64_t k = st.first + kb;
         uint64_t *sub = st.digests + k * g.sub_digests * 4;
         uint32_t m = (uint32_t)(g.sub_leaves >> st.u);
         for (uint32_t j = threadIdx.x; j < 4 * m; j += LOOP_THREADS) bufa[j >> 2][j & 3] = sub[4 * (m - 2) + j];
@@ -441,89 +460,104 @@ __global__ void __launch_bounds__(LOOP_THREADS, ZK_LOOP_MIN_CTAS) serve_loop_ker
     extern __shared__ __align__(16) uint64_t loop_sm[];
     __shared__ LoopStage s_stage;
     __shared__ int s_cur;
-    __shared__ uint32_t s_n;
-    __shared__ const LoopStage *s_plan;
+    __shared__ const LoopStage *s_next;
     const bool leader = blockIdx.x == 0 && threadIdx.x == 0;
     const uint64_t barrier_ns = ring->barrier_ns;
     const uint32_t rank = loop_rank(ctl, barrier_ns);
     for (;;) {
         if (leader) {
-            int cur = -1;
-            const uint64_t taken = ctl->taken;
+            // take posted entries (waiting, bounded, only when nothing is active)
             const uint64_t t0 = globaltimer_ns();
-            bool have = false;
             for (;;) {
-                if (ld_acquire_sys_u64(&ring->head) > taken) {
-                    have = true;
-                    break;
+                const uint64_t head = ld_acquire_sys_u64(&ring->head);
+                while (ctl->taken < head && ctl->n_active < LOOP_RING) {
+                    const uint32_t k = *(volatile uint32_t *)&ring->order[ctl->taken % LOOP_RING] % LOOP_RING;
+                    LoopSlot *sl = &ring->slot[k];
+                    const uint64_t t1 = globaltimer_ns();
+                    bool ready = false;
+                    for (;;) {
+                        if (ld_acquire_sys_u32(&sl->ready)) {
+                            ready = true;
+                            break;
+                        }
+                        if (globaltimer_ns() - t1 > sl->ready_ns) break;
+                        __nanosleep(1000);
+                    }
+                    if (ready) {
+                        LoopActive &e = ctl->active[ctl->n_active++];
+                        e.slot = k;
+                        e.cursor = 0;
+                        const uint32_t n = *(volatile uint32_t *)&sl->n_stages;
+                        e.n = n < LOOP_MAX_STAGES ? n : LOOP_MAX_STAGES;
+                        e.plan = *(const LoopStage *const volatile *)&sl->stages;
+                        uint64_t rem = 0;
+                        for (uint32_t q = 0; q < e.n; q++) rem += *(const volatile uint64_t *)&e.plan[q].cost_ns;
+                        e.remaining_ns = rem;
+                    } else {
+                        // only the leader writes status: no atomics on host memory
+                        st_release_sys_u32(&ring->status, *(volatile uint32_t *)&ring->status | 1u);
+                        st_release_sys_u32(&sl->done, LOOP_DONE_TIMEOUT);
+                        st_release_sys_u64(&ring->tail, ++ctl->finished);
+                    }
+                    st_release_sys_u64(&ring->taken, ++ctl->taken);
                 }
+                if (ctl->n_active) break;
                 if (ld_acquire_sys_u32(&ring->close) || globaltimer_ns() - t0 > ring->idle_ns) break;
                 __nanosleep(1000);
             }
-            if (have) {
-                LoopSlot *sl = &ring->slot[taken % LOOP_RING];
-                const uint64_t t1 = globaltimer_ns();
-                bool ready = false;
-                for (;;) {
-                    if (ld_acquire_sys_u32(&sl->ready)) {
-                        ready = true;
-                        break;
-                    }
-                    if (globaltimer_ns() - t1 > sl->ready_ns) break;
-                    __nanosleep(1000);
-                }
-                if (ready) {
-                    cur = (int)(taken % LOOP_RING);
-                    // what every CTA needs of the entry, in device memory
-                    ctl->n_stages = *(volatile uint32_t *)&sl->n_stages;
-                    ctl->plan = *(const LoopStage *const volatile *)&sl->stages;
-                } else {
-                    // only the leader writes status: no atomics on host memory
-                    st_release_sys_u32(&ring->status, *(volatile uint32_t *)&ring->status | 1u);
-                    st_release_sys_u32(&sl->done, LOOP_DONE_TIMEOUT);
-                    ctl->taken = taken + 1;
-                    st_release_sys_u64(&ring->tail, taken + 1);
-                    cur = -2;
-                }
+            // the active entry with the least estimated work left runs its next stage
+            int cur = -1;
+            if (ctl->n_active) {
+                uint32_t best = 0;
+                for (uint32_t q = 1; q < ctl->n_active; q++)
+                    if (ctl->active[q].remaining_ns < ctl->active[best].remaining_ns) best = q;
+                const LoopActive &e = ctl->active[best];
+                ctl->pick = best;
+                ctl->stage = e.plan + e.cursor;
+                cur = (int)e.slot;
             }
             ctl->cur = cur;
         }
         if (!loop_grid_sync(ctl, barrier_ns)) break;
         if (threadIdx.x == 0) {
             s_cur = *(volatile int *)&ctl->cur;
-            if (s_cur >= 0) {
-                s_n = *(volatile uint32_t *)&ctl->n_stages;
-                s_plan = *(const LoopStage *const volatile *)&ctl->plan;
-            }
+            s_next = *(const LoopStage *const volatile *)&ctl->stage;
         }
         __syncthreads();
-        const int cur = s_cur;
-        if (cur == -1) break;
-        if (cur == -2) continue;
-        const uint32_t n = s_n < LOOP_MAX_STAGES ? s_n : LOOP_MAX_STAGES;
-        if (leader) *(volatile uint64_t *)&ring->slot[cur].t_start = globaltimer_ns();
-        bool ok = true;
-        for (uint32_t s = 0; s < n && ok; s++) {
-            // the stage description into shared memory (volatile loads: the
-            // plan buffer is rewritten between requests)
-            for (uint32_t w = threadIdx.x; w < sizeof(LoopStage) / 8; w += LOOP_THREADS)
-                ((uint64_t *)&s_stage)[w] = ((const volatile uint64_t *)(s_plan + s))[w];
-            __syncthreads();
-            const LoopStage &st = s_stage;
-            if (st.kind == LS_PASS) loop_run_pass(st, &st.a, loop_sm, rank);
-            else if (st.hash == HASH_POSEIDON2) loop_run_merkle<HASH_POSEIDON2>(st, loop_sm, rank);
-            else loop_run_merkle<HASH_POSEIDON>(st, loop_sm, rank);
-            ok = loop_grid_sync(ctl, barrier_ns);
-            if (leader) *(volatile uint64_t *)&ring->slot[cur].t_stage[s] = globaltimer_ns();
-        }
+        if (s_cur < 0) break;
+        const uint64_t t_begin = leader ? globaltimer_ns() : 0;
+        // the stage description into shared memory (volatile loads: the plan
+        // buffers are rewritten between requests)
+        for (uint32_t w = threadIdx.x; w < sizeof(LoopStage) / 8; w += LOOP_THREADS)
+            ((uint64_t *)&s_stage)[w] = ((const volatile uint64_t *)s_next)[w];
+        __syncthreads();
+        const LoopStage &st = s_stage;
+        if (st.kind == LS_PASS) loop_run_pass(st, &st.a, loop_sm, rank);
+        else if (st.hash == HASH_POSEIDON2) loop_run_merkle<HASH_POSEIDON2>(st, loop_sm, rank);
+        else loop_run_merkle<HASH_POSEIDON>(st, loop_sm, rank);
+        const bool ok = loop_grid_sync(ctl, barrier_ns);
         if (leader) {
-            LoopSlot *sl = &ring->slot[cur];
-            const uint64_t taken = ctl->taken + 1;
-            __threadfence_system();
-            if (!ok) st_release_sys_u32(&ring->status, *(volatile uint32_t *)&ring->status | 2u);
-            st_release_sys_u32(&sl->done, ok ? LOOP_DONE_OK : LOOP_DONE_ABORT);
-            ctl->taken = taken;
-            st_release_sys_u64(&ring->tail, taken);
+            LoopActive &e = ctl->active[ctl->pick];
+            LoopSlot *sl = &ring->slot[e.slot];
+            *(volatile uint64_t *)&sl->t_stage[e.cursor] = globaltimer_ns() - t_begin;
+            e.remaining_ns = e.remaining_ns > st.cost_ns ? e.remaining_ns - st.cost_ns : 0;
+            e.cursor++;
+            if (!ok) {
+                // every active entry fails: the loop leaves
+                st_release_sys_u32(&ring->status, *(volatile uint32_t *)&ring->status | 2u);
+                __threadfence_system();
+                for (uint32_t q = 0; q < ctl->n_active; q++) {
+                    st_release_sys_u32(&ring->slot[ctl->active[q].slot].done, LOOP_DONE_ABORT);
+                    ++ctl->finished;
+                }
+                ctl->n_active = 0;
+                st_release_sys_u64(&ring->tail, ctl->finished);
+            } else if (e.cursor >= e.n) {
+                __threadfence_system();
+                st_release_sys_u32(&sl->done, LOOP_DONE_OK);
+                st_release_sys_u64(&ring->tail, ++ctl->finished);
+                ctl->active[ctl->pick] = ctl->active[--ctl->n_active];
+            }
         }
         if (!ok) break;
     }
