@@ -504,6 +504,7 @@ def measure_batch(steps, budget_gb):
     total_perms = sum(perms_of(1 << (j["lg_n"] + j["rate"]), j["cols"], j["cap"]) for j in jobs)
     t_batch, t_plain = 0.0, 0.0
     t_stages = {"lde": 0.0, "forest": 0.0}
+    all_caps = []
     for wave in waves:
         bufs, cjobs = [], []
         for jb in wave:
@@ -518,6 +519,7 @@ def measure_batch(steps, budget_gb):
         zk.commit_batch(0, cjobs)  # capture
         torch.cuda.synchronize()
         caps_b = [b[3].clone() for b in bufs]
+        all_caps.extend(cb.cpu() for cb in caps_b)
         a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         for _ in range(steps):
             a.record()
@@ -561,12 +563,41 @@ def measure_batch(steps, budget_gb):
                 t_stages[stage] += a.elapsed_time(b)
         del bufs, cjobs, caps_b, ev_all
         torch.cuda.empty_cache()
+    # the whole batch through the device-resident loop: every job submitted at
+    # once to a server whose persistent kernel runs them (one launch while the
+    # stream lasts); results released as they complete; wall clock, submit of
+    # the first job -> completion of the last
+    inputs = [dev_field((1 << jb["lg_n"]) * jb["cols"], jb["seed"]) for jb in jobs]
+    caps_loop = [torch.zeros((1 << jb["cap"]) * 4, dtype=torch.int64).pin_memory() for jb in jobs]
+    with zk.Server(0, 100 << 30, 16, device_loop=True) as srv:
+        for r in (1, 2, 3):
+            srv.prepare(10, 20, r)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        pending = {srv.submit(jb["lg_n"], jb["rate"], jb["cols"], jb["cap"], jb["hash"], inp, caps_host=ch): i
+                   for i, (jb, inp, ch) in enumerate(zip(jobs, inputs, caps_loop))}
+        while pending:
+            for t in list(pending):
+                res = srv.wait(t, timeout_ms=0.0)
+                if res.status == 2:
+                    srv.release(t)
+                    del pending[t]
+                elif res.status < 0:
+                    raise RuntimeError("device-loop job failed: %d" % res.status)
+            time.sleep(0.0002)
+        t_loop = (time.perf_counter() - t0) * 1e3
+    for cl, cb in zip(caps_loop, all_caps):
+        assert torch.equal(cl, cb), "device-loop and batched commitments differ"
+    del inputs, caps_loop
+    torch.cuda.empty_cache()
     rate = poseidon_perm_rate()
     floor_ms = total_perms / rate * 1e3
     return {"batched_elems_per_s": total_elems / (t_batch * 1e-3), "plain_elems_per_s": total_elems / (t_plain * 1e-3),
             "batched_over_plain": t_plain / t_batch, "batched_ms": t_batch, "plain_ms": t_plain,
             "poseidon_perms": total_perms, "poseidon_perms_per_s": rate, "perm_floor_ms": floor_ms,
             "batched_frac_of_perm_floor": floor_ms / t_batch, "plain_bound_over_floor": t_plain / floor_ms,
+            "device_loop_ms": t_loop, "device_loop_elems_per_s": total_elems / (t_loop * 1e-3),
+            "device_loop_over_plain": t_plain / t_loop,
             "stage_sum_ms": t_stages["lde"] + t_stages["forest"], "stage_lde_ms": t_stages["lde"],
             "stage_forest_ms": t_stages["forest"], "batched_over_stage_sum": t_batch / (t_stages["lde"] + t_stages["forest"]),
             "jobs": len(jobs), "waves": len(waves), "elements": total_elems, "steps": steps,

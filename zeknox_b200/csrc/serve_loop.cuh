@@ -43,10 +43,12 @@ namespace zk {
 constexpr uint32_t LOOP_RING = 16;        // ring entries (requests posted and not yet retired)
 constexpr uint32_t LOOP_MAX_STAGES = 384;  // stages (pieces) of one request
 constexpr uint32_t LOOP_THREADS = 256;
-constexpr uint32_t LOOP_TAIL_MAXM = 1024;  // nodes a tail CTA takes (as merkle.cu)
+constexpr uint32_t LOOP_TAIL_MAXM = 512;   // nodes a tail CTA takes (half of merkle.cu's: 24 KiB)
 constexpr uint32_t LOOP_PASS_TILE = 4096;  // words of an NTT pass tile (as ntt.cu)
-constexpr uint32_t LOOP_SMEM_BYTES = (LOOP_TAIL_MAXM + LOOP_TAIL_MAXM / 2) * 32;  // tail buffers >= pass tile
-static_assert(LOOP_SMEM_BYTES >= LOOP_PASS_TILE * 8, "shared memory of a pass tile");
+// shared memory of a CTA: the pass tile (32 KiB; measured 1.6% faster on a
+// 2^20 x 256 request than 48 KiB for 1024-node tails: passes 57.5 against 64.1 ms)
+constexpr uint32_t LOOP_SMEM_BYTES = LOOP_PASS_TILE * 8;
+static_assert(LOOP_SMEM_BYTES >= (LOOP_TAIL_MAXM + LOOP_TAIL_MAXM / 2) * 32, "tail buffers");
 
 enum LoopStageKind : uint32_t {
     LS_PASS = 1,       // one NTT pass: a.grid tiles
