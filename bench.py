@@ -792,6 +792,62 @@ def measure_serve(requests, serial_sample=24):
                         "8 slots, seed 5; latency = submit -> caps on host"}
 
 
+def run_loop_trace(args):
+    """Per-stage device time of the device-resident loop (zeknox_server_trace)
+    against the same work through the standalone calls (zeknox_lde_rows and
+    fill_digests_buf_linear_gpu_with_gpu_ptr, CUDA events), for single
+    Poseidon requests of 2^12 x 16, 2^16 x 128 and 2^20 x 256 (rate 3, cap 4)."""
+    import torch
+    import zeknox_b200 as zk
+    torch.cuda.set_device(0)
+    pool = dev_field(256 << 20, 77)
+    legacy = torch.cuda.default_stream()
+    names = {2: "leaf", 3: "leaf_coop", 4: "level", 5: "fold", 6: "tail"}
+    out = []
+    for lg, c in [(12, 16), (16, 128), (20, 256)]:
+        N = 1 << (lg + 3)
+        inp = pool[: c << lg]
+        leaves = torch.empty(N * c, dtype=torch.int64, device="cuda")
+        n_dig, n_cap = zk.merkle_sizes(N, 4)
+        dig = torch.empty(n_dig * 4, dtype=torch.int64, device="cuda")
+        caps = torch.empty(n_cap * 4, dtype=torch.int64, device="cuda")
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        t_lde, t_forest = [], []
+        for _ in range(4):
+            a.record(legacy)
+            zk.lde_rows(0, leaves, inp, lg, 3, c)
+            b.record(legacy)
+            torch.cuda.synchronize()
+            t_lde.append(a.elapsed_time(b))
+            a.record(legacy)
+            zk.fill_digests_buf_linear_gpu(dig, caps, leaves, N, c, 4, 0)
+            b.record(legacy)
+            torch.cuda.synchronize()
+            t_forest.append(a.elapsed_time(b))
+        del leaves, dig, caps
+        torch.cuda.empty_cache()
+        with zk.Server(0, 40 << 30, 8, device_loop=True) as srv:
+            srv.prepare(lg, lg, 3)
+            ch = torch.zeros(n_cap * 4, dtype=torch.int64).pin_memory()
+            for _ in range(3):
+                t = srv.submit(lg, 3, c, 4, 0, inp, caps_host=ch)
+                r = srv.wait(t)
+                assert r.status == 2, r.status
+                tr = srv.trace(t)
+                srv.release(t)
+        stages = {}
+        for kind, ns in tr:
+            key = "lde_pass_radix_2^%d" % (kind - 16) if kind >= 16 else names[kind]
+            stages[key] = stages.get(key, 0.0) + ns / 1e6
+        out.append({"request": [lg, 3, c, 4, 0], "loop_latency_ms": r.latency_ms, "loop_stages_ms": stages,
+                    "loop_lde_ms": sum(ns for k, ns in tr if k >= 16) / 1e6,
+                    "loop_forest_ms": sum(ns for k, ns in tr if k < 16) / 1e6,
+                    "standalone_lde_ms": statistics.median(t_lde[1:]),
+                    "standalone_forest_ms": statistics.median(t_forest[1:])})
+    print(json.dumps({"metric": "device loop per-stage device time against standalone calls", "unit": "ms",
+                      "requests": out}), flush=True)
+
+
 def run_serve(args):
     import torch
     torch.cuda.set_device(0)
@@ -818,7 +874,7 @@ def main():
     ap.add_argument("--batch-steps", type=int, default=1, help="uneven batch: timed passes per wave")
     ap.add_argument("--no-extras", action="store_true",
                     help="headline only: skip the uneven-batch and serving measurements of the default run")
-    ap.add_argument("--workload", default="commit", choices=["commit", "batch", "hashes", "serve"],
+    ap.add_argument("--workload", default="commit", choices=["commit", "batch", "hashes", "serve", "loop-trace"],
                     help="commit: the headline line; batch: uneven 64-job batch vs plain calls; hashes: 2^20 x 135 "
                          "forests with Poseidon2, Monolith and Keccak")
     ap.add_argument("--budget-gb", type=float, default=48.0, help="batch workload: device memory per wave")
@@ -835,6 +891,8 @@ def main():
         return run_hashes(args)
     if args.workload == "serve":
         return run_serve(args)
+    if args.workload == "loop-trace":
+        return run_loop_trace(args)
     if world > 1:
         import datetime
 
