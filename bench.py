@@ -550,15 +550,18 @@ def measure_batch(steps, budget_gb):
         # the batch's own stages one at a time: each job's fused LDE and its
         # forest, each call alone and waited for (what the graph would take
         # if nothing overlapped and nothing were left idle)
+        # (events on the legacy stream: the forest call queues there and
+        # returns at once; the LDE call waits for its blocking stream)
+        legacy = torch.cuda.default_stream()
         for jb, (inp, leaves, dig, caps, n_dig, n_cap) in zip(wave, bufs):
             N = 1 << (jb["lg_n"] + jb["rate"])
             for stage in ("lde", "forest"):
-                a.record()
+                a.record(legacy)
                 if stage == "lde":
                     zk.lde_rows(0, leaves, inp, jb["lg_n"], jb["rate"], jb["cols"])
                 else:
                     zk.fill_digests_buf_linear_gpu(dig, caps, leaves, N, jb["cols"], jb["cap"], jb["hash"])
-                b.record()
+                b.record(legacy)
                 torch.cuda.synchronize()
                 t_stages[stage] += a.elapsed_time(b)
         del bufs, cjobs, caps_b, ev_all
