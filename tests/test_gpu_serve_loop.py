@@ -19,7 +19,10 @@ pytestmark = pytest.mark.gpu
 # leaves) and by the tail, one cap, two and three passes per column chunk,
 # three column chunks (2^22 rows: 16 columns a chunk), ragged column counts
 SHAPES = [(9, 1, 16, 4, 0), (10, 3, 33, 0, 3), (12, 2, 64, 4, 0), (13, 3, 24, 4, 3), (11, 1, 100, 2, 0),
-          (19, 3, 40, 4, 0), (19, 1, 8, 3, 3), (9, 3, 7, 4, 3), (14, 2, 17, 1, 0)]
+          (19, 3, 40, 4, 0), (19, 1, 8, 3, 3), (9, 3, 7, 4, 3), (14, 2, 17, 1, 0),
+          # the hashes without a cooperative form: one permutation per thread
+          # in the fold and tail (Keccak 1, Poseidon-BN128 2, Monolith 4)
+          (12, 3, 17, 4, 1), (10, 1, 5, 0, 1), (9, 1, 12, 2, 2), (13, 2, 30, 4, 4), (10, 3, 9, 0, 4)]
 
 
 def alone(lg, rate, cols, cap, h, inp):
@@ -60,7 +63,7 @@ def test_results_same_as_alone():
     inputs[2] = inputs[2].cpu().pin_memory()
     solo = [alone(*s, inp.cuda()) for s, inp in zip(SHAPES, inputs)]
     caps_host = [torch.zeros((1 << s[3]) * 4, dtype=torch.int64).pin_memory() for s in SHAPES]
-    with zk.Server(0, 8 << 30, 8, device_loop=True) as srv:
+    with zk.Server(0, 8 << 30, 16, device_loop=True) as srv:
         tickets = [srv.submit(*s, inp, caps_host=ch) for s, inp, ch in zip(SHAPES, inputs, caps_host)]
         for t, s, so, ch in zip(tickets, SHAPES, solo, caps_host):
             check(srv, t, s, so, ch)
@@ -117,7 +120,7 @@ def test_loop_exits_when_idle_and_restarts():
 def test_unsupported_requests_rejected_at_submit():
     inp = to_dev(O.field_data(1, 16 << 12))
     with zk.Server(0, 1 << 30, 2, device_loop=True) as srv:
-        for args in [(12, 2, 16, 2, 1), (8, 2, 16, 2, 0), (23, 1, 1, 0, 0)]:
+        for args in [(8, 2, 16, 2, 0), (23, 1, 1, 0, 0), (12, 2, 16, 2, 5)]:
             with pytest.raises(zk.ZeknoxError):
                 srv.submit(*args, inp)
         with pytest.raises(zk.ZeknoxError):

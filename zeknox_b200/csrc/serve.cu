@@ -282,10 +282,11 @@ struct Server {
         loop_live = false;
     }
 
-    // Stages of the forest, as merkle.cu launches them for Poseidon and
-    // Poseidon2 (cooperative leaves up to coop_leaves, node-parallel wide
-    // levels, the cooperative fold, levels beyond the tail's capacity, the
-    // cooperative tail); every stage gives the same digests as its kernel.
+    // Stages of the forest, as merkle.cu launches them (for Poseidon and
+    // Poseidon2 cooperative leaves up to coop_leaves; node-parallel wide
+    // levels; the fold; levels beyond the tail's capacity; the tail; the fold
+    // and tail cooperative for Poseidon and Poseidon2); every stage gives the
+    // same digests as its kernel.
     // Device time estimates of the scheduler (only their ratios matter): one
     // width-12 permutation and one LDE element of the whole GPU's throughput.
     static constexpr double PERM_NS = 1.27, LDE_ELEM_NS = 0.016;
@@ -314,6 +315,20 @@ struct Server {
         }
     }
 
+    // Device time of one permutation at the whole GPU's throughput, per hash
+    // (measured forests of 2^20 x 135 leaves: Poseidon 788, Keccak 3300,
+    // Poseidon-BN128 35, Poseidon2 1190, Monolith 2060 M/s).
+    static double perm_ns(uint32_t hash)
+    {
+        switch (hash) {
+        case HASH_KECCAK: return 0.30;
+        case HASH_POSEIDON_BN128: return 28.6;
+        case HASH_POSEIDON2: return 0.84;
+        case HASH_MONOLITH: return 0.49;
+        default: return 1.27;
+        }
+    }
+
     static void merkle_stages(std::vector<LoopStage> &out, uint64_t *digests, uint64_t *caps, const uint64_t *leaves,
                               uint64_t n_leaves, uint64_t leaf_size, uint32_t cap_height, uint32_t hash, uint64_t grid)
     {
@@ -324,7 +339,11 @@ struct Server {
         g.sub_leaves = n_leaves >> cap_height;
         g.sub_digests = 2 * g.sub_leaves - 2;
         g.log_sub = ilog2_exact(g.sub_leaves);
-        const double leaf_perms = leaf_size > 4 ? (double)((leaf_size + 7) / 8) : 0.0;
+        const bool coop = hash == HASH_POSEIDON || hash == HASH_POSEIDON2;
+        const double leaf_perms = hash == HASH_KECCAK ? (double)(leaf_size * 8 / 136 + 1)
+                                  : leaf_size > 4    ? (double)((leaf_size + 7) / 8)
+                                                     : 0.0;
+        const double pns = perm_ns(hash);
         auto stage = [&](uint32_t kind, uint32_t u, uint64_t blocks) {
             LoopStage st{};
             st.kind = kind;
@@ -344,13 +363,14 @@ struct Server {
             case LS_LEAF_COOP: per = LOOP_THREADS / 4 * leaf_perms; break;
             case LS_LEVEL: per = LOOP_THREADS; break;
             case LS_FOLD_COOP: per = 2.0 * LOOP_THREADS / 4; break;
+            case LS_FOLD: per = 2.0 * LOOP_THREADS; break;
             default: per = 2.0 * (double)(g.sub_leaves >> u); break;
             }
-            push_split(out, st, per * PERM_NS, grid);
+            push_split(out, st, per * pns, grid);
         };
         const uint32_t lg_leaves = ilog2_exact(n_leaves);
         const std::string h = std::to_string(hash);
-        if (n_leaves <= tune_get("coop_leaves." + h, lg_leaves, 1ULL << 13))
+        if (coop && n_leaves <= tune_get("coop_leaves." + h, lg_leaves, 1ULL << 13))
             stage(LS_LEAF_COOP, 0, (n_leaves + LOOP_THREADS / 4 - 1) / (LOOP_THREADS / 4));
         else
             stage(LS_LEAF, 0, (n_leaves + LOOP_THREADS - 1) / LOOP_THREADS);
@@ -362,8 +382,10 @@ struct Server {
             u0++;
             stage(LS_LEVEL, u0, ((n_leaves >> u0) + LOOP_THREADS - 1) / LOOP_THREADS);
         }
-        constexpr uint32_t NG = LOOP_THREADS / 4;
-        stage(LS_FOLD_COOP, u0, ((n_leaves >> u0) + NG - 1) / NG);
+        // the fold takes 64 nodes per CTA (cooperative) or 256 (one permutation
+        // per thread), as merkle.cu's fold kernels do
+        const uint32_t NG = coop ? LOOP_THREADS / 4 : LOOP_THREADS;
+        stage(coop ? LS_FOLD_COOP : LS_FOLD, u0, ((n_leaves >> u0) + NG - 1) / NG);
         if ((g.sub_leaves >> u0) <= NG) return;  // caps written by the fold
         uint32_t U = 0;
         while ((1u << (U + 1)) <= NG && u0 + U + 1 <= top) U++;
@@ -372,7 +394,7 @@ struct Server {
             u0++;
             stage(LS_LEVEL, u0, (((g.sub_leaves >> u0) * g.n_caps) + LOOP_THREADS - 1) / LOOP_THREADS);
         }
-        stage(LS_TAIL_COOP, u0, g.n_caps);
+        stage(coop ? LS_TAIL_COOP : LS_TAIL, u0, g.n_caps);
     }
 
     // Plan an admitted job, copy the plan to the device and post it to the
@@ -810,11 +832,8 @@ extern "C" RustError zeknox_server_submit(void *server, const zk_serve_request *
         j.digests = (uint64_t *)1;
         j.caps = (uint64_t *)1;
         zk::check_job(j);
-        if (s->device_loop &&
-            (req->input_is_values || (req->hash_type != zk::HASH_POSEIDON && req->hash_type != zk::HASH_POSEIDON2) ||
-             req->lg_n < 9 || req->lg_n > 22))
-            throw zk::arg_failure("the device loop takes coefficient inputs of 2^9 .. 2^22 per column and "
-                                  "Poseidon or Poseidon2 forests");
+        if (s->device_loop && (req->input_is_values || req->lg_n < 9 || req->lg_n > 22))
+            throw zk::arg_failure("the device loop takes coefficient inputs of 2^9 .. 2^22 per column");
         const uint64_t bytes = Server::job_bytes(*req);
         std::lock_guard<std::mutex> lk(s->mu);
         if (bytes > s->budget) throw zk::arg_failure("request needs more device memory than the server's budget");

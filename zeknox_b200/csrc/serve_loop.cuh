@@ -3,9 +3,10 @@
 // One cooperative, persistent kernel (every CTA resident at once) takes
 // requests from a ring in mapped host memory and runs their stages itself,
 // across the whole GPU: the fused LDE's passes (ntt_pass_body, every tile of
-// a pass handed out to the CTAs in turn), then the Merkle forest (leaf
-// hashes, node-parallel levels, the cooperative fold and tail).  A grid
-// barrier separates the stages.  The host admits requests against the arena
+// a pass handed out to the CTAs in turn), then the Merkle forest of any of
+// the five hashes (leaf hashes, node-parallel levels, the fold and the tail;
+// four threads per permutation for Poseidon and Poseidon2, one for the
+// others).  A grid barrier separates the stages.  The host admits requests against the arena
 // budget, plans their stages (long ones split into pieces of a few
 // milliseconds), copies the plan into device memory and posts the entry.
 //
@@ -57,6 +58,8 @@ enum LoopStageKind : uint32_t {
     LS_LEVEL = 4,      // one tree level (height u), one node per thread
     LS_FOLD_COOP = 5,  // 64 nodes of height u per CTA folded upwards in shared memory
     LS_TAIL_COOP = 6,  // one subtree per CTA from height u to its cap
+    LS_FOLD = 7,       // 256 nodes of height u per CTA, one permutation per thread
+    LS_TAIL = 8,       // one subtree per CTA, one permutation per thread
 };
 
 enum LoopDone : uint32_t { LOOP_DONE_NONE = 0, LOOP_DONE_OK = 1, LOOP_DONE_TIMEOUT = 2, LOOP_DONE_ABORT = 3 };
@@ -234,6 +237,11 @@ __device__ __noinline__ void loop_leaf(const LoopStage *pst, uint32_t rank)
         if (i >= g.n_leaves) continue;
         uint64_t *dst = g.sub_leaves == 1 ? st.caps + 4 * i : st.digests + 4 * merkle_node_index(g, i, 0);
         uint64_t d[4];
+        if (H == HASH_KECCAK && g.leaf_size < 4) {
+            // Keccak copies a < 4-word leaf over the words already there
+#pragma unroll
+            for (int q = 0; q < 4; q++) d[q] = dst[q];
+        }
         leaf_hash<H>(st.leaves + i * g.leaf_size, g.leaf_size, d);
 #pragma unroll
         for (int q = 0; q < 4; q++) dst[q] = d[q];
@@ -396,16 +404,120 @@ __device__ __noinline__ void loop_tail_coop(const LoopStage *pst, uint64_t (*buf
     }
 }
 
+// 256 consecutive nodes of height u per work item, one permutation per
+// thread (merkle.cuh's merkle_fold_kernel: the hashes without a cooperative
+// form).
+template <int H>
+__device__ __noinline__ void loop_fold(const LoopStage *pst, uint64_t (*node)[4], uint32_t rank)
+{
+    constexpr uint32_t T = LOOP_THREADS;
+    const LoopStage st = *pst;
+    const MerkleGeom &g = st.g;
+    const uint32_t u0 = st.u, t = threadIdx.x;
+    const uint64_t count = g.n_leaves >> u0;
+    const uint32_t top = g.log_sub - 1;
+    uint32_t U = 0;
+    while ((1u << (U + 1)) <= T && u0 + U + 1 <= top) U++;
+    for (uint64_t b = rank; b < st.blocks; b += gridDim.x) {
+        const uint64_t i0 = (st.first + b) * T;
+        const uint64_t cta_nodes = count - i0 < (uint64_t)T ? count - i0 : (uint64_t)T;
+        if (t < cta_nodes) {
+            const uint64_t di = merkle_node_index(g, (i0 + t) << u0, u0);
+#pragma unroll
+            for (int q = 0; q < 4; q++) node[t][q] = st.digests[4 * di + q];
+        }
+        for (uint32_t v = 1; v <= U; v++) {
+            __syncthreads();
+            const uint32_t nodes = T >> v;
+            uint64_t h[4];
+            const bool act = t < nodes && ((uint64_t)t << v) < cta_nodes;
+            if (act) {
+                hash_two<H>(node[2 * t], node[2 * t + 1], h);
+                const uint64_t di = merkle_node_index(g, (i0 + ((uint64_t)t << v)) << u0, u0 + v);
+#pragma unroll
+                for (int q = 0; q < 4; q++) st.digests[4 * di + q] = h[q];
+            }
+            __syncthreads();
+            if (act) {
+#pragma unroll
+                for (int q = 0; q < 4; q++) node[t][q] = h[q];
+            }
+        }
+        const uint64_t sub_nodes = g.sub_leaves >> u0;
+        if (u0 + U == top && sub_nodes <= (uint64_t)T) {
+            __syncthreads();
+            const uint32_t subs = (uint32_t)(cta_nodes / sub_nodes);
+            if (t < subs) {
+                uint64_t h[4];
+                hash_two<H>(node[2 * t], node[2 * t + 1], h);
+                const uint64_t k = ((i0 << u0) >> g.log_sub) + t;
+#pragma unroll
+                for (int q = 0; q < 4; q++) st.caps[4 * k + q] = h[q];
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// One subtree per work item from height u to its cap, one permutation per
+// thread (merkle.cuh's merkle_tail_kernel).
+template <int H>
+__device__ __noinline__ void loop_tail(const LoopStage *pst, uint64_t (*bufa)[4], uint64_t (*bufb)[4], uint32_t rank)
+{
+    const LoopStage st = *pst;
+    const MerkleGeom &g = st.g;
+    for (uint64_t kb = rank; kb < st.blocks; kb += gridDim.x) {
+        const uint64_t k = st.first + kb;
+        uint64_t *sub = st.digests + k * g.sub_digests * 4;
+        uint32_t m = (uint32_t)(g.sub_leaves >> st.u);
+        for (uint32_t j = threadIdx.x; j < m; j += LOOP_THREADS) {
+#pragma unroll
+            for (int q = 0; q < 4; q++) bufa[j][q] = sub[4 * (m - 2 + j) + q];
+        }
+        uint64_t(*src)[4] = bufa;
+        uint64_t(*dst)[4] = bufb;
+        while (m > 2) {
+            __syncthreads();
+            const uint32_t half = m / 2;
+            for (uint32_t j = threadIdx.x; j < half; j += LOOP_THREADS) {
+                uint64_t h[4];
+                hash_two<H>(src[2 * j], src[2 * j + 1], h);
+#pragma unroll
+                for (int q = 0; q < 4; q++) {
+                    sub[4 * (half - 2 + j) + q] = h[q];
+                    dst[j][q] = h[q];
+                }
+            }
+            uint64_t(*tmp)[4] = src;
+            src = dst;
+            dst = tmp;
+            m = half;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            uint64_t h[4];
+            hash_two<H>(src[0], src[1], h);
+#pragma unroll
+            for (int q = 0; q < 4; q++) st.caps[4 * k + q] = h[q];
+        }
+        __syncthreads();
+    }
+}
+
 template <int H>
 __device__ __forceinline__ void loop_run_merkle(const LoopStage &st, uint64_t *sm, uint32_t rank)
 {
     switch (st.kind) {
     case LS_LEAF: loop_leaf<H>(&st, rank); break;
-    case LS_LEAF_COOP: loop_leaf_coop<H>(&st, rank); break;
     case LS_LEVEL: loop_level<H>(&st, rank); break;
-    case LS_FOLD_COOP: loop_fold_coop<H>(&st, (uint64_t(*)[4])sm, rank); break;
+    case LS_FOLD: loop_fold<H>(&st, (uint64_t(*)[4])sm, rank); break;
+    case LS_TAIL: loop_tail<H>(&st, (uint64_t(*)[4])sm, (uint64_t(*)[4])(sm + 4 * LOOP_TAIL_MAXM), rank); break;
     default:
-        loop_tail_coop<H>(&st, (uint64_t(*)[4])sm, (uint64_t(*)[4])(sm + 4 * LOOP_TAIL_MAXM), rank);
+        if constexpr (HasCoop<H>::value) {
+            if (st.kind == LS_LEAF_COOP) loop_leaf_coop<H>(&st, rank);
+            else if (st.kind == LS_FOLD_COOP) loop_fold_coop<H>(&st, (uint64_t(*)[4])sm, rank);
+            else loop_tail_coop<H>(&st, (uint64_t(*)[4])sm, (uint64_t(*)[4])(sm + 4 * LOOP_TAIL_MAXM), rank);
+        }
         break;
     }
 }
@@ -536,6 +648,9 @@ __global__ void __launch_bounds__(LOOP_THREADS, ZK_LOOP_MIN_CTAS) serve_loop_ker
         const LoopStage &st = s_stage;
         if (st.kind == LS_PASS) loop_run_pass(st, &st.a, loop_sm, rank);
         else if (st.hash == HASH_POSEIDON2) loop_run_merkle<HASH_POSEIDON2>(st, loop_sm, rank);
+        else if (st.hash == HASH_KECCAK) loop_run_merkle<HASH_KECCAK>(st, loop_sm, rank);
+        else if (st.hash == HASH_MONOLITH) loop_run_merkle<HASH_MONOLITH>(st, loop_sm, rank);
+        else if (st.hash == HASH_POSEIDON_BN128) loop_run_merkle<HASH_POSEIDON_BN128>(st, loop_sm, rank);
         else loop_run_merkle<HASH_POSEIDON>(st, loop_sm, rank);
         const bool ok = loop_grid_sync(ctl, barrier_ns);
         if (leader) {
