@@ -117,6 +117,7 @@ struct LoopCtl {  // device memory, zeroed (but for taken / finished) before eac
     uint64_t taken, finished;
     const LoopStage *stage;  // the stage that runs next
     uint32_t n_active, pad;
+    unsigned long long next_item;  // work items of the running stage handed out past the first round
     LoopActive active[LOOP_RING];
     uint32_t cta_sm[LOOP_MAX_CTAS];  // %smid of every CTA
 };
@@ -189,11 +190,33 @@ __device__ __forceinline__ bool loop_grid_sync(LoopCtl *ctl, uint64_t limit_ns)
 // of one allocation over every stage of the loop.  A pass copies its
 // arguments out of shared memory first: shared stores to the tile could
 // otherwise alias them and force a reload at every use.
+// Where a CTA takes its work items: its first by rank (spread over SMs),
+// the rest from the stage's counter in turn (a CTA that finishes early takes
+// more), as a hardware grid scheduler would.  Measured on a 2^20 x 256
+// request: LDE passes 53.8 against 57.8 ms with every item by rank, wide
+// levels 10.5 against 11.1 ms.  The leaf stages keep the rank stride: the
+// barrier of each hand-out lines a CTA's warps up again, where by rank they
+// run ahead into the next item (leaf hashes 354.0 against 352.1 ms with the
+// counter, 11.38 against 10.97 ms at 2^16 x 128).
+struct LoopWork {
+    uint32_t rank;
+    unsigned long long *next;
+};
+
+__device__ __forceinline__ uint64_t loop_grab(const LoopWork &w)
+{
+    __shared__ uint64_t s_b;
+    __syncthreads();
+    if (threadIdx.x == 0) s_b = gridDim.x + atomicAdd(w.next, 1ULL);
+    __syncthreads();
+    return s_b;
+}
+
 template <int LOGR, int LOADM, int STOREM>
-__device__ __noinline__ void loop_pass(const NttPassArgs *pa, uint64_t first, uint64_t blocks, uint64_t *sm, uint32_t rank)
+__device__ __noinline__ void loop_pass(const NttPassArgs *pa, uint64_t first, uint64_t blocks, uint64_t *sm, LoopWork w)
 {
     const NttPassArgs a = *pa;
-    for (uint64_t b = rank; b < blocks; b += gridDim.x) {
+    for (uint64_t b = w.rank; b < blocks; b = loop_grab(w)) {
         ntt_pass_body<LOGR, 0, LOOP_THREADS, LOOP_PASS_TILE, LOADM, STOREM, 1>(a, (uint32_t)(first + b), sm);
         __syncthreads();
     }
@@ -201,34 +224,34 @@ __device__ __noinline__ void loop_pass(const NttPassArgs *pa, uint64_t first, ui
 
 // The pass shapes a planned fused LDE of 2^9 .. 2^22-point columns uses with
 // the row-output radix 2^8 (the host rejects any other before posting).
-__device__ __forceinline__ void loop_run_pass(const LoopStage &st, const NttPassArgs *a, uint64_t *sm, uint32_t rank)
+__device__ __forceinline__ void loop_run_pass(const LoopStage &st, const NttPassArgs *a, uint64_t *sm, LoopWork w)
 {
     if (st.load == LOAD_COSETS && st.store == STORE_SAME) {
         switch (st.logr) {
-        case 1: loop_pass<1, LOAD_COSETS, STORE_SAME>(a, st.first, st.blocks, sm, rank); break;
-        case 2: loop_pass<2, LOAD_COSETS, STORE_SAME>(a, st.first, st.blocks, sm, rank); break;
-        case 3: loop_pass<3, LOAD_COSETS, STORE_SAME>(a, st.first, st.blocks, sm, rank); break;
-        case 4: loop_pass<4, LOAD_COSETS, STORE_SAME>(a, st.first, st.blocks, sm, rank); break;
-        case 5: loop_pass<5, LOAD_COSETS, STORE_SAME>(a, st.first, st.blocks, sm, rank); break;
-        case 6: loop_pass<6, LOAD_COSETS, STORE_SAME>(a, st.first, st.blocks, sm, rank); break;
-        case 7: loop_pass<7, LOAD_COSETS, STORE_SAME>(a, st.first, st.blocks, sm, rank); break;
-        case 8: loop_pass<8, LOAD_COSETS, STORE_SAME>(a, st.first, st.blocks, sm, rank); break;
-        case 9: loop_pass<9, LOAD_COSETS, STORE_SAME>(a, st.first, st.blocks, sm, rank); break;
-        default: loop_pass<10, LOAD_COSETS, STORE_SAME>(a, st.first, st.blocks, sm, rank); break;
+        case 1: loop_pass<1, LOAD_COSETS, STORE_SAME>(a, st.first, st.blocks, sm, w); break;
+        case 2: loop_pass<2, LOAD_COSETS, STORE_SAME>(a, st.first, st.blocks, sm, w); break;
+        case 3: loop_pass<3, LOAD_COSETS, STORE_SAME>(a, st.first, st.blocks, sm, w); break;
+        case 4: loop_pass<4, LOAD_COSETS, STORE_SAME>(a, st.first, st.blocks, sm, w); break;
+        case 5: loop_pass<5, LOAD_COSETS, STORE_SAME>(a, st.first, st.blocks, sm, w); break;
+        case 6: loop_pass<6, LOAD_COSETS, STORE_SAME>(a, st.first, st.blocks, sm, w); break;
+        case 7: loop_pass<7, LOAD_COSETS, STORE_SAME>(a, st.first, st.blocks, sm, w); break;
+        case 8: loop_pass<8, LOAD_COSETS, STORE_SAME>(a, st.first, st.blocks, sm, w); break;
+        case 9: loop_pass<9, LOAD_COSETS, STORE_SAME>(a, st.first, st.blocks, sm, w); break;
+        default: loop_pass<10, LOAD_COSETS, STORE_SAME>(a, st.first, st.blocks, sm, w); break;
         }
     } else if (st.store == STORE_SAME) {
         switch (st.logr) {
-        case 5: loop_pass<5, LOAD_PLAIN, STORE_SAME>(a, st.first, st.blocks, sm, rank); break;
-        case 6: loop_pass<6, LOAD_PLAIN, STORE_SAME>(a, st.first, st.blocks, sm, rank); break;
-        default: loop_pass<7, LOAD_PLAIN, STORE_SAME>(a, st.first, st.blocks, sm, rank); break;
+        case 5: loop_pass<5, LOAD_PLAIN, STORE_SAME>(a, st.first, st.blocks, sm, w); break;
+        case 6: loop_pass<6, LOAD_PLAIN, STORE_SAME>(a, st.first, st.blocks, sm, w); break;
+        default: loop_pass<7, LOAD_PLAIN, STORE_SAME>(a, st.first, st.blocks, sm, w); break;
         }
     } else {
-        loop_pass<8, LOAD_PLAIN, STORE_ROWS>(a, st.first, st.blocks, sm, rank);
+        loop_pass<8, LOAD_PLAIN, STORE_ROWS>(a, st.first, st.blocks, sm, w);
     }
 }
 
 template <int H>
-__device__ __noinline__ void loop_leaf(const LoopStage *pst, uint32_t rank)
+__device__ __noinline__ void loop_leaf(const LoopStage *pst, LoopWork w)
 {
     // only the loop bounds and the row address stay live across the
     // permutation; the destination's geometry is read again from shared
@@ -236,7 +259,7 @@ __device__ __noinline__ void loop_leaf(const LoopStage *pst, uint32_t rank)
     const uint64_t blocks = pst->blocks, first = pst->first;
     const uint64_t n_leaves = pst->g.n_leaves, leaf_size = pst->g.leaf_size;
     const uint64_t *leaves = pst->leaves;
-    for (uint64_t b = rank; b < blocks; b += gridDim.x) {
+    for (uint64_t b = w.rank; b < blocks; b += gridDim.x) {
         const uint64_t i = (first + b) * LOOP_THREADS + threadIdx.x;
         if (i >= n_leaves) continue;
         uint64_t d[4];
@@ -263,13 +286,13 @@ __device__ __noinline__ void loop_leaf(const LoopStage *pst, uint32_t rank)
 }
 
 template <int H>
-__device__ __noinline__ void loop_leaf_coop(const LoopStage *pst, uint32_t rank)
+__device__ __noinline__ void loop_leaf_coop(const LoopStage *pst, LoopWork w)
 {
     const LoopStage st = *pst;
     const MerkleGeom &g = st.g;
     CoopGroup c;
     c.init();
-    for (uint64_t b = rank; b < st.blocks; b += gridDim.x) {
+    for (uint64_t b = w.rank; b < st.blocks; b += gridDim.x) {
         const uint64_t gi = ((st.first + b) * LOOP_THREADS + threadIdx.x) >> 2;
         if ((gi & ~7ULL) >= g.n_leaves) continue;  // the whole warp is past the end
         const uint64_t i = gi < g.n_leaves ? gi : g.n_leaves - 1;
@@ -284,12 +307,12 @@ __device__ __noinline__ void loop_leaf_coop(const LoopStage *pst, uint32_t rank)
 }
 
 template <int H>
-__device__ __noinline__ void loop_level(const LoopStage *pst, uint32_t rank)
+__device__ __noinline__ void loop_level(const LoopStage *pst, LoopWork w)
 {
     const LoopStage st = *pst;
     const MerkleGeom &g = st.g;
     const uint64_t per_sub = g.sub_leaves >> st.u, total = per_sub * g.n_caps;
-    for (uint64_t b = rank; b < st.blocks; b += gridDim.x) {
+    for (uint64_t b = w.rank; b < st.blocks; b = loop_grab(w)) {
         const uint64_t x = (st.first + b) * LOOP_THREADS + threadIdx.x;
         if (x >= total) continue;
         const uint64_t k = x / per_sub, j = x % per_sub;
@@ -305,7 +328,7 @@ __device__ __noinline__ void loop_level(const LoopStage *pst, uint32_t rank)
 // 64 consecutive nodes of height u per work item, folded upwards inside the
 // CTA (the cooperative fold of merkle.cuh, with the caps of whole subtrees).
 template <int H>
-__device__ __noinline__ void loop_fold_coop(const LoopStage *pst, uint64_t (*node)[4], uint32_t rank)
+__device__ __noinline__ void loop_fold_coop(const LoopStage *pst, uint64_t (*node)[4], LoopWork w)
 {
     const LoopStage st = *pst;
     constexpr uint32_t NG = LOOP_THREADS / 4;
@@ -319,7 +342,7 @@ __device__ __noinline__ void loop_fold_coop(const LoopStage *pst, uint64_t (*nod
     const uint32_t top = g.log_sub - 1;
     uint32_t U = 0;
     while ((1u << (U + 1)) <= NG && u0 + U + 1 <= top) U++;
-    for (uint64_t b = rank; b < st.blocks; b += gridDim.x) {
+    for (uint64_t b = w.rank; b < st.blocks; b = loop_grab(w)) {
         const uint64_t i0 = (st.first + b) * NG;
         const uint64_t cta_nodes = count - i0 < (uint64_t)NG ? count - i0 : (uint64_t)NG;
         for (uint32_t t = threadIdx.x; t < 4 * cta_nodes; t += LOOP_THREADS)
@@ -368,7 +391,7 @@ __device__ __noinline__ void loop_fold_coop(const LoopStage *pst, uint64_t (*nod
 // One subtree per work item, from height u to its cap (the cooperative tail
 // of merkle.cuh).
 template <int H>
-__device__ __noinline__ void loop_tail_coop(const LoopStage *pst, uint64_t (*bufa)[4], uint64_t (*bufb)[4], uint32_t rank)
+__device__ __noinline__ void loop_tail_coop(const LoopStage *pst, uint64_t (*bufa)[4], uint64_t (*bufb)[4], LoopWork w)
 {
     const LoopStage st = *pst;
     constexpr uint32_t NG = LOOP_THREADS / 4;
@@ -376,7 +399,7 @@ __device__ __noinline__ void loop_tail_coop(const LoopStage *pst, uint64_t (*buf
     CoopGroup c;
     c.init();
     const uint32_t grp = threadIdx.x >> 2;
-    for (uint64_t kb = rank; kb < st.blocks; kb += gridDim.x) {
+    for (uint64_t kb = w.rank; kb < st.blocks; kb = loop_grab(w)) {
         const uint64_t k = st.first + kb;
         uint64_t *sub = st.digests + k * g.sub_digests * 4;
         uint32_t m = (uint32_t)(g.sub_leaves >> st.u);
@@ -422,7 +445,7 @@ __device__ __noinline__ void loop_tail_coop(const LoopStage *pst, uint64_t (*buf
 // thread (merkle.cuh's merkle_fold_kernel: the hashes without a cooperative
 // form).
 template <int H>
-__device__ __noinline__ void loop_fold(const LoopStage *pst, uint64_t (*node)[4], uint32_t rank)
+__device__ __noinline__ void loop_fold(const LoopStage *pst, uint64_t (*node)[4], LoopWork w)
 {
     constexpr uint32_t T = LOOP_THREADS;
     const LoopStage st = *pst;
@@ -432,7 +455,7 @@ __device__ __noinline__ void loop_fold(const LoopStage *pst, uint64_t (*node)[4]
     const uint32_t top = g.log_sub - 1;
     uint32_t U = 0;
     while ((1u << (U + 1)) <= T && u0 + U + 1 <= top) U++;
-    for (uint64_t b = rank; b < st.blocks; b += gridDim.x) {
+    for (uint64_t b = w.rank; b < st.blocks; b = loop_grab(w)) {
         const uint64_t i0 = (st.first + b) * T;
         const uint64_t cta_nodes = count - i0 < (uint64_t)T ? count - i0 : (uint64_t)T;
         if (t < cta_nodes) {
@@ -476,11 +499,11 @@ __device__ __noinline__ void loop_fold(const LoopStage *pst, uint64_t (*node)[4]
 // One subtree per work item from height u to its cap, one permutation per
 // thread (merkle.cuh's merkle_tail_kernel).
 template <int H>
-__device__ __noinline__ void loop_tail(const LoopStage *pst, uint64_t (*bufa)[4], uint64_t (*bufb)[4], uint32_t rank)
+__device__ __noinline__ void loop_tail(const LoopStage *pst, uint64_t (*bufa)[4], uint64_t (*bufb)[4], LoopWork w)
 {
     const LoopStage st = *pst;
     const MerkleGeom &g = st.g;
-    for (uint64_t kb = rank; kb < st.blocks; kb += gridDim.x) {
+    for (uint64_t kb = w.rank; kb < st.blocks; kb = loop_grab(w)) {
         const uint64_t k = st.first + kb;
         uint64_t *sub = st.digests + k * g.sub_digests * 4;
         uint32_t m = (uint32_t)(g.sub_leaves >> st.u);
@@ -519,18 +542,18 @@ __device__ __noinline__ void loop_tail(const LoopStage *pst, uint64_t (*bufa)[4]
 }
 
 template <int H>
-__device__ __forceinline__ void loop_run_merkle(const LoopStage &st, uint64_t *sm, uint32_t rank)
+__device__ __forceinline__ void loop_run_merkle(const LoopStage &st, uint64_t *sm, LoopWork w)
 {
     switch (st.kind) {
-    case LS_LEAF: loop_leaf<H>(&st, rank); break;
-    case LS_LEVEL: loop_level<H>(&st, rank); break;
-    case LS_FOLD: loop_fold<H>(&st, (uint64_t(*)[4])sm, rank); break;
-    case LS_TAIL: loop_tail<H>(&st, (uint64_t(*)[4])sm, (uint64_t(*)[4])(sm + 4 * LOOP_TAIL_MAXM), rank); break;
+    case LS_LEAF: loop_leaf<H>(&st, w); break;
+    case LS_LEVEL: loop_level<H>(&st, w); break;
+    case LS_FOLD: loop_fold<H>(&st, (uint64_t(*)[4])sm, w); break;
+    case LS_TAIL: loop_tail<H>(&st, (uint64_t(*)[4])sm, (uint64_t(*)[4])(sm + 4 * LOOP_TAIL_MAXM), w); break;
     default:
         if constexpr (HasCoop<H>::value) {
-            if (st.kind == LS_LEAF_COOP) loop_leaf_coop<H>(&st, rank);
-            else if (st.kind == LS_FOLD_COOP) loop_fold_coop<H>(&st, (uint64_t(*)[4])sm, rank);
-            else loop_tail_coop<H>(&st, (uint64_t(*)[4])sm, (uint64_t(*)[4])(sm + 4 * LOOP_TAIL_MAXM), rank);
+            if (st.kind == LS_LEAF_COOP) loop_leaf_coop<H>(&st, w);
+            else if (st.kind == LS_FOLD_COOP) loop_fold_coop<H>(&st, (uint64_t(*)[4])sm, w);
+            else loop_tail_coop<H>(&st, (uint64_t(*)[4])sm, (uint64_t(*)[4])(sm + 4 * LOOP_TAIL_MAXM), w);
         }
         break;
     }
@@ -592,6 +615,7 @@ __global__ void __launch_bounds__(LOOP_THREADS, ZK_LOOP_MIN_CTAS) serve_loop_ker
     const bool leader = blockIdx.x == 0 && threadIdx.x == 0;
     const uint64_t barrier_ns = ring->barrier_ns;
     const uint32_t rank = loop_rank(ctl, barrier_ns);
+    const LoopWork w{rank, &ctl->next_item};
     for (;;) {
         if (leader) {
             // take posted entries (waiting, bounded, only when nothing is active)
@@ -642,6 +666,7 @@ __global__ void __launch_bounds__(LOOP_THREADS, ZK_LOOP_MIN_CTAS) serve_loop_ker
                 const LoopActive &e = ctl->active[best];
                 ctl->pick = best;
                 ctl->stage = e.plan + e.cursor;
+                ctl->next_item = 0;
                 cur = (int)e.slot;
             }
             ctl->cur = cur;
@@ -660,12 +685,12 @@ __global__ void __launch_bounds__(LOOP_THREADS, ZK_LOOP_MIN_CTAS) serve_loop_ker
             ((uint64_t *)&s_stage)[w] = ((const volatile uint64_t *)s_next)[w];
         __syncthreads();
         const LoopStage &st = s_stage;
-        if (st.kind == LS_PASS) loop_run_pass(st, &st.a, loop_sm, rank);
-        else if (st.hash == HASH_POSEIDON2) loop_run_merkle<HASH_POSEIDON2>(st, loop_sm, rank);
-        else if (st.hash == HASH_KECCAK) loop_run_merkle<HASH_KECCAK>(st, loop_sm, rank);
-        else if (st.hash == HASH_MONOLITH) loop_run_merkle<HASH_MONOLITH>(st, loop_sm, rank);
-        else if (st.hash == HASH_POSEIDON_BN128) loop_run_merkle<HASH_POSEIDON_BN128>(st, loop_sm, rank);
-        else loop_run_merkle<HASH_POSEIDON>(st, loop_sm, rank);
+        if (st.kind == LS_PASS) loop_run_pass(st, &st.a, loop_sm, w);
+        else if (st.hash == HASH_POSEIDON2) loop_run_merkle<HASH_POSEIDON2>(st, loop_sm, w);
+        else if (st.hash == HASH_KECCAK) loop_run_merkle<HASH_KECCAK>(st, loop_sm, w);
+        else if (st.hash == HASH_MONOLITH) loop_run_merkle<HASH_MONOLITH>(st, loop_sm, w);
+        else if (st.hash == HASH_POSEIDON_BN128) loop_run_merkle<HASH_POSEIDON_BN128>(st, loop_sm, w);
+        else loop_run_merkle<HASH_POSEIDON>(st, loop_sm, w);
         const bool ok = loop_grid_sync(ctl, barrier_ns);
         if (leader) {
             LoopActive &e = ctl->active[ctl->pick];
