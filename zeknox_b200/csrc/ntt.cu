@@ -25,6 +25,7 @@ static constexpr int PASS_TILE = 4096;  // 32 KiB of shared memory; measured 1.0
 static constexpr uint32_t LOG_PASS_TILE = __builtin_ctz(PASS_TILE);
 static constexpr uint32_t MAX_SPLIT_LOGR = LOG_PASS_TILE - 2;  // passes before the last (see plan_passes)
 static constexpr uint32_t MAX_ROWS_LOGR = LOG_PASS_TILE - 4;   // row-output passes: 16 columns x 2^LOGR
+static constexpr uint32_t COL_SPLIT_LOGR = 9;  // largest pass of a multi-pass column-output transform
 
 // ------------------------------------------------------------- pass dispatch
 
@@ -90,15 +91,22 @@ struct Pass {
 // 32-byte sectors); a row-output pass spans at most 2^(LT - 4) positions of 16
 // columns.  Single-pass transforms may use the whole tile.
 
-static std::vector<Pass> plan_passes_last(uint32_t L, bool rows, uint32_t last_rows)
+static std::vector<Pass> plan_passes_last(uint32_t L, bool rows, uint32_t last_rows, uint32_t split_logr = 0)
 {
     std::vector<uint32_t> sizes;
     last_rows = last_rows < 1 ? 1 : (last_rows > MAX_ROWS_LOGR ? MAX_ROWS_LOGR : last_rows);
-    const uint32_t last_max = rows ? last_rows : LOG_PASS_TILE;
+    // column output: one pass up to the whole tile, else passes of at most
+    // 2^COL_SPLIT_LOGR points -- or, with split_logr set (knob
+    // ntt_split_logr), passes of at most 2^split_logr points whatever the
+    // size.  Radix-2^10 passes are the slowest per stage: at 2^19 and 2^20
+    // points three passes beat two (measured on B200: column LDE 8.90 -> 8.05
+    // ms for 64 columns x 2^19 at rate 3, NTT 7.24 -> 7.09 ms for 512 x 2^19).
+    const uint32_t split = split_logr ? (split_logr < MAX_SPLIT_LOGR ? split_logr : MAX_SPLIT_LOGR) : COL_SPLIT_LOGR;
+    const uint32_t last_max = rows ? last_rows : (split_logr ? split : LOG_PASS_TILE);
     if (L <= last_max) {
         sizes.push_back(L);
     } else if (!rows) {
-        uint32_t np = (L + MAX_SPLIT_LOGR - 1) / MAX_SPLIT_LOGR;
+        uint32_t np = (L + split - 1) / split;
         for (uint32_t i = 0; i < np; i++) sizes.push_back(L / np + (i < L % np ? 1 : 0));
     } else {
         uint32_t rem = L - last_rows;
@@ -118,7 +126,8 @@ static std::vector<Pass> plan_passes_last(uint32_t L, bool rows, uint32_t last_r
 // The last pass of a row-output transform has radix 2^lde_last_logr (tuned).
 static std::vector<Pass> plan_passes(uint32_t L, bool rows)
 {
-    return plan_passes_last(L, rows, (uint32_t)tune_get("lde_last_logr", L, MAX_ROWS_LOGR));
+    return plan_passes_last(L, rows, (uint32_t)tune_get("lde_last_logr", L, MAX_ROWS_LOGR),
+                            rows ? 0 : (uint32_t)tune_get("ntt_split_logr", L, 0));
 }
 
 // Batched DIF over `vcols` virtual columns of size 2^L; output in bit-reversed

@@ -107,7 +107,8 @@ uint32_t ilog2_exact(uint64_t x);  // -1u if x is not a power of two
 // entry and then to `dflt`.  Knobs: "leaf_threads.<hash>" (64/128/256),
 // "lde_chunk_mib", "lde_host_chunk_mib", "lde_last_logr" (1..8), "wide_level_nodes.<hash>",
 // "coop_leaves.<hash>", "transpose_bulk" (0 16-byte form, 1..8 bulk-copy tile
-// shape, 9 by column count).
+// shape, 9 by column count), "ntt_split_logr" (largest pass of a
+// column-output transform, 1..10; 0 the built-in split).
 uint64_t tune_get(const std::string &name, uint32_t lg, uint64_t dflt);
 void tune_set(const std::string &name, uint32_t lg, uint64_t value);
 void tune_clear();
