@@ -14,7 +14,8 @@ from zeknox_b200 import autotune
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 KNOBS = {"leaf_threads": {64, 128, 256}, "lde_chunk_mib": None, "lde_last_logr": set(range(1, 9)),
-         "wide_level_nodes": None, "coop_leaves": None, "lde_host_chunk_mib": None}
+         "wide_level_nodes": None, "coop_leaves": None, "lde_host_chunk_mib": None,
+         "ntt_split_logr": {0, 7, 8, 9, 10}, "transpose_bulk": set(range(10))}
 
 
 @pytest.fixture
@@ -95,7 +96,17 @@ def test_committed_table_is_well_formed():
         assert lg == "*" or 0 <= int(lg) <= 32, (ln, lg)
         allowed = KNOBS[base]
         assert allowed is None or int(value) in allowed, (ln, value)
-        assert int(value) > 0
+        assert int(value) > 0 or (allowed is not None and 0 in allowed), (ln, value)
+
+
+def test_autotune_partial_run_keeps_other_knobs(tmp_path):
+    """A run of some searches only (--only) keeps the other knobs' lines."""
+    p = tmp_path / "t.txt"
+    p.write_text("# header\nleaf_threads.3 18 128   # ms\nntt_split_logr 20 9 # ms\n"
+                 "transpose_bulk 18 3\nlde_last_logr 13 8\n")
+    kept = autotune.kept_table_lines(str(p), {"ntt_split_logr", "transpose_bulk"})
+    assert [k.split()[0] for k in kept] == ["leaf_threads.3", "lde_last_logr"]
+    assert autotune.kept_table_lines(str(tmp_path / "missing.txt"), {"lde_last_logr"}) == []
 
 
 def test_autotune_candidates_include_the_defaults():
