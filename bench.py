@@ -397,6 +397,14 @@ def run_stage(args):
     import torch
     import zeknox_b200 as zk
     lg = args.lg_n
+    if args.only == "ntt":
+        # compute_batched_ntt of COLS natural-order columns of 2^lg_n, in place
+        x = dev_field(COLS << lg, 5)
+        for _ in range(args.warmup + args.steps):
+            zk.ntt_batch(0, x, lg, COLS)
+        torch.cuda.synchronize()
+        print("stage ntt lg_n %d done, %d launches" % (lg, zk.launch_count()))
+        return
     n, N = 1 << lg, 1 << (lg + RATE)
     inp = torch.from_numpy(field_data(5, COLS * n).view(np.int64).copy()).cuda()
     leaves = torch.empty(N * COLS, dtype=torch.int64, device="cuda")
@@ -869,7 +877,7 @@ def main():
     ap.add_argument("--cpu-lg", type=int, default=15, help="log2 coefficients per column of the CPU sample")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     ap.add_argument("--lg-n", type=int, default=LG_N, help="log2 coefficients per column (profiling cases)")
-    ap.add_argument("--only", default=None, choices=["lde", "merkle", "transpose"],
+    ap.add_argument("--only", default=None, choices=["lde", "merkle", "transpose", "ntt"],
                     help="profiling: run only this stage for warmup+steps iterations and exit")
     ap.add_argument("--hash", type=int, default=HASH, help="--only merkle: hash type (0 Poseidon, 1 Keccak, "
                     "2 Poseidon-BN128, 3 Poseidon2, 4 Monolith)")
