@@ -163,9 +163,9 @@ RustError zeknox_server_create(size_t device_id, uint64_t budget_bytes, uint32_t
  * one.  The kernel marks each entry done in host memory, and exits after
  * 20 ms without requests (the next post relaunches it).  Every wait of the
  * kernel is bounded in time.  A request whose wait runs out fails with
- * -cudaErrorLaunchTimeout.  Requests in this mode: coefficients
- * (input_is_values 0), any hash type, 2^9 <= 2^lg_n <= 2^22.
- * No reference counterpart. */
+ * -cudaErrorLaunchTimeout.  Requests in this mode: coefficients or
+ * evaluations (the loop then runs the inverse transform first), any hash
+ * type, 2^9 <= 2^lg_n <= 2^22.  No reference counterpart. */
 #define ZK_SERVE_DEVICE_LOOP 1u
 RustError zeknox_server_create_ex(size_t device_id, uint64_t budget_bytes, uint32_t slots, uint32_t flags,
                                   void **server);

@@ -1,7 +1,8 @@
 """Device-resident request loop (zeknox_server_create_ex with
 ZK_SERVE_DEVICE_LOOP): every request's leaves, digests and caps equal the
-same job committed alone through zeknox_commit; a request whose bounded wait
-runs out fails alone; the loop exits when idle and comes back."""
+same job committed alone through zeknox_commit, from coefficients and from
+evaluations; a request whose bounded wait runs out fails alone; the loop
+exits when idle and comes back."""
 import time
 
 import numpy as np
@@ -71,6 +72,40 @@ def test_results_same_as_alone():
         assert st["in_use"] == 0 and st["completed"] == len(SHAPES)
 
 
+# evaluation-form inputs: the loop runs the inverse transform first (copy,
+# inverse passes of 1-3 per column, bit-reversal reorder); 2^9 .. 2^20 points
+# (single passes of 2^9 .. 2^12, two and three passes), one from pinned host
+# memory
+VALUE_SHAPES = [(9, 1, 16, 4, 0), (12, 2, 33, 3, 3), (14, 3, 20, 4, 0), (17, 1, 8, 2, 3), (20, 1, 4, 4, 0),
+                (11, 3, 12, 0, 1)]
+
+
+def test_evaluation_inputs_same_as_alone():
+    inputs = [to_dev(O.field_data(4700 + i, s[2] << s[0])) for i, s in enumerate(VALUE_SHAPES)]
+    inputs[1] = inputs[1].cpu().pin_memory()
+    solo = []
+    for s, inp in zip(VALUE_SHAPES, inputs):
+        lg, rate, cols, cap, h = s
+        N = 1 << (lg + rate)
+        leaves = torch.zeros(N * cols, dtype=torch.int64, device="cuda")
+        n_dig, n_cap = zk.merkle_sizes(N, cap)
+        dig = torch.zeros(max(n_dig, 1) * 4, dtype=torch.int64, device="cuda")
+        caps = torch.zeros(n_cap * 4, dtype=torch.int64, device="cuda")
+        zk.commit(0, zk.commit_job(lg, rate, cols, cap, h, inp.cuda(), leaves, dig, caps, input_is_values=True))
+        solo.append((to_np(leaves), to_np(dig)[: n_dig * 4], to_np(caps)))
+    caps_host = [torch.zeros((1 << s[3]) * 4, dtype=torch.int64).pin_memory() for s in VALUE_SHAPES]
+    with zk.Server(0, 4 << 30, 8, device_loop=True) as srv:
+        tickets = [srv.submit(*s, inp, caps_host=ch, input_is_values=True)
+                   for s, inp, ch in zip(VALUE_SHAPES, inputs, caps_host)]
+        for t, s, so, ch in zip(tickets, VALUE_SHAPES, solo, caps_host):
+            check(srv, t, s, so, ch)
+        # and a coefficient-form request after them, through the same loop
+        shape = (13, 3, 24, 4, 3)
+        inp = to_dev(O.field_data(4790, shape[2] << shape[0]))
+        ch = torch.zeros((1 << shape[3]) * 4, dtype=torch.int64).pin_memory()
+        check(srv, srv.submit(*shape, inp, caps_host=ch), shape, alone(*shape, inp), ch)
+
+
 def test_more_requests_than_ring_entries():
     shapes = [(9 + i % 4, 1 + i % 3, 8 + 5 * i, i % 5, (0, 3)[i % 2]) for i in range(40)]
     inputs = [to_dev(O.field_data(4300 + i, s[2] << s[0])) for i, s in enumerate(shapes)]
@@ -124,4 +159,4 @@ def test_unsupported_requests_rejected_at_submit():
             with pytest.raises(zk.ZeknoxError):
                 srv.submit(*args, inp)
         with pytest.raises(zk.ZeknoxError):
-            srv.submit(12, 2, 16, 2, 0, inp, input_is_values=True)
+            srv.submit(8, 2, 16, 2, 0, inp, input_is_values=True)

@@ -495,6 +495,61 @@ std::vector<PlannedPass> lde_rows_plan(DeviceCtx &c, uint64_t *rows, const uint6
     return out;
 }
 
+bool ntt_inverse_plan_tables_resident(DeviceCtx &c, uint32_t lg)
+{
+    if (!c.tw[1][12]) return false;
+    for (const Pass &ps : plan_passes(lg, false))
+        if (ps.s_lo && !c.tw[1][ps.s_lo + ps.logr]) return false;
+    return true;
+}
+
+void ntt_inverse_plan_tables(DeviceCtx &c, uint32_t lg)
+{
+    c.twiddles(12, true);
+    for (const Pass &ps : plan_passes(lg, false))
+        if (ps.s_lo) c.twiddles(ps.s_lo + ps.logr, true);
+}
+
+std::vector<PlannedPass> ntt_inverse_plan(DeviceCtx &c, uint64_t *inout, uint32_t lg, uint64_t batches,
+                                          uint64_t *scratch, PlannedReorder &ro)
+{
+    if (lg == 0 || batches == 0) throw arg_failure("empty transform");
+    if (!ntt_inverse_plan_tables_resident(c, lg)) throw arg_failure("tables of this shape not built");
+    const uint64_t n = 1ULL << lg;
+    const auto passes = plan_passes(lg, false);
+    std::vector<PlannedPass> out;
+    for (size_t pi = 0; pi < passes.size(); pi++) {
+        const Pass &ps = passes[pi];
+        const bool first = pi == 0;
+        PlannedPass pp{};
+        NttPassArgs &a = pp.a;
+        // as run_dif for a column-output inverse DIF: inout -> scratch, then in place
+        a.src = first ? inout : scratch;
+        a.src_len = n * batches;
+        a.src_stride = n;
+        a.tw_small = c.twiddles(12, true);
+        a.tw_pass = ps.s_lo ? c.twiddles(ps.s_lo + ps.logr, true) : nullptr;
+        a.vcols = batches;
+        a.L = lg;
+        a.s_lo = ps.s_lo;
+        a.dst = scratch;
+        a.dst_stride = n;
+        a.dst_len = n * batches;
+        pp.grid = batches * (n / std::min<uint64_t>(n, PASS_TILE));
+        pp.logr = ps.logr;
+        pp.load = LOAD_PLAIN;
+        pp.store = STORE_SAME;
+        pp.direct = direct_io(ps.logr, a, false) ? 1 : 0;
+        pp.inv = 1;
+        out.push_back(pp);
+    }
+    // bit-reversed -> natural order, times n^-1 (reorder(), no coset table)
+    const uint32_t ra = lg >= 10 ? 5 : lg / 2;
+    ro = PlannedReorder{scratch, inout, n, n, lg, 0, batches, H_SIZE_INV[lg], n * batches, n * batches,
+                        batches * (1ULL << (lg - 2 * ra))};
+    return out;
+}
+
 // Passes of the fused LDE of 2^lg_n-point columns: (s_lo, log radix) pairs.
 std::vector<std::pair<uint32_t, uint32_t>> lde_rows_passes(uint32_t lg_n)
 {

@@ -384,47 +384,22 @@ static __global__ void __launch_bounds__(256) bitrev_reorder_kernel(const uint64
                                                              const uint64_t *__restrict__ tab, uint64_t src_len,
                                                              uint64_t dst_len)
 {
-    // Natural output index i = c + 2^rate * t, t < 2^lg_t, c < 2^rate.
-    // Source: virtual column (v << rate) + c, position rev(t).
-    // Split t = hi * 2^(lg_t - a) + mid * 2^a + lo with a = min(5, lg_t / 2).
     __shared__ uint64_t tile[32][33];
-    const uint32_t a = lg_t >= 10 ? 5 : lg_t / 2;
-    const uint32_t A = 1u << a;
-    const uint32_t mid_bits = lg_t - 2 * a;
-    const uint64_t n_mid = 1ULL << mid_bits;
-    const uint64_t per_col = n_mid << rate;  // (mid, c) tiles per column
-    uint64_t blk = blockIdx.x;
-    uint64_t v = blk / per_col;
-    uint64_t rem = blk % per_col;
-    uint32_t c = (uint32_t)(rem % (1u << rate));
-    uint64_t mid = rem >> rate;
-    if (v >= cols) return;
-    const uint32_t tx = threadIdx.x & 31, ty = threadIdx.x >> 5;  // 32 x 8
-    const uint64_t *s = src + ((v << rate) + c) * src_stride;
-    // read: source position q = rev(t) = rev(lo) * 2^(lg_t-a) + rev(mid) * 2^a + rev(hi)
-    // fix lo (row ry), vary hi (tx) -> contiguous source positions rev(hi)
-    uint64_t rmid = bitrev64(mid, mid_bits);
-    for (uint32_t ry = ty; ry < A; ry += 8) {
-        if (tx < A) {
-            uint64_t q = ((uint64_t)bitrev32(ry, a) << (lg_t - a)) + (rmid << a) + tx;
-            // tx = rev(hi) -> hi = rev(tx)
-            const uint64_t si = ((v << rate) + c) * src_stride + q;
-            tile[ry][bitrev32(tx, a)] = ZK_IN_BOUNDS(si, src_len, OOB_REORDER_SRC) ? src[si] : 0;
-        }
-    }
-    __syncthreads();
-    // write: t = hi * 2^(lg_t-a) + mid * 2^a + lo; fix hi (row), vary lo (tx) -> contiguous t
-    uint64_t *d = dst + v * dst_stride;
-    for (uint32_t hy = ty; hy < A; hy += 8) {
-        if (tx < A) {
-            uint64_t t = ((uint64_t)hy << (lg_t - a)) + (mid << a) + tx;
-            uint64_t i = (t << rate) + c;
-            uint64_t val = tile[tx][hy];
-            if (mul != 1) val = gl_mul(val, mul);
-            if (tab) val = gl_mul(val, __ldg(tab + i));
-            if (ZK_IN_BOUNDS(v * dst_stride + i, dst_len, OOB_REORDER_DST)) d[i] = val;
-        }
-    }
+#define ZK_REORDER_BLK blockIdx.x
+#include "ntt_reorder_body.inc"
+#undef ZK_REORDER_BLK
+}
+
+// One tile of the reorder: tile `blk` of the launch described by the
+// arguments, with `tile` (32 x 33 words) in shared memory.
+__device__ __forceinline__ void bitrev_reorder_body(const uint64_t *src, uint64_t *dst, uint64_t src_stride,
+                                                    uint64_t dst_stride, uint32_t lg_t, uint32_t rate, uint64_t cols,
+                                                    uint64_t mul, const uint64_t *tab, uint64_t src_len,
+                                                    uint64_t dst_len, uint64_t blk_index, uint64_t (*tile)[33])
+{
+#define ZK_REORDER_BLK blk_index
+#include "ntt_reorder_body.inc"
+#undef ZK_REORDER_BLK
 }
 
 // out[rev_lg(i) * cols + b] = in[b * n + i]: tiles of 64 positions x 32

@@ -62,11 +62,29 @@ struct PlannedPass {
     uint64_t grid;
     uint32_t logr;
     int load, store, direct;
+    int inv;  // inverse roots
+};
+// The bit-reversal reorder after a column-output transform, as data.
+struct PlannedReorder {
+    const uint64_t *src;
+    uint64_t *dst;
+    uint64_t src_stride, dst_stride;
+    uint32_t lg_t, rate;
+    uint64_t cols, mul, src_len, dst_len, blocks;
 };
 bool lde_rows_plan_tables_resident(DeviceCtx &c, uint32_t lg_n, uint32_t rate, uint64_t coset_gen);
 void lde_rows_plan_tables(DeviceCtx &c, uint32_t lg_n, uint32_t rate, uint64_t coset_gen);
 std::vector<PlannedPass> lde_rows_plan(DeviceCtx &c, uint64_t *rows, const uint64_t *coeffs, uint32_t lg_n,
                                        uint32_t rate, uint64_t cols, uint64_t coset_gen, uint64_t *scratch);
+
+// compute_batched_ntt's inverse (no coset) on device memory as data: the
+// passes of ntt_batch_device into `scratch` (n * batches words) and the
+// reorder back into `inout` with the factor n^-1.  Its tables must be
+// resident (ntt_inverse_plan_tables).
+bool ntt_inverse_plan_tables_resident(DeviceCtx &c, uint32_t lg);
+void ntt_inverse_plan_tables(DeviceCtx &c, uint32_t lg);
+std::vector<PlannedPass> ntt_inverse_plan(DeviceCtx &c, uint64_t *inout, uint32_t lg, uint64_t batches,
+                                          uint64_t *scratch, PlannedReorder &reorder);
 
 // Build every table a commit of this shape uses (before graph capture).
 void prepare_tables(DeviceCtx &c, uint32_t lg_n, uint32_t rate, uint64_t coset_gen, bool values);

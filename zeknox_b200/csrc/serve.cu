@@ -410,15 +410,64 @@ struct Server {
                 throw cuda_failure(-(int)cudaErrorMemoryAllocation, "device allocation refused (injected)");
             if (inject == ZK_SERVE_FAIL_SHAPE) throw arg_failure("shape rejected (injected)");
             const uint64_t gen = (r.coset_gen ? r.coset_gen : ZK_GENERATOR) % GL_P;
-            if (!lde_rows_plan_tables_resident(*ctx, r.lg_n, r.rate_bits, gen)) {
+            const bool values = r.input_is_values != 0;
+            if (!lde_rows_plan_tables_resident(*ctx, r.lg_n, r.rate_bits, gen) ||
+                (values && !ntt_inverse_plan_tables_resident(*ctx, r.lg_n))) {
                 // the table kernels need SMs the loop occupies
                 loop_stop();
                 lde_rows_plan_tables(*ctx, r.lg_n, r.rate_bits, gen);
+                if (values) ntt_inverse_plan_tables(*ctx, r.lg_n);
                 ctx->sync();
             }
             std::vector<LoopStage> plan;
+            const uint64_t *coeffs = r.input;
+            if (values) {
+                // evaluations on H -> coefficients, in the job's scratch after the
+                // LDE's (as commit_enqueue): copy, inverse transform, reorder
+                const uint64_t n = 1ULL << r.lg_n, words = n * r.cols;
+                uint64_t *cf = t.scratch + lde_rows_scratch_elems(r.lg_n, r.rate_bits, r.cols);
+                LoopStage cp{};
+                cp.kind = LS_COPY;
+                cp.blocks = (words + 16 * LOOP_THREADS - 1) / (16 * LOOP_THREADS);
+                cp.a.src = r.input;
+                cp.a.dst = cf;
+                cp.a.n_src = words;
+                push_split(plan, cp, 16.0 * LOOP_THREADS * 0.002, (uint64_t)loop_grid);
+                PlannedReorder ro{};
+                for (const PlannedPass &pp : ntt_inverse_plan(*ctx, cf, r.lg_n, r.cols, cf + words, ro)) {
+                    const bool ok = pp.inv && pp.load == LOAD_PLAIN && pp.store == STORE_SAME &&
+                                    ((pp.direct && pp.logr >= 6 && pp.logr <= 9) ||
+                                     (!pp.direct && pp.logr >= 6 && pp.logr <= 12));
+                    if (!ok) throw arg_failure("an inverse pass shape the device loop does not run");
+                    LoopStage st{};
+                    st.kind = LS_PASS;
+                    st.logr = pp.logr;
+                    st.load = (uint32_t)pp.load;
+                    st.store = (uint32_t)pp.store;
+                    st.inv = 1;
+                    st.direct = (uint32_t)pp.direct;
+                    st.blocks = pp.grid;
+                    st.a = pp.a;
+                    push_split(plan, st, LOOP_PASS_TILE * LDE_ELEM_NS, (uint64_t)loop_grid);
+                }
+                LoopStage rs{};
+                rs.kind = LS_REORDER;
+                rs.blocks = ro.blocks;
+                rs.a.src = ro.src;
+                rs.a.dst = ro.dst;
+                rs.a.src_stride = ro.src_stride;
+                rs.a.dst_stride = ro.dst_stride;
+                rs.a.L = ro.lg_t;
+                rs.a.rate = ro.rate;
+                rs.a.vcols = ro.cols;
+                rs.a.n_src = ro.mul;
+                rs.a.src_len = ro.src_len;
+                rs.a.dst_len = ro.dst_len;
+                push_split(plan, rs, (double)words / (double)ro.blocks * 0.004, (uint64_t)loop_grid);
+                coeffs = cf;
+            }
             for (const PlannedPass &pp :
-                 lde_rows_plan(*ctx, t.leaves, r.input, r.lg_n, r.rate_bits, r.cols, gen, t.scratch)) {
+                 lde_rows_plan(*ctx, t.leaves, coeffs, r.lg_n, r.rate_bits, r.cols, gen, t.scratch)) {
                 const bool ok = pp.direct && ((pp.load == LOAD_COSETS && pp.store == STORE_SAME && pp.logr >= 1 &&
                                                pp.logr <= 10) ||
                                               (pp.load == LOAD_PLAIN && pp.store == STORE_SAME && pp.logr >= 5 &&
@@ -430,6 +479,7 @@ struct Server {
                 st.logr = pp.logr;
                 st.load = (uint32_t)pp.load;
                 st.store = (uint32_t)pp.store;
+                st.direct = 1;
                 st.blocks = pp.grid;
                 st.a = pp.a;
                 push_split(plan, st, LOOP_PASS_TILE * LDE_ELEM_NS, (uint64_t)loop_grid);
@@ -832,8 +882,8 @@ extern "C" RustError zeknox_server_submit(void *server, const zk_serve_request *
         j.digests = (uint64_t *)1;
         j.caps = (uint64_t *)1;
         zk::check_job(j);
-        if (s->device_loop && (req->input_is_values || req->lg_n < 9 || req->lg_n > 22))
-            throw zk::arg_failure("the device loop takes coefficient inputs of 2^9 .. 2^22 per column");
+        if (s->device_loop && (req->lg_n < 9 || req->lg_n > 22))
+            throw zk::arg_failure("the device loop takes inputs of 2^9 .. 2^22 per column");
         const uint64_t bytes = Server::job_bytes(*req);
         std::lock_guard<std::mutex> lk(s->mu);
         if (bytes > s->budget) throw zk::arg_failure("request needs more device memory than the server's budget");

@@ -60,13 +60,19 @@ enum LoopStageKind : uint32_t {
     LS_TAIL_COOP = 6,  // one subtree per CTA from height u to its cap
     LS_FOLD = 7,       // 256 nodes of height u per CTA, one permutation per thread
     LS_TAIL = 8,       // one subtree per CTA, one permutation per thread
+    LS_COPY = 9,       // a.n_src words from a.src to a.dst, 4096 per CTA
+    LS_REORDER = 10,   // the bit-reversal reorder of a column-output transform (fields below)
 };
 
 enum LoopDone : uint32_t { LOOP_DONE_NONE = 0, LOOP_DONE_OK = 1, LOOP_DONE_TIMEOUT = 2, LOOP_DONE_ABORT = 3 };
 
+// LS_REORDER keeps its arguments in `a`: src, dst, src_stride, dst_stride,
+// L (log2 of the transform), rate, vcols (columns), n_src (the factor), tab
+// (a per-position table or null), src_len, dst_len.
 struct LoopStage {
     uint32_t kind, hash;                 // LoopStageKind; hash type of Merkle stages
     uint32_t logr, load, store, u;       // LS_PASS kernel shape; Merkle height
+    uint32_t inv, direct;                // LS_PASS: inverse roots; first sub-step straight from global memory
     uint64_t blocks;                     // CTA-sized work items of this piece
     uint64_t first;                      // index of its first work item
     uint64_t cost_ns;                    // estimated device time (the scheduler's measure of work)
@@ -222,10 +228,71 @@ __device__ __noinline__ void loop_pass(const NttPassArgs *pa, uint64_t first, ui
     }
 }
 
+// Inverse column passes (the inverse transform of an evaluation-form input).
+template <int LOGR, int DIRECT>
+__device__ __noinline__ void loop_pass_inv(const NttPassArgs *pa, uint64_t first, uint64_t blocks, uint64_t *sm,
+                                           LoopWork w)
+{
+    const NttPassArgs a = *pa;
+    for (uint64_t b = w.rank; b < blocks; b = loop_grab(w)) {
+        ntt_pass_body<LOGR, 1, LOOP_THREADS, LOOP_PASS_TILE, LOAD_PLAIN, STORE_SAME, DIRECT>(a, (uint32_t)(first + b),
+                                                                                         sm);
+        __syncthreads();
+    }
+}
+
+__device__ __noinline__ void loop_copy(const LoopStage *pst, LoopWork w)
+{
+    const uint64_t *src = pst->a.src;
+    uint64_t *dst = pst->a.dst;
+    const uint64_t count = pst->a.n_src, first = pst->first, blocks = pst->blocks;
+    for (uint64_t b = w.rank; b < blocks; b = loop_grab(w)) {
+        const uint64_t base = (first + b) * (16 * LOOP_THREADS);
+#pragma unroll 4
+        for (uint32_t k = 0; k < 16; k++) {
+            const uint64_t i = base + k * LOOP_THREADS + threadIdx.x;
+            if (i < count) dst[i] = src[i];
+        }
+    }
+}
+
+__device__ __noinline__ void loop_reorder(const LoopStage *pst, uint64_t (*tile)[33], LoopWork w)
+{
+    const NttPassArgs a = pst->a;
+    const uint64_t first = pst->first, blocks = pst->blocks;
+    for (uint64_t b = w.rank; b < blocks; b = loop_grab(w)) {
+        bitrev_reorder_body(a.src, a.dst, a.src_stride, a.dst_stride, a.L, a.rate, a.vcols, a.n_src, a.tab,
+                            a.src_len, a.dst_len, first + b, tile);
+        __syncthreads();
+    }
+}
+
 // The pass shapes a planned fused LDE of 2^9 .. 2^22-point columns uses with
-// the row-output radix 2^8 (the host rejects any other before posting).
+// the row-output radix 2^8, and the inverse column passes of the same sizes
+// (the host rejects any other before posting).
 __device__ __forceinline__ void loop_run_pass(const LoopStage &st, const NttPassArgs *a, uint64_t *sm, LoopWork w)
 {
+    if (st.inv) {
+        if (st.direct) {
+            switch (st.logr) {
+            case 6: loop_pass_inv<6, 1>(a, st.first, st.blocks, sm, w); break;
+            case 7: loop_pass_inv<7, 1>(a, st.first, st.blocks, sm, w); break;
+            case 8: loop_pass_inv<8, 1>(a, st.first, st.blocks, sm, w); break;
+            default: loop_pass_inv<9, 1>(a, st.first, st.blocks, sm, w); break;
+            }
+        } else {
+            switch (st.logr) {
+            case 6: loop_pass_inv<6, 0>(a, st.first, st.blocks, sm, w); break;
+            case 7: loop_pass_inv<7, 0>(a, st.first, st.blocks, sm, w); break;
+            case 8: loop_pass_inv<8, 0>(a, st.first, st.blocks, sm, w); break;
+            case 9: loop_pass_inv<9, 0>(a, st.first, st.blocks, sm, w); break;
+            case 10: loop_pass_inv<10, 0>(a, st.first, st.blocks, sm, w); break;
+            case 11: loop_pass_inv<11, 0>(a, st.first, st.blocks, sm, w); break;
+            default: loop_pass_inv<12, 0>(a, st.first, st.blocks, sm, w); break;
+            }
+        }
+        return;
+    }
     if (st.load == LOAD_COSETS && st.store == STORE_SAME) {
         switch (st.logr) {
         case 1: loop_pass<1, LOAD_COSETS, STORE_SAME>(a, st.first, st.blocks, sm, w); break;
@@ -686,6 +753,8 @@ __global__ void __launch_bounds__(LOOP_THREADS, ZK_LOOP_MIN_CTAS) serve_loop_ker
         __syncthreads();
         const LoopStage &st = s_stage;
         if (st.kind == LS_PASS) loop_run_pass(st, &st.a, loop_sm, w);
+        else if (st.kind == LS_COPY) loop_copy(&st, w);
+        else if (st.kind == LS_REORDER) loop_reorder(&st, (uint64_t(*)[33])loop_sm, w);
         else if (st.hash == HASH_POSEIDON2) loop_run_merkle<HASH_POSEIDON2>(st, loop_sm, w);
         else if (st.hash == HASH_KECCAK) loop_run_merkle<HASH_KECCAK>(st, loop_sm, w);
         else if (st.hash == HASH_MONOLITH) loop_run_merkle<HASH_MONOLITH>(st, loop_sm, w);
