@@ -201,9 +201,12 @@ RustError zeknox_server_cancel(void *server, uint64_t ticket);
 RustError zeknox_server_inject_failure(void *server, int stage);
 /* Device-loop servers: the per-stage trace of a finished request (until it is
  * released).  *n = its number of stages; for the first `max` of them kinds[q]
- * = the stage (16 + log2 radix: an LDE pass; 2 leaves; 3 leaves, four threads
- * per leaf; 4 a tree level; 5 the cooperative fold; 6 the tail) and ns[q] =
- * its time on the device, barrier to barrier (%globaltimer).  Either array may
+ * = the stage (16 + log2 radix: a transform pass, forward or inverse; 2
+ * leaves; 3 leaves, four threads per leaf; 4 a tree level; 5 / 6 the
+ * cooperative fold / tail; 7 / 8 the fold / tail with one permutation per
+ * thread; 9 the copy of an evaluation-form input; 10 the bit-reversal
+ * reorder) and ns[q] = its time on the device, barrier to barrier
+ * (%globaltimer).  Either array may
  * be NULL.  Requests of the host-driven mode have no trace (*n = 0). */
 RustError zeknox_server_trace(void *server, uint64_t ticket, uint32_t *kinds, uint64_t *ns, uint32_t max, uint32_t *n);
 /* Free the ticket's device results (returns their bytes to the budget). */

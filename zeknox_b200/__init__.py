@@ -586,8 +586,8 @@ class Server:
 
     def trace(self, ticket):
         """zeknox_server_trace: [(stage kind, device ns)] of a finished
-        device-loop request (16 + log2 radix: LDE pass; 2/3 leaves; 4 level;
-        5 fold; 6 tail)."""
+        device-loop request (16 + log2 radix: transform pass; 2/3 leaves; 4
+        level; 5/6 cooperative fold/tail; 7/8 fold/tail; 9 copy; 10 reorder)."""
         n = ctypes.c_uint32()
         _check(load().zeknox_server_trace(self._h, ticket, None, None, 0, ctypes.byref(n)))
         kinds, ns = (ctypes.c_uint32 * max(n.value, 1))(), (ctypes.c_uint64 * max(n.value, 1))()
