@@ -133,7 +133,9 @@ RustError zeknox_lde_rows_noalloc(size_t device_id, uint64_t *rows, const uint64
 typedef struct {
     uint32_t lg_n, rate_bits, cols, cap_height, hash_type, input_is_values;
     uint64_t coset_gen;       /* 0 means 7 */
-    const uint64_t *input;    /* device: cols x 2^lg_n, column-major; must stay valid until done */
+    const uint64_t *input;    /* cols x 2^lg_n, column-major, read in place by the server's kernels:
+                                 device or pinned host memory (pageable host memory is rejected at
+                                 submit unless the GPU can read it); must stay valid until done */
     uint64_t *caps_host;      /* host buffer of 2^cap_height x 4 words, filled on completion (may be NULL) */
 } zk_serve_request;
 

@@ -160,3 +160,24 @@ def test_unsupported_requests_rejected_at_submit():
                 srv.submit(*args, inp)
         with pytest.raises(zk.ZeknoxError):
             srv.submit(8, 2, 16, 2, 0, inp, input_is_values=True)
+
+
+def test_pageable_input_rejected_unless_readable():
+    # the server's kernels read the input in place: pageable host memory is
+    # refused at submit on a GPU without pageable-memory access (no fault)
+    s = (12, 2, 16, 2, 0)
+    pageable = torch.from_numpy(O.field_data(17, 16 << 12).view(np.int64).copy())
+    assert not pageable.is_pinned()
+    from cuda.bindings import runtime as rt
+
+    err, readable = rt.cudaDeviceGetAttribute(rt.cudaDeviceAttr.cudaDevAttrPageableMemoryAccess, 0)
+    assert err == rt.cudaError_t.cudaSuccess
+    for loop in (False, True):
+        with zk.Server(0, 1 << 30, 2, device_loop=loop) as srv:
+            if not readable:
+                with pytest.raises(zk.ZeknoxError, match="pageable"):
+                    srv.submit(*s, pageable)
+                assert srv.stats()["completed"] == 0
+            else:
+                ch = torch.zeros((1 << s[3]) * 4, dtype=torch.int64).pin_memory()
+                check(srv, srv.submit(*s, pageable, caps_host=ch), s, alone(*s, pageable.cuda()), ch)

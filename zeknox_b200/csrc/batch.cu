@@ -40,6 +40,22 @@ bool is_host_pointer(const void *p)
     return a.type == cudaMemoryTypeHost || a.type == cudaMemoryTypeUnregistered;
 }
 
+bool device_can_read(const void *p, int dev)
+{
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        (void)cudaGetLastError();
+        a.type = cudaMemoryTypeUnregistered;
+    }
+    if (a.type != cudaMemoryTypeUnregistered) return true;  // device, managed or pinned (mapped) host memory
+    int pageable = 0;
+    if (cudaDeviceGetAttribute(&pageable, cudaDevAttrPageableMemoryAccess, dev) != cudaSuccess) {
+        (void)cudaGetLastError();
+        return false;
+    }
+    return pageable != 0;
+}
+
 static uint64_t gen_of(const zk_commit_job &j) { return j.coset_gen ? j.coset_gen : ZK_GENERATOR; }
 
 void prepare_job(DeviceCtx &c, const zk_commit_job &j)

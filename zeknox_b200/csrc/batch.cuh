@@ -16,6 +16,9 @@ uint64_t commit_scratch_words(uint32_t lg_n, uint32_t rate_bits, uint32_t cols, 
 
 // True when p is host memory (pinned or pageable).
 bool is_host_pointer(const void *p);
+// False for pageable host memory when device `dev` cannot read pageable memory
+// (no HMM / ATS): kernels that read such a pointer directly would fault.
+bool device_can_read(const void *p, int dev);
 
 // Queue one commit on `s` using `scratch` (commit_scratch_words words, may be
 // null when that is 0).  Allocates nothing and never synchronises, so it can be

@@ -884,6 +884,9 @@ extern "C" RustError zeknox_server_submit(void *server, const zk_serve_request *
         zk::check_job(j);
         if (s->device_loop && (req->lg_n < 9 || req->lg_n > 22))
             throw zk::arg_failure("the device loop takes inputs of 2^9 .. 2^22 per column");
+        // the server's kernels read the input in place
+        if (!zk::device_can_read(req->input, s->ctx->id))
+            throw zk::arg_failure("input is pageable host memory this GPU cannot read: pass device or pinned host memory");
         const uint64_t bytes = Server::job_bytes(*req);
         std::lock_guard<std::mutex> lk(s->mu);
         if (bytes > s->budget) throw zk::arg_failure("request needs more device memory than the server's budget");
