@@ -640,10 +640,11 @@ __device__ uint32_t loop_rank(LoopCtl *ctl, uint64_t barrier_ns)
     if (threadIdx.x < 8) s_sm_bits[threadIdx.x] = 0;
     if (threadIdx.x == 0) {
         s_slot = 0;
-        ctl->cta_sm[blockIdx.x] = smid;
+        if (blockIdx.x < LOOP_MAX_CTAS) ctl->cta_sm[blockIdx.x] = smid;
         if (smid >= 256 || gridDim.x > LOOP_MAX_CTAS) atomicExch(&ctl->rank_bad, 1u);
     }
     if (!loop_grid_sync(ctl, barrier_ns)) return blockIdx.x;
+    if (gridDim.x > LOOP_MAX_CTAS) return blockIdx.x;  // ranks = block indices (rank_bad is set)
     for (uint32_t j = threadIdx.x; j < gridDim.x; j += LOOP_THREADS) {
         const uint32_t sm_j = *(volatile uint32_t *)&ctl->cta_sm[j];
         if (sm_j < 256) atomicOr(&s_sm_bits[sm_j >> 5], 1u << (sm_j & 31));
