@@ -181,3 +181,39 @@ def test_pageable_input_rejected_unless_readable():
             else:
                 ch = torch.zeros((1 << s[3]) * 4, dtype=torch.int64).pin_memory()
                 check(srv, srv.submit(*s, pageable, caps_host=ch), s, alone(*s, pageable.cuda()), ch)
+
+
+def _corner_columns(lg, seed):
+    P = O.P
+    n = 1 << lg
+    canon = np.array(O.CANONICAL_CORNERS, dtype=np.uint64)
+    pick = canon[np.random.default_rng(seed).integers(0, canon.size, n)]
+    cols = [np.zeros(n, np.uint64), np.full(n, P - 1, np.uint64), np.tile(np.array([0, P - 1], np.uint64), n // 2),
+            np.tile(np.array([P - 1, 1], np.uint64), n // 2), np.full(n, P - (1 << 32), np.uint64),
+            np.full(n, (1 << 32) - 1, np.uint64), pick, pick[::-1].copy()]
+    return np.concatenate(cols)
+
+
+@pytest.mark.parametrize("values", [False, True])
+@pytest.mark.parametrize("h", [zk.HASH_POSEIDON, zk.HASH_POSEIDON2, zk.HASH_KECCAK])
+def test_corner_columns_through_loop_match_oracle(values, h):
+    """Columns of field corner values (0, p-1, alternating, p-2^32, 2^32-1,
+    corner draws) through the device loop, bit-exact against the oracle."""
+    lg, rate, cap = 10, 2, 3
+    x = _corner_columns(lg, 990 + h)
+    cols = x.size >> lg
+    coeffs = O.batched_ntt(x, lg, cols, inverse=True) if values else x
+    rows = O.lde_rows(coeffs, lg, rate, cols)
+    d, c = O.merkle(rows, cols, cap, h)
+    N = 1 << (lg + rate)
+    ch = torch.zeros((1 << cap) * 4, dtype=torch.int64).pin_memory()
+    inp = to_dev(x)  # held until the request is done
+    with zk.Server(0, 1 << 30, 2, device_loop=True) as srv:
+        t = srv.submit(lg, rate, cols, cap, h, inp, caps_host=ch, input_is_values=values)
+        r = srv.wait(t)
+        assert r.status == 2, r.status
+        n_dig, _ = zk.merkle_sizes(N, cap)
+        assert np.array_equal(device_words(r.leaves, N * cols), rows)
+        assert np.array_equal(device_words(r.digests, n_dig * 4).reshape(-1, 4), d)
+        assert np.array_equal(ch.numpy().view(np.uint64).reshape(-1, 4), c)
+        srv.release(t)
