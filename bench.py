@@ -652,6 +652,11 @@ def measure_hashes(steps):
     torch.cuda.synchronize()
     batch_ms = a.elapsed_time(b) / steps
     per = {}
+    # Poseidon-BN128 (hash type 2) alone on the same shape, outside the batch
+    leaves_bn = dev_field(nl * ls, 43)
+    n_dig, n_cap = zk.merkle_sizes(nl, ch)
+    trees.append((2, leaves_bn, torch.empty(n_dig * 4, dtype=torch.int64, device="cuda"),
+                  torch.empty(n_cap * 4, dtype=torch.int64, device="cuda")))
     for h, l, d, c in trees:
         zk.fill_digests_buf_linear_gpu(d, c, l, nl, ls, ch, h)
         torch.cuda.synchronize()
@@ -661,13 +666,14 @@ def measure_hashes(steps):
         b.record(legacy)
         torch.cuda.synchronize()
         ms = a.elapsed_time(b) / steps
-        name = {3: "poseidon2", 4: "monolith", 1: "keccak"}[h]
+        name = {3: "poseidon2", 4: "monolith", 1: "keccak", 2: "poseidon_bn128"}[h]
         perms = perms_of(nl, ls, ch) if h != 1 else nl * ((ls * 8) // 136 + 1) + (nl - (1 << ch))
         per[name] = {"ms": ms, "leaves_per_s": nl / (ms * 1e-3), "perms_per_s": perms / (ms * 1e-3)}
     del trees, jobs
     torch.cuda.empty_cache()
     return {"batched_leaves_per_s": 3 * nl / (batch_ms * 1e-3), "batched_ms": batch_ms, "per_hash": per,
-            "steps": steps, "workload": "Poseidon2 + Monolith + Keccak forests, 2^20 leaves x 135, cap 4, one batch"}
+            "steps": steps, "workload": "Poseidon2 + Monolith + Keccak forests, 2^20 leaves x 135, cap 4, one batch; "
+                                        "each alone, and Poseidon-BN128 alone"}
 
 
 def run_hashes(args):

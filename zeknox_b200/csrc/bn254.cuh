@@ -133,6 +133,69 @@ ZK_FR_HD Fr fr_exp5(const Fr &x)
     return fr_mul(x4, x);
 }
 
+// Sums of products reduced once (the matrix layers' dot products): a 512-bit
+// accumulator of products of elements < r, then one Montgomery reduction.
+// For at most five products the sum is below 5 r^2 < 2^510 and the reduced
+// value (sum + m r) / 2^256 below (5r / 2^256 + 1) r < 2r, so one conditional
+// subtraction makes it canonical: the same value as five fr_mul and four
+// fr_add, for one reduction instead of five.
+struct FrWide {
+    uint32_t w[16];
+};
+
+ZK_FR_HD void fr_wide_zero(FrWide &t)
+{
+#pragma unroll
+    for (int i = 0; i < 16; i++) t.w[i] = 0;
+}
+
+// t += a * b  (t stays below 2^512 for the sums above)
+ZK_FR_HD void fr_mac_wide(FrWide &t, const Fr &a, const Fr &b)
+{
+#pragma unroll
+    for (int i = 0; i < 8; i++) {
+        uint64_t c = 0;
+#pragma unroll
+        for (int j = 0; j < 8; j++) {
+            const uint64_t p = (uint64_t)a.w[i] * b.w[j] + t.w[i + j] + c;
+            t.w[i + j] = (uint32_t)p;
+            c = p >> 32;
+        }
+#pragma unroll
+        for (int k = i + 8; k < 16; k++) {
+            const uint64_t s = (uint64_t)t.w[k] + c;
+            t.w[k] = (uint32_t)s;
+            c = s >> 32;
+        }
+    }
+}
+
+// t * R^-1 mod r for t < 5 r^2, canonical
+ZK_FR_HD Fr fr_reduce_wide(FrWide t)
+{
+#pragma unroll
+    for (int i = 0; i < 8; i++) {
+        const uint32_t m = t.w[i] * ZK_BN254_NP;
+        uint64_t c = 0;
+#pragma unroll
+        for (int j = 0; j < 8; j++) {
+            const uint64_t p = (uint64_t)m * bn_r_limb(j) + t.w[i + j] + c;
+            t.w[i + j] = (uint32_t)p;
+            c = p >> 32;
+        }
+#pragma unroll
+        for (int k = i + 8; k < 16; k++) {
+            const uint64_t s = (uint64_t)t.w[k] + c;
+            t.w[k] = (uint32_t)s;
+            c = s >> 32;
+        }
+    }
+    Fr z;
+#pragma unroll
+    for (int i = 0; i < 8; i++) z.w[i] = t.w[8 + i];
+    return fr_reduce_once(z);
+}
+
 // Montgomery form of a value < r given as plain limbs, and back
 ZK_FR_HD Fr fr_to_mont(const Fr &x)
 {

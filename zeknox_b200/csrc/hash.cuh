@@ -442,10 +442,58 @@ ZK_HD void keccak_f(uint64_t st[25])
         return x_;                                                           \
     }())
 
-// new_i = sum_j m[j][i] * s_j with m = P (pre = true) or M
+// The matrix layers' dot products of five terms as one reduction (1) or as
+// five fr_mul and four fr_add (0).  Both give the same canonical values.  The
+// first measured 1.26x on Poseidon-BN128 forests (2^14 x 135: 23.5 ms
+// against 29.5) and is the default.  The device-resident request loop
+// compiles the second: built with the first, its kernel's register frame grew
+// and its transform stages ran 14% slower (2^20 x 256 LDE: 61.0 ms against
+// 53.7), because all stages share that kernel's 64-register budget.
+#ifndef ZK_BN128_DOT_ONE_REDUCTION
+#define ZK_BN128_DOT_ONE_REDUCTION 1
+#endif
+
+// sum_j c_j * s_j, c_j = constant element c0 + j * cstep of a table
+#if ZK_BN128_DOT_ONE_REDUCTION
+#define ZK_BN_DOT5(out, tab, c0, cstep, s0, s1, s2, s3, s4)                          \
+    do {                                                                               \
+        FrWide acc_;                                                                   \
+        fr_wide_zero(acc_);                                                            \
+        fr_mac_wide(acc_, ZK_BN_CONST(tab, (c0)), s0);                                 \
+        fr_mac_wide(acc_, ZK_BN_CONST(tab, (c0) + (cstep)), s1);                       \
+        fr_mac_wide(acc_, ZK_BN_CONST(tab, (c0) + 2 * (cstep)), s2);                   \
+        fr_mac_wide(acc_, ZK_BN_CONST(tab, (c0) + 3 * (cstep)), s3);                   \
+        fr_mac_wide(acc_, ZK_BN_CONST(tab, (c0) + 4 * (cstep)), s4);                   \
+        out = fr_reduce_wide(acc_);                                                    \
+    } while (0)
+#else
+#define ZK_BN_DOT5(out, tab, c0, cstep, s0, s1, s2, s3, s4)                          \
+    do {                                                                               \
+        out = fr_mul(ZK_BN_CONST(tab, (c0)), s0);                                      \
+        out = fr_add(out, fr_mul(ZK_BN_CONST(tab, (c0) + (cstep)), s1));               \
+        out = fr_add(out, fr_mul(ZK_BN_CONST(tab, (c0) + 2 * (cstep)), s2));           \
+        out = fr_add(out, fr_mul(ZK_BN_CONST(tab, (c0) + 3 * (cstep)), s3));           \
+        out = fr_add(out, fr_mul(ZK_BN_CONST(tab, (c0) + 4 * (cstep)), s4));           \
+    } while (0)
+#endif
+
+// new_i = sum_j m[j][i] * s_j with m = P (pre = true) or M.  With one
+// reduction per output the outputs are computed in a rolled loop (one copy of
+// the dot product's code) and shifted into place.
 ZK_HD void bn128_mix(Fr st[5], bool pre)
 {
     Fr ns[5];
+#if ZK_BN128_DOT_ONE_REDUCTION
+#pragma unroll 1
+    for (int i = 0; i < 5; i++) {
+        Fr o;
+        if (pre) ZK_BN_DOT5(o, BN128_P, i, 5, st[0], st[1], st[2], st[3], st[4]);
+        else ZK_BN_DOT5(o, BN128_M, i, 5, st[0], st[1], st[2], st[3], st[4]);
+#pragma unroll
+        for (int q = 0; q < 4; q++) ns[q] = ns[q + 1];
+        ns[4] = o;
+    }
+#else
 #pragma unroll
     for (int i = 0; i < 5; i++) {
 #pragma unroll
@@ -455,6 +503,7 @@ ZK_HD void bn128_mix(Fr st[5], bool pre)
             ns[i] = j == 0 ? t : fr_add(ns[i], t);
         }
     }
+#endif
 #pragma unroll
     for (int i = 0; i < 5; i++) st[i] = ns[i];
 }
@@ -491,9 +540,8 @@ ZK_HD void poseidon_bn128_permute(uint64_t s[12])
 #pragma unroll 1
             for (int r = 0; r < 60; r++) {
                 const Fr x0 = fr_add(fr_exp5(st[0]), ZK_BN_CONST(BN128_C, 25 + r));
-                Fr n0 = fr_mul(ZK_BN_CONST(BN128_S, 9 * r), x0);
-#pragma unroll
-                for (int j = 1; j < 5; j++) n0 = fr_add(n0, fr_mul(ZK_BN_CONST(BN128_S, 9 * r + j), st[j]));
+                Fr n0;
+                ZK_BN_DOT5(n0, BN128_S, 9 * r, 1, x0, st[1], st[2], st[3], st[4]);
 #pragma unroll
                 for (int k = 1; k < 5; k++) st[k] = fr_add(st[k], fr_mul(x0, ZK_BN_CONST(BN128_S, 9 * r + 4 + k)));
                 st[0] = n0;

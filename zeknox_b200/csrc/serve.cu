@@ -38,6 +38,9 @@
 #include <thread>
 #include <vector>
 
+// the loop kernel's Poseidon-BN128 matrix layers as five reductions per dot
+// product (the register budget the loop's stages share; hash.cuh)
+#define ZK_BN128_DOT_ONE_REDUCTION 0
 #include "../../include/zeknox_b200.h"
 #include "batch.cuh"
 #include "ntt_api.cuh"
