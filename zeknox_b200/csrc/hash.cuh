@@ -444,8 +444,10 @@ ZK_HD void keccak_f(uint64_t st[25])
 
 // The matrix layers' dot products of five terms as one reduction (1) or as
 // five fr_mul and four fr_add (0).  Both give the same canonical values.  The
-// first measured 1.26x on Poseidon-BN128 forests (2^14 x 135: 23.5 ms
-// against 29.5) and is the default.  The device-resident request loop
+// first measured 1.26x on a 2^14 x 135 Poseidon-BN128 forest (23.5 ms against
+// 29.5), where the permutation's latency bounds the time, and no change on a
+// 2^20 x 135 forest, which fills the GPU (555 ms against 540); it is the
+// default.  The device-resident request loop
 // compiles the second: built with the first, its kernel's register frame grew
 // and its transform stages ran 14% slower (2^20 x 256 LDE: 61.0 ms against
 // 53.7), because all stages share that kernel's 64-register budget.
