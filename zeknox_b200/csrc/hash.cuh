@@ -447,10 +447,12 @@ ZK_HD void keccak_f(uint64_t st[25])
 // first measured 1.26x on a 2^14 x 135 Poseidon-BN128 forest (23.5 ms against
 // 29.5), where the permutation's latency bounds the time, and no change on a
 // 2^20 x 135 forest, which fills the GPU (555 ms against 540); it is the
-// default.  The device-resident request loop
-// compiles the second: built with the first, its kernel's register frame grew
-// and its transform stages ran 14% slower (2^20 x 256 LDE: 61.0 ms against
-// 53.7), because all stages share that kernel's 64-register budget.
+// default.  The device-resident request loop compiles the second: built with
+// the first, its kernel's register frame grew and its transform stages ran
+// 14% slower (2^20 x 256 LDE: 61.0 ms against 53.7), because all stages share
+// that kernel's 64-register budget.  Units built with different settings
+// hold different bodies of the functions below; they are force-inlined (no
+// out-of-line host symbol) and device code is not linked across units.
 #ifndef ZK_BN128_DOT_ONE_REDUCTION
 #define ZK_BN128_DOT_ONE_REDUCTION 1
 #endif
