@@ -196,6 +196,16 @@ ZK_FR_HD Fr fr_reduce_wide(FrWide t)
     return fr_reduce_once(z);
 }
 
+// Out-of-line copies of the two steps: a permutation that takes many dot
+// products then holds one copy of their code (the instruction cache).
+ZK_FR_NOINLINE FrWide fr_mac_wide_ol(FrWide t, const Fr a, const Fr b)
+{
+    fr_mac_wide(t, a, b);
+    return t;
+}
+
+ZK_FR_NOINLINE Fr fr_reduce_wide_ol(const FrWide t) { return fr_reduce_wide(t); }
+
 // Montgomery form of a value < r given as plain limbs, and back
 ZK_FR_HD Fr fr_to_mont(const Fr &x)
 {

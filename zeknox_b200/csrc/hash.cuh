@@ -444,15 +444,17 @@ ZK_HD void keccak_f(uint64_t st[25])
 
 // The matrix layers' dot products of five terms as one reduction (1) or as
 // five fr_mul and four fr_add (0).  Both give the same canonical values.  The
-// first measured 1.26x on a 2^14 x 135 Poseidon-BN128 forest (23.5 ms against
-// 29.5), where the permutation's latency bounds the time, and no change on a
-// 2^20 x 135 forest, which fills the GPU (555 ms against 540); it is the
-// default.  The device-resident request loop compiles the second: built with
-// the first, its kernel's register frame grew and its transform stages ran
-// 14% slower (2^20 x 256 LDE: 61.0 ms against 53.7), because all stages share
-// that kernel's 64-register budget.  Units built with different settings
-// hold different bodies of the functions below; they are force-inlined (no
-// out-of-line host symbol) and device code is not linked across units.
+// first, with its product and reduction steps out of line (one copy of their
+// code: inlined at the call sites they stalled the leaf kernel on instruction
+// fetch), measured 1.20x on a 2^20 x 135 Poseidon-BN128 forest (450 ms against
+// 540) and 1.64x on a 2^14 x 135 one (18.0 against 29.5), with 128-thread leaf
+// CTAs; it is the default.  The device-resident request loop compiles the
+// second: built with the first (inlined), its kernel's register frame grew
+// and its transform stages ran 14% slower (2^20 x 256 LDE: 61.0 ms against
+// 53.7), because all stages share that kernel's 64-register budget.  Units
+// built with different settings hold different bodies of the functions
+// below; they are force-inlined (no out-of-line host symbol), the steps they
+// call are file-local, and device code is not linked across units.
 #ifndef ZK_BN128_DOT_ONE_REDUCTION
 #define ZK_BN128_DOT_ONE_REDUCTION 1
 #endif
@@ -463,12 +465,12 @@ ZK_HD void keccak_f(uint64_t st[25])
     do {                                                                               \
         FrWide acc_;                                                                   \
         fr_wide_zero(acc_);                                                            \
-        fr_mac_wide(acc_, ZK_BN_CONST(tab, (c0)), s0);                                 \
-        fr_mac_wide(acc_, ZK_BN_CONST(tab, (c0) + (cstep)), s1);                       \
-        fr_mac_wide(acc_, ZK_BN_CONST(tab, (c0) + 2 * (cstep)), s2);                   \
-        fr_mac_wide(acc_, ZK_BN_CONST(tab, (c0) + 3 * (cstep)), s3);                   \
-        fr_mac_wide(acc_, ZK_BN_CONST(tab, (c0) + 4 * (cstep)), s4);                   \
-        out = fr_reduce_wide(acc_);                                                    \
+        acc_ = fr_mac_wide_ol(acc_, ZK_BN_CONST(tab, (c0)), s0);                       \
+        acc_ = fr_mac_wide_ol(acc_, ZK_BN_CONST(tab, (c0) + (cstep)), s1);             \
+        acc_ = fr_mac_wide_ol(acc_, ZK_BN_CONST(tab, (c0) + 2 * (cstep)), s2);         \
+        acc_ = fr_mac_wide_ol(acc_, ZK_BN_CONST(tab, (c0) + 3 * (cstep)), s3);         \
+        acc_ = fr_mac_wide_ol(acc_, ZK_BN_CONST(tab, (c0) + 4 * (cstep)), s4);         \
+        out = fr_reduce_wide_ol(acc_);                                                 \
     } while (0)
 #else
 #define ZK_BN_DOT5(out, tab, c0, cstep, s0, s1, s2, s3, s4)                          \
