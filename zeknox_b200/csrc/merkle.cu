@@ -30,6 +30,13 @@ constexpr int leaf_t_default()
 {
     return H == HASH_POSEIDON_BN128 ? 128 : LEAF_T;
 }
+// Threads per CTA of the node-parallel level kernel: 128 for Poseidon-BN128
+// (158 registers: three CTAs per SM instead of one), 256 otherwise.
+template <int H>
+constexpr unsigned level_t()
+{
+    return H == HASH_POSEIDON_BN128 ? 128u : 256u;
+}
 static constexpr int FOLD_T = 256;     // leaf digests per CTA of the fold kernel
 static constexpr int TAIL_MAXM = 1024; // nodes a tail CTA can take
 static constexpr int LEAF_LEVELS = 3;  // tree levels the Poseidon2 leaf kernel folds in its CTAs
@@ -87,7 +94,8 @@ static void merkle_launch(uint64_t *digests, uint64_t *caps, const uint64_t *lea
     while (u0 + 1 <= top && (g.n_leaves >> (u0 + 1)) >= wide) {
         u0++;
         const uint64_t total = g.n_leaves >> u0;
-        merkle_level_kernel<H><<<(unsigned)((total + 255) / 256), 256, 0, s>>>(digests, g, u0);
+        merkle_level_kernel<H><<<(unsigned)((total + level_t<H>() - 1) / level_t<H>()), level_t<H>(), 0, s>>>(digests, g,
+                                                                                                          u0);
         note_launch();
     }
     // Narrow levels: folded inside CTAs of fold_nodes nodes.
@@ -106,9 +114,9 @@ static void merkle_launch(uint64_t *digests, uint64_t *caps, const uint64_t *lea
     while ((g.sub_leaves >> u0) > (uint64_t)TAIL_MAXM) {
         u0++;
         uint64_t total = (g.sub_leaves >> u0) * g.n_caps;
-        uint64_t nb = (total + 255) / 256;
+        uint64_t nb = (total + level_t<H>() - 1) / level_t<H>();
         if (nb > 65535) nb = 65535;
-        merkle_level_kernel<H><<<(unsigned)nb, 256, 0, s>>>(digests, g, u0);
+        merkle_level_kernel<H><<<(unsigned)nb, level_t<H>(), 0, s>>>(digests, g, u0);
         note_launch();
     }
     if constexpr (COOP) merkle_tail_coop_kernel<H, TAIL_MAXM><<<g.n_caps, 256, 0, s>>>(digests, caps, g, u0);
