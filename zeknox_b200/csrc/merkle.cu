@@ -31,7 +31,9 @@ constexpr int leaf_t_default()
     return H == HASH_POSEIDON_BN128 ? 128 : LEAF_T;
 }
 // Threads per CTA of the node-parallel level kernel: 128 for Poseidon-BN128
-// (158 registers: three CTAs per SM instead of one), 256 otherwise.
+// (158 registers: three CTAs per SM instead of one), 256 otherwise.  The wide
+// levels are ~6% of a forest's permutations: 2^20 x 135 Poseidon-BN128
+// forest 449.0 against 450.2 ms.
 template <int H>
 constexpr unsigned level_t()
 {
